@@ -1,0 +1,981 @@
+// context.cu -- the C ABI (include/gev.h): context, device memory, call
+// sequencing of the kernels, background integrator and step driver.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "gev.h"
+#include "kernels.h"
+
+namespace gev {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct ArgError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct StateError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct DeviceError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct CapacityError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct NoMemError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+static void ck(cudaError_t e, const char *what)
+{
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        throw NoMemError(std::string(what) + ": " + cudaGetErrorString(e));
+    }
+    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class T> struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count, const char *what)
+    {
+        free();
+        if (count == 0) return;
+        ck(cudaMalloc((void **)&p, count * sizeof(T)), what);
+        n = count;
+    }
+    void free()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DBuf() { free(); }
+};
+
+template <class A, class B>
+__global__ void k_convert(const A *src, B *dst, int64_t n)
+{
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = (B)src[i];
+}
+
+// ---------------------------------------------------------------------------
+// findIntersectingLightcones (tools.hpp:637-886), one domain = the whole box.
+// Up to 64 periodic images are kept (the reference keeps MAX_INTERSECTS = 12 and
+// warns that data is lost beyond that, tools.hpp:877-882).
+// ---------------------------------------------------------------------------
+static int find_intersecting(const double *lcv, const double *dir, double opening, double outer, double inner,
+                             const double *domain, double vtx[64][3])
+{
+    int range = (int)std::ceil(outer) + 1, n = 0;
+    double cen[3], rdom = 0.0;
+    for (int i = 0; i < 3; i++) {
+        cen[i] = 0.5 * domain[i] + 0.5 * domain[i + 3];
+        rdom += (domain[i + 3] - domain[i]) * (domain[i + 3] - domain[i]);
+    }
+    rdom = 0.5 * std::sqrt(rdom);
+    for (int u = -range; u <= range; u++)
+        for (int v = -range; v <= range; v++)
+            for (int w = -range; w <= range; w++) {
+                const double x[3] = {lcv[0] + u, lcv[1] + v, lcv[2] + w};
+                double dd = 0.0;   // distance from the image to the domain box
+                for (int i = 0; i < 3; i++) {
+                    double e = x[i] < domain[i] ? domain[i] - x[i] : (x[i] > domain[i + 3] ? x[i] - domain[i + 3] : 0.0);
+                    dd += e * e;
+                }
+                if (std::sqrt(dd) > outer) continue;
+                bool inside = true;   // domain entirely within the inner sphere
+                for (int c = 0; c < 8 && inside; c++) {
+                    double cc[3] = {domain[(c & 1) ? 3 : 0], domain[(c & 2) ? 4 : 1], domain[(c & 4) ? 5 : 2]};
+                    double r = std::sqrt((cc[0] - x[0]) * (cc[0] - x[0]) + (cc[1] - x[1]) * (cc[1] - x[1]) + (cc[2] - x[2]) * (cc[2] - x[2]));
+                    if (!(r < inner)) inside = false;
+                }
+                if (inside) continue;
+                double dist = std::sqrt((cen[0] - x[0]) * (cen[0] - x[0]) + (cen[1] - x[1]) * (cen[1] - x[1]) + (cen[2] - x[2]) * (cen[2] - x[2]));
+                bool take = dist <= rdom;
+                if (!take) {
+                    double ca = ((cen[0] - x[0]) * dir[0] + (cen[1] - x[1]) * dir[1] + (cen[2] - x[2]) * dir[2]) / dist;
+                    if (ca >= opening) take = true;
+                    else if (dist > outer && std::acos(ca) - std::acos(opening) <= std::acos((outer * outer + dist * dist - rdom * rdom) / (2. * outer * dist))) take = true;
+                    else if (dist <= outer && std::acos(ca) - std::acos(opening) <= std::asin(rdom / dist)) take = true;
+                }
+                if (take) {
+                    if (n < 64)
+                        for (int i = 0; i < 3; i++) vtx[n][i] = x[i];
+                    n++;
+                }
+            }
+    return n < 64 ? n : 64;
+}
+
+// ---------------------------------------------------------------------------
+// background.hpp:200-207, :235-244, :268-291 (CDM + Lambda + radiation)
+// ---------------------------------------------------------------------------
+static double hconf(double a, double fourpiG, const gev_cosmo &c)
+{
+    return std::sqrt((2. * fourpiG / 3.) * ((c.Omega_m / a) + (c.Omega_Lambda * a * a) + (c.Omega_rad / a / a)));
+}
+
+static void rk4bg(double &a, double fourpiG, const gev_cosmo &c, double dtau)
+{
+    double k1a = a * hconf(a, fourpiG, c);
+    double k2a = (a + k1a * dtau / 2.) * hconf(a + k1a * dtau / 2., fourpiG, c);
+    double k3a = (a + k2a * dtau / 2.) * hconf(a + k2a * dtau / 2., fourpiG, c);
+    double k4a = (a + k3a * dtau) * hconf(a + k3a * dtau, fourpiG, c);
+    a += dtau * (k1a + 2. * k2a + 2. * k3a + k4a) / 6.;
+}
+
+static double horizon_integrand(double s, const gev_cosmo &c) { return 2. / (s * hconf(s * s, 1., c)); }
+
+static double simpson(double lo, double hi, double flo, double fmid, double fhi, double whole, double tol, int depth,
+                      const gev_cosmo &c)
+{
+    double mid = 0.5 * (lo + hi), lm = 0.5 * (lo + mid), rm = 0.5 * (mid + hi);
+    double flm = horizon_integrand(lm, c), frm = horizon_integrand(rm, c);
+    double left = (mid - lo) / 6. * (flo + 4 * flm + fmid), right = (hi - mid) / 6. * (fmid + 4 * frm + fhi);
+    if (depth <= 0 || std::fabs(left + right - whole) <= 15 * tol) return left + right + (left + right - whole) / 15.;
+    return simpson(lo, mid, flo, flm, fmid, left, tol / 2, depth - 1, c) + simpson(mid, hi, fmid, frm, fhi, right, tol / 2, depth - 1, c);
+}
+
+static double particle_horizon(double a, double fourpiG, const gev_cosmo &c)
+{
+    double lo = std::sqrt(a) * 1.0e-7, hi = std::sqrt(a);
+    double flo = horizon_integrand(lo, c), fhi = horizon_integrand(hi, c), fm = horizon_integrand(0.5 * (lo + hi), c);
+    double whole = (hi - lo) / 6. * (flo + 4 * fm + fhi);
+    return simpson(lo, hi, flo, fm, fhi, whole, 1e-13, 60, c) / std::sqrt(fourpiG);
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct CtxBase {
+    gev_config cfg{};
+    std::string err;
+    virtual ~CtxBase() {}
+    virtual void particles_set(const double *pos, const double *q, const int64_t *id, int64_t n, double mass) = 0;
+    virtual void particles_get(double *pos, double *q, int64_t *id, int64_t cap, int64_t *n_out) = 0;
+    virtual int64_t particles_count() const = 0;
+    virtual void field_get(int f, double *host) = 0;
+    virtual void field_set(int f, const double *host) = 0;
+    virtual void project(uint32_t which, double a, double coeff, int use_phi, int accumulate) = 0;
+    virtual void solve_phi(int prepare, double bg, double c, double c2, double c3, double pc, double modif, double *sum, double *phom) = 0;
+    virtual void solve_chi(double coeff, int cycle0, double hubble, double dtau, double dtau_old, double a2dtau) = 0;
+    virtual void solve_B(double coeff, double modif) = 0;
+    virtual double kick_drift(const KickDriftParams &kp) = 0;
+    virtual void power_spectrum(int nb, double kmax, double *kb, double *pw, double *ks, double *ps, int32_t *occ) = 0;
+    virtual void lightcone(const gev_lightcone_args &lc, double tau, double dtau, double dtau_old, double a, double dadtau,
+                           int64_t cap, float *pos, float *vel, int64_t *ids, int64_t *n_out) = 0;
+    virtual void sync() = 0;
+    virtual cudaStream_t stream() = 0;
+};
+
+template <class R> struct Ctx final : CtxBase {
+    using C = typename CT<R>::C;
+    Geom g{};
+    cudaStream_t st = nullptr;
+    DBuf<R> phi, chi, source, Sij, Bi;
+    DBuf<C> W, hij, hijp, bstate;
+    DBuf<C> tw_full, tw_half;
+    DBuf<double> k2;
+    DBuf<double2> ks;
+    DBuf<uint32_t> cellA, cellB, bucket, rank, counts, bstart, bsums;
+    DBuf<double> offA, offB;
+    DBuf<R> qA, qB;
+    DBuf<int64_t> idA, idB;
+    DBuf<double> partial, scal;          // scal: [0] sum, [1] phi_hom
+    DBuf<unsigned long long> u64;        // [0] vmax bits, [1] lc count, [2] prelog count
+    DBuf<int> derr;
+    DBuf<double> bins;
+    DBuf<unsigned long long> occ;
+    DBuf<double> stage;                  // particle / field transfer staging
+    DBuf<int64_t> stage_id;
+    DBuf<float> lc_pos, lc_vel;
+    DBuf<int64_t> lc_id, prelog;
+    DBuf<int64_t> backlog[8];
+    int64_t backlog_n[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    bool cur_is_A = true;
+    int64_t np = 0;
+    double mass = 0.0;
+    bool have_particles = false;
+    static constexpr int64_t CHUNK = 1 << 22;
+
+    explicit Ctx(const gev_config &c)
+    {
+        cfg = c;
+        const int N = c.N;
+        g.N = N;
+        g.P = N / 2 + 1;
+        g.nt = N / 8;
+        g.n3 = (int64_t)N * N * N;
+        g.nk = (int64_t)g.P * N * N;
+        g.ntiles = (int64_t)g.nt * g.nt * g.nt;
+        ck(cudaSetDevice(c.device), "cudaSetDevice");
+        ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+        phi.alloc(g.n3, "phi");
+        chi.alloc(g.n3, "chi");
+        source.alloc(g.n3, "source");
+        Sij.alloc(6 * g.n3, "Sij");
+        Bi.alloc(3 * g.n3, "Bi");
+        W.alloc(6 * g.nk, "Fourier workspace");
+        if (c.tensor) { hij.alloc(6 * g.nk, "hij"); hijp.alloc(6 * g.nk, "hij'"); }
+        if (c.vector_method == GEV_VECTOR_PARABOLIC) bstate.alloc(3 * g.nk, "B state");
+        for (auto *b : {&phi, &chi, &source}) ck(cudaMemsetAsync(b->p, 0, b->n * sizeof(R), st), "memset");
+        ck(cudaMemsetAsync(Sij.p, 0, Sij.n * sizeof(R), st), "memset");
+        ck(cudaMemsetAsync(Bi.p, 0, Bi.n * sizeof(R), st), "memset");
+        if (hij.p) { ck(cudaMemsetAsync(hij.p, 0, hij.n * sizeof(C), st), "memset"); ck(cudaMemsetAsync(hijp.p, 0, hijp.n * sizeof(C), st), "memset"); }
+        if (bstate.p) ck(cudaMemsetAsync(bstate.p, 0, bstate.n * sizeof(C), st), "memset");
+        make_tables();
+        const int64_t cap = c.capacity;
+        cellA.alloc(cap, "particles"); cellB.alloc(cap, "particles");
+        offA.alloc(3 * cap, "particles"); offB.alloc(3 * cap, "particles");
+        qA.alloc(3 * cap, "particles"); qB.alloc(3 * cap, "particles");
+        idA.alloc(cap, "particles"); idB.alloc(cap, "particles");
+        bucket.alloc(cap, "buckets"); rank.alloc(cap, "buckets");
+        const int64_t nb = g.ntiles * 8;
+        counts.alloc(nb, "bucket counts");
+        bstart.alloc(nb + 1, "bucket starts");
+        bsums.alloc((nb + 1023) / 1024 + 1, "scan");
+        ck(cudaMemsetAsync(bstart.p, 0, (nb + 1) * sizeof(uint32_t), st), "memset");
+        partial.alloc((int64_t)N * N, "partials");
+        scal.alloc(4, "scalars");
+        u64.alloc(4, "scalars");
+        derr.alloc(1, "error word");
+        ck(cudaMemsetAsync(derr.p, 0, sizeof(int), st), "memset");
+        ck(cudaStreamSynchronize(st), "init");
+    }
+
+    ~Ctx() override
+    {
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+    }
+
+    cudaStream_t stream() override { return st; }
+
+    void make_tables()
+    {
+        const int N = g.N;
+        std::vector<C> tf(N), th(N / 2);
+        for (int k = 0; k < N; k++) {
+            double ang = -2.0 * M_PI * (double)k / N;
+            tf[k].x = (R)std::cos(ang);
+            tf[k].y = (R)std::sin(ang);
+        }
+        for (int k = 0; k < N / 2; k++) {
+            double ang = -2.0 * M_PI * (double)k / (N / 2);
+            th[k].x = (R)std::cos(ang);
+            th[k].y = (R)std::sin(ang);
+        }
+        // gevolution.hpp:269-275
+        std::vector<double> hk2(N);
+        std::vector<double2> hks(N);
+        for (int i = 0; i < N; i++) {
+            double gk = 2.0 * (double)N * std::sin(M_PI * (double)i / (double)N);
+            hks[i] = make_double2(gk * std::cos(M_PI * (double)i / (double)N), -gk * std::sin(M_PI * (double)i / (double)N));
+            hk2[i] = gk * gk;
+        }
+        tw_full.alloc(N, "twiddles"); tw_half.alloc(N / 2, "twiddles");
+        k2.alloc(N, "k tables"); ks.alloc(N, "k tables");
+        ck(cudaMemcpy(tw_full.p, tf.data(), N * sizeof(C), cudaMemcpyHostToDevice), "tables");
+        ck(cudaMemcpy(tw_half.p, th.data(), (N / 2) * sizeof(C), cudaMemcpyHostToDevice), "tables");
+        ck(cudaMemcpy(k2.p, hk2.data(), N * sizeof(double), cudaMemcpyHostToDevice), "tables");
+        ck(cudaMemcpy(ks.p, hks.data(), N * sizeof(double2), cudaMemcpyHostToDevice), "tables");
+    }
+
+    FftTables<R> tables() const { return FftTables<R>{tw_full.p, tw_half.p, k2.p, ks.p}; }
+
+    PView<R> view(bool A) const
+    {
+        PView<R> v;
+        v.cell = A ? cellA.p : cellB.p;
+        v.off = A ? offA.p : offB.p;
+        v.q = A ? qA.p : qB.p;
+        v.id = A ? idA.p : idB.p;
+        v.cap = cfg.capacity;
+        v.n = np;
+        return v;
+    }
+    PView<R> cur() const { return view(cur_is_A); }
+
+    void launched(const char *what) { ck(cudaGetLastError(), what); }
+
+    void check_device_error()
+    {
+        int e = 0;
+        ck(cudaMemcpyAsync(&e, derr.p, sizeof(int), cudaMemcpyDeviceToHost, st), "error word");
+        ck(cudaStreamSynchronize(st), "synchronize");
+        if (e) {
+            ck(cudaMemsetAsync(derr.p, 0, sizeof(int), st), "memset");
+            char buf[160];
+            snprintf(buf, sizeof buf, "device error word 0x%x (%s%s%s)", e, (e & ERR_NONFINITE) ? "non-finite particle coordinate " : "",
+                     (e & ERR_LC_OVERFLOW) ? "lightcone buffer overflow " : "", (e & ERR_BAD_CELL) ? "cell index out of range" : "");
+            throw DeviceError(buf);
+        }
+    }
+
+    void sync() override
+    {
+        ck(cudaStreamSynchronize(st), "synchronize");
+        check_device_error();
+    }
+
+    void ensure_stage(int64_t doubles, int64_t ids)
+    {
+        if ((int64_t)stage.n < doubles) stage.alloc(doubles, "staging");
+        if ((int64_t)stage_id.n < ids) stage_id.alloc(ids, "staging");
+    }
+
+    // bucket order from the current cell indices
+    void rebin_from_cells()
+    {
+        const int64_t nb = g.ntiles * 8;
+        ck(cudaMemsetAsync(counts.p, 0, nb * sizeof(uint32_t), st), "memset");
+        launch_bin_count<R>(cur(), g.N, counts.p, bucket.p, rank.p, st);
+        launched("bin_count");
+        finish_rebin();
+    }
+
+    void finish_rebin()
+    {
+        const int64_t nb = g.ntiles * 8;
+        launch_scan(counts.p, bstart.p, nb, bsums.p, st);
+        launched("scan");
+        launch_scatter<R>(cur(), view(!cur_is_A), bstart.p, bucket.p, rank.p, st);
+        launched("scatter");
+        cur_is_A = !cur_is_A;
+    }
+
+    void particles_set(const double *pos, const double *q, const int64_t *id, int64_t n, double m) override
+    {
+        if (n < 0 || n > cfg.capacity) throw ArgError("particle count exceeds the context capacity");
+        if (n > 0 && (!pos || !q)) throw ArgError("null particle array");
+        if (n >= (int64_t)UINT32_MAX) throw ArgError("particle count exceeds 2^32 - 1");
+        np = n;
+        mass = m;
+        const int64_t ch = std::min<int64_t>(std::max<int64_t>(n, 1), CHUNK);
+        ensure_stage(6 * ch, ch);
+        PView<R> v = view(true);
+        for (int64_t o = 0; o < n; o += ch) {
+            int64_t c = std::min(ch, n - o);
+            ck(cudaMemcpyAsync(stage.p, pos + 3 * o, 3 * c * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
+            ck(cudaMemcpyAsync(stage.p + 3 * ch, q + 3 * o, 3 * c * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
+            if (id) ck(cudaMemcpyAsync(stage_id.p, id + o, c * sizeof(int64_t), cudaMemcpyHostToDevice, st), "H2D");
+            PView<R> vo = v;
+            vo.cell += o; vo.off += o; vo.q += o; vo.id += o;
+            launch_load_particles<R>(vo, stage.p, stage.p + 3 * ch, id ? stage_id.p : nullptr, c, g.N, derr.p, st);
+            launched("load_particles");
+            if (!id) {
+                // default IDs: the particle's index in the caller's array
+                std::vector<int64_t> ids(c);
+                for (int64_t k = 0; k < c; k++) ids[k] = o + k;
+                ck(cudaMemcpyAsync(vo.id, ids.data(), c * sizeof(int64_t), cudaMemcpyHostToDevice, st), "H2D");
+                ck(cudaStreamSynchronize(st), "synchronize");
+            }
+            ck(cudaStreamSynchronize(st), "synchronize");
+        }
+        cur_is_A = true;
+        rebin_from_cells();
+        have_particles = true;
+        sync();
+    }
+
+    void particles_get(double *pos, double *q, int64_t *id, int64_t cap, int64_t *n_out) override
+    {
+        if (n_out) *n_out = np;
+        if (cap < np) throw CapacityError("host arrays smaller than the particle count");
+        const int64_t ch = std::min<int64_t>(std::max<int64_t>(np, 1), CHUNK);
+        ensure_stage(6 * ch, ch);
+        PView<R> v = cur();
+        for (int64_t o = 0; o < np; o += ch) {
+            int64_t c = std::min(ch, np - o);
+            PView<R> vo = v;
+            vo.cell += o; vo.off += o; vo.q += o; vo.id += o;
+            launch_store_particles<R>(vo, pos ? stage.p : nullptr, q ? stage.p + 3 * ch : nullptr, id ? stage_id.p : nullptr, c, g.N, st);
+            launched("store_particles");
+            if (pos) ck(cudaMemcpyAsync(pos + 3 * o, stage.p, 3 * c * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+            if (q) ck(cudaMemcpyAsync(q + 3 * o, stage.p + 3 * ch, 3 * c * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+            if (id) ck(cudaMemcpyAsync(id + o, stage_id.p, c * sizeof(int64_t), cudaMemcpyDeviceToHost, st), "D2H");
+            ck(cudaStreamSynchronize(st), "synchronize");
+        }
+    }
+
+    int64_t particles_count() const override { return np; }
+
+    // (device pointer, number of planes, complex?) of a field
+    void field_ref(int f, void **p, int *planes, bool *cplx)
+    {
+        *cplx = false;
+        switch (f) {
+        case GEV_FIELD_PHI: *p = phi.p; *planes = 1; break;
+        case GEV_FIELD_CHI: *p = chi.p; *planes = 1; break;
+        case GEV_FIELD_SOURCE: *p = source.p; *planes = 1; break;
+        case GEV_FIELD_SIJ: *p = Sij.p; *planes = 6; break;
+        case GEV_FIELD_BI: *p = Bi.p; *planes = 3; break;
+        case GEV_FIELD_HIJ_FT: *p = hij.p; *planes = 6; *cplx = true; break;
+        case GEV_FIELD_HIJP_FT: *p = hijp.p; *planes = 6; *cplx = true; break;
+        case GEV_FIELD_BI_FT: *p = bstate.p; *planes = 3; *cplx = true; break;
+        default: throw ArgError("unknown field id");
+        }
+        if (!*p) throw StateError("field not allocated in this configuration");
+    }
+
+    void field_get(int f, double *host) override
+    {
+        void *p; int planes; bool cplx;
+        field_ref(f, &p, &planes, &cplx);
+        if (!host) throw ArgError("null host pointer");
+        const int64_t n = cplx ? 2 * g.nk : g.n3;
+        ensure_stage(n, 0);
+        for (int c = 0; c < planes; c++) {
+            const R *src = (const R *)p + (int64_t)c * n;
+            k_convert<R, double><<<cdiv(n, 256), 256, 0, st>>>(src, stage.p, n);
+            launched("convert");
+            ck(cudaMemcpyAsync(host + (int64_t)c * n, stage.p, n * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+            ck(cudaStreamSynchronize(st), "synchronize");
+        }
+    }
+
+    void field_set(int f, const double *host) override
+    {
+        void *p; int planes; bool cplx;
+        field_ref(f, &p, &planes, &cplx);
+        if (!host) throw ArgError("null host pointer");
+        const int64_t n = cplx ? 2 * g.nk : g.n3;
+        ensure_stage(n, 0);
+        for (int c = 0; c < planes; c++) {
+            ck(cudaMemcpyAsync(stage.p, host + (int64_t)c * n, n * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
+            k_convert<double, R><<<cdiv(n, 256), 256, 0, st>>>(stage.p, (R *)p + (int64_t)c * n, n);
+            launched("convert");
+            ck(cudaStreamSynchronize(st), "synchronize");
+        }
+    }
+
+    void need_particles() const
+    {
+        if (!have_particles) throw StateError("no particles loaded");
+    }
+
+    void project(uint32_t which, double a, double coeff, int use_phi, int accumulate) override
+    {
+        need_particles();
+        if (which & ~(GEV_PROJ_T00 | GEV_PROJ_TIJ | GEV_PROJ_T0I | GEV_PROJ_CIC)) throw ArgError("unknown projection");
+        if ((which & GEV_PROJ_CIC) && (which & GEV_PROJ_T00)) throw ArgError("CIC and T00 both target the source field");
+        if (use_phi && a <= 0.0 && (which & (GEV_PROJ_T00 | GEV_PROJ_TIJ))) throw ArgError("scale factor must be positive");
+        const double n3 = (double)g.n3;   // 1/dx^3
+        const PView<R> v = cur();
+        if ((which & GEV_PROJ_T00) || (which & GEV_PROJ_TIJ)) {
+            double m00 = mass * coeff * n3;
+            if (use_phi) m00 /= a;                       // gevolution.hpp:1731, :1750
+            double mij = mass * coeff * n3 / a;          // gevolution.hpp:2584
+            DepOut<R> o{};
+            int kind;
+            if ((which & GEV_PROJ_T00) && (which & GEV_PROJ_TIJ)) {
+                kind = DEP_T00_TIJ;
+                o.p[0] = source.p;
+                for (int c = 0; c < 6; c++) o.p[1 + c] = Sij.p + c * g.n3;
+            } else if (which & GEV_PROJ_T00) {
+                kind = DEP_T00;
+                o.p[0] = source.p;
+            } else {
+                kind = DEP_TIJ;
+                for (int c = 0; c < 6; c++) o.p[c] = Sij.p + c * g.n3;
+            }
+            launch_deposit<R>(kind, use_phi != 0, v, bstart.p, g.N, phi.p, o, a, m00, mij, accumulate, st);
+            launched("deposit T00/Tij");
+        }
+        if (which & GEV_PROJ_CIC) {
+            DepOut<R> o{};
+            o.p[0] = source.p;
+            launch_deposit<R>(DEP_T00, false, v, bstart.p, g.N, phi.p, o, 1.0, mass * coeff * n3, 0.0, accumulate, st);
+            launched("deposit CIC");
+        }
+        if (which & GEV_PROJ_T0I) {
+            DepOut<R> o{};
+            for (int c = 0; c < 3; c++) o.p[c] = Bi.p + c * g.n3;
+            launch_deposit<R>(DEP_T0I, use_phi != 0, v, bstart.p, g.N, phi.p, o, 1.0, mass * coeff * n3, 0.0, accumulate, st);
+            launched("deposit T0i");
+        }
+    }
+
+    void solve_phi(int prepare, double bg, double c, double c2, double c3, double pc, double modif, double *sum,
+                   double *phom) override
+    {
+        const int N = g.N;
+        const FftTables<R> tb = tables();
+        fx_forward<R>(N, prepare ? FX_PREP_T00 : FX_COPY, source.p, g.n3, 1, 0, phi.p, chi.p, bg, c, c2, c3, W.p, g.nk,
+                      partial.p, tb, st);
+        launched("fx forward (phi)");
+        if (prepare) {
+            launch_reduce_sum(partial.p, (int64_t)(N / fx_rows_per_block(N, sizeof(R) == 8)) * N, scal.p, st);
+            launched("reduce");
+        }
+        fy_pass<R>(N, -1, W.p, g.nk, 1, tb, st);
+        launched("fy forward (phi)");
+        FzParams fp{};
+        fp.op = OP_POISSON;
+        fp.p0 = pc / -((double)N * (double)N * (double)N);
+        fp.p1 = modif;
+        fp.phi_hom = scal.p + 1;
+        fz_pass<R>(N, fp, W.p, g.nk, nullptr, nullptr, nullptr, tb, st);
+        launched("fz Poisson");
+        fy_pass<R>(N, 1, W.p, g.nk, 1, tb, st);
+        launched("fy inverse (phi)");
+        fx_inverse<R>(N, W.p, g.nk, phi.p, g.n3, 1, tb, st);
+        launched("fx inverse (phi)");
+        if (sum || phom) {
+            double h[2] = {0.0, 0.0};
+            ck(cudaMemcpyAsync(h, scal.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+            sync();
+            if (sum) *sum = prepare ? h[0] : 0.0;
+            if (phom) *phom = h[1];
+        }
+    }
+
+    void solve_chi(double coeff, int cycle0, double hubble, double dtau, double dtau_old, double a2dtau) override
+    {
+        const int N = g.N;
+        const FftTables<R> tb = tables();
+        fx_forward<R>(N, FX_PREP_TIJ, Sij.p, g.n3, 6, 0, phi.p, chi.p, 0, coeff, 0, 0, W.p, g.nk, nullptr, tb, st);
+        launched("fx forward (Sij)");
+        fy_pass<R>(N, -1, W.p, g.nk, 6, tb, st);
+        launched("fy forward (Sij)");
+        FzParams fp{};
+        fp.op = OP_SCALAR;
+        fp.extra = 0;
+        if (cfg.tensor) fp.extra |= cycle0 ? EXTRA_TENSOR_PROJECT : EXTRA_TENSOR_EVOLVE;
+        const bool parab = cfg.vector_method == GEV_VECTOR_PARABOLIC;
+        if (parab) fp.extra |= EXTRA_VECTOR_EVOLVE;
+        fp.p0 = hubble; fp.p1 = dtau; fp.p2 = dtau_old; fp.p3 = a2dtau;
+        fz_pass<R>(N, fp, W.p, g.nk, hij.p, hijp.p, bstate.p, tb, st);
+        launched("fz scalar projection");
+        const int nout = parab ? 4 : 1;
+        fy_pass<R>(N, 1, W.p, g.nk, nout, tb, st);
+        launched("fy inverse (chi)");
+        fx_inverse<R>(N, W.p, g.nk, chi.p, g.n3, 1, tb, st);
+        launched("fx inverse (chi)");
+        if (parab) {
+            fx_inverse<R>(N, W.p + g.nk, g.nk, Bi.p, g.n3, 3, tb, st);
+            launched("fx inverse (B)");
+        }
+    }
+
+    void solve_B(double coeff, double modif) override
+    {
+        const int N = g.N;
+        const FftTables<R> tb = tables();
+        fx_forward<R>(N, FX_COPY, Bi.p, g.n3, 3, 0, nullptr, nullptr, 0, 0, 0, 0, W.p, g.nk, nullptr, tb, st);
+        launched("fx forward (T0i)");
+        fy_pass<R>(N, -1, W.p, g.nk, 3, tb, st);
+        launched("fy forward (T0i)");
+        FzParams fp{};
+        fp.op = OP_VECTOR;
+        fp.p0 = coeff;
+        fp.p1 = modif;
+        fz_pass<R>(N, fp, W.p, g.nk, nullptr, nullptr, nullptr, tb, st);
+        launched("fz vector projection");
+        fy_pass<R>(N, 1, W.p, g.nk, 3, tb, st);
+        launched("fy inverse (B)");
+        fx_inverse<R>(N, W.p, g.nk, Bi.p, g.n3, 3, tb, st);
+        launched("fx inverse (B)");
+    }
+
+    double kick_drift(const KickDriftParams &kp) override
+    {
+        need_particles();
+        const int64_t nb = g.ntiles * 8;
+        if (kp.do_bin) ck(cudaMemsetAsync(counts.p, 0, nb * sizeof(uint32_t), st), "memset");
+        ck(cudaMemsetAsync(u64.p, 0, sizeof(unsigned long long), st), "memset");
+        launch_kick_drift<R>(cur(), bstart.p, g.N, phi.p, chi.p, Bi.p, g.n3, kp, counts.p, bucket.p, rank.p, u64.p, derr.p, st);
+        launched("kick/drift");
+        if (kp.do_bin) finish_rebin();
+        double maxvel = 0.0;
+        if (kp.do_kick) {
+            unsigned long long bits = 0;
+            ck(cudaMemcpyAsync(&bits, u64.p, sizeof(bits), cudaMemcpyDeviceToHost, st), "D2H");
+            sync();
+            double v2;
+            std::memcpy(&v2, &bits, sizeof v2);
+            maxvel = std::sqrt(v2);
+        }
+        return maxvel;
+    }
+
+    void power_spectrum(int nb, double kmax, double *kb, double *pw, double *ksc, double *ps, int32_t *occo) override
+    {
+        need_particles();
+        if (nb <= 0) throw ArgError("numbins must be positive");
+        const int N = g.N;
+        if (kmax <= 0.0) kmax = std::sqrt(3.0) * M_PI * N;   // tools.hpp:144-145 with KTYPE_LINEAR
+        project(GEV_PROJ_CIC, 1.0, 1.0, 0, 0);
+        const FftTables<R> tb = tables();
+        fx_forward<R>(N, FX_COPY, source.p, g.n3, 1, 0, nullptr, nullptr, 0, 0, 0, 0, W.p, g.nk, nullptr, tb, st);
+        launched("fx forward (CIC)");
+        fy_pass<R>(N, -1, W.p, g.nk, 1, tb, st);
+        launched("fy forward (CIC)");
+        if ((int)occ.n < nb) { bins.alloc(4 * nb, "bins"); occ.alloc(nb, "bins"); }
+        ck(cudaMemsetAsync(bins.p, 0, 4 * nb * sizeof(double), st), "memset");
+        ck(cudaMemsetAsync(occ.p, 0, nb * sizeof(unsigned long long), st), "memset");
+        FzParams fp{};
+        fp.op = OP_BIN;
+        fp.p0 = nb;
+        fp.p1 = kmax;
+        fp.bins = bins.p;
+        fp.occ = occ.p;
+        fz_pass<R>(N, fp, W.p, g.nk, nullptr, nullptr, nullptr, tb, st);
+        launched("fz binning");
+        std::vector<double> acc(4 * nb);
+        std::vector<unsigned long long> oc(nb);
+        ck(cudaMemcpyAsync(acc.data(), bins.p, 4 * nb * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaMemcpyAsync(oc.data(), occ.p, nb * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st), "D2H");
+        sync();
+        // final normalisation, tools.hpp:292-313
+        for (int i = 0; i < nb; i++) {
+            occo[i] = (int32_t)oc[i];
+            if (oc[i] > 0) {
+                double o = (double)oc[i];
+                kb[i] = acc[i];
+                ksc[i] = std::sqrt(acc[nb + i] * o - kb[i] * kb[i]) / o;
+                if (!std::isfinite(ksc[i])) ksc[i] = 0.0;
+                kb[i] /= o;
+                pw[i] = acc[2 * nb + i] / o;
+                ps[i] = std::sqrt(acc[3 * nb + i] / o - pw[i] * pw[i]);
+                if (!std::isfinite(ps[i])) ps[i] = 0.0;
+            } else {
+                kb[i] = pw[i] = ksc[i] = ps[i] = 0.0;
+            }
+        }
+    }
+
+    void lightcone(const gev_lightcone_args &lc, double tau, double dtau, double dtau_old, double a, double dadtau,
+                   int64_t cap, float *pos, float *vel, int64_t *ids, int64_t *n_out) override
+    {
+        need_particles();
+        if (lc.shell < 0 || lc.shell >= 8) throw ArgError("lightcone shell slot must be 0..7");
+        const int s = lc.shell;
+        const double dist = lc.d - tau;
+        *n_out = 0;
+        // output condition, output.hpp:2093
+        if (!(lc.distance[0] > dist + 0.5 * dtau_old && lc.distance[1] <= dist + 0.5 * dtau_old && dist + 0.5 * dtau_old > 0.)) {
+            backlog_n[s] = 0;   // the reference clears the backlog every cycle (output.hpp:2172)
+            return;
+        }
+        LcKernelArgs la{};
+        const int N = g.N;
+        double domain[6];
+        for (int i = 0; i < 3; i++) { domain[i] = -0.5 / N; domain[i + 3] = (N + 0.5) / N; }   // output.hpp:1174-1186
+        la.inner = dist - 0.5 * dtau;
+        la.outer = dist + (0.5 + 0.05) * dtau_old;
+        la.dist = dist;
+        la.nvtx = find_intersecting(lc.vertex, lc.direction, lc.opening, la.outer, la.inner, domain, la.vtx);
+        for (int i = 0; i < 3; i++) { la.lc_vertex[i] = lc.vertex[i]; la.direction[i] = lc.direction[i]; }
+        la.opening = lc.opening;
+        la.dtau = dtau; la.dtau_old = dtau_old; la.a = a; la.dadtau = dadtau; la.boxsize = cfg.boxsize;
+        la.tracer_factor = lc.tracer_factor > 0 ? lc.tracer_factor : 1;
+        la.backlog = backlog[s].p;
+        la.backlog_n = backlog_n[s];
+        const int64_t lcap = std::max<int64_t>(cap, 1);
+        la.capacity = lcap;
+        if ((int64_t)lc_id.n < lcap) { lc_pos.alloc(3 * lcap, "lightcone"); lc_vel.alloc(3 * lcap, "lightcone"); lc_id.alloc(lcap, "lightcone"); }
+        const int64_t pcap = std::max<int64_t>(np / 8, 1024);
+        if ((int64_t)prelog.n < pcap) prelog.alloc(pcap, "lightcone log");
+        ck(cudaMemsetAsync(u64.p + 1, 0, 2 * sizeof(unsigned long long), st), "memset");
+        launch_lightcone<R>(cur(), N, phi.p, la, lc_pos.p, lc_vel.p, lc_id.p, u64.p + 1, prelog.p, u64.p + 2, (int64_t)prelog.n,
+                            derr.p, st);
+        launched("lightcone");
+        unsigned long long cnt[2];
+        ck(cudaMemcpyAsync(cnt, u64.p + 1, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaStreamSynchronize(st), "synchronize");
+        *n_out = (int64_t)cnt[0];
+        if ((int64_t)cnt[0] > cap || (int64_t)cnt[1] > (int64_t)prelog.n) {
+            ck(cudaMemsetAsync(derr.p, 0, sizeof(int), st), "memset");
+            throw CapacityError("lightcone output exceeds the buffer capacity (n_out holds the required size)");
+        }
+        const int64_t n = (int64_t)cnt[0];
+        if (n > 0) {
+            ck(cudaMemcpyAsync(pos, lc_pos.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, st), "D2H");
+            ck(cudaMemcpyAsync(vel, lc_vel.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, st), "D2H");
+            ck(cudaMemcpyAsync(ids, lc_id.p, n * sizeof(int64_t), cudaMemcpyDeviceToHost, st), "D2H");
+        }
+        // the IDs logged near the inner edge become the next cycle's backlog (sorted, unique)
+        std::vector<int64_t> lg((size_t)cnt[1]);
+        if (cnt[1]) ck(cudaMemcpyAsync(lg.data(), prelog.p, cnt[1] * sizeof(int64_t), cudaMemcpyDeviceToHost, st), "D2H");
+        sync();
+        std::sort(lg.begin(), lg.end());
+        lg.erase(std::unique(lg.begin(), lg.end()), lg.end());
+        if ((int64_t)backlog[s].n < (int64_t)lg.size()) backlog[s].alloc(std::max<size_t>(lg.size(), 1024), "backlog");
+        if (!lg.empty()) ck(cudaMemcpyAsync(backlog[s].p, lg.data(), lg.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st), "H2D");
+        backlog_n[s] = (int64_t)lg.size();
+        ck(cudaStreamSynchronize(st), "synchronize");
+    }
+};
+
+}  // namespace gev
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+struct gev_ctx {
+    std::unique_ptr<gev::CtxBase> impl;
+    std::string err;
+};
+
+namespace {
+
+int fail(gev_ctx *ctx, int code, const char *msg)
+{
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+template <class F> int guarded(gev_ctx *ctx, F &&f)
+{
+    if (!ctx || !ctx->impl) return GEV_ERR_ARG;
+    try {
+        f(*ctx->impl);
+        return GEV_OK;
+    } catch (const gev::ArgError &e) {
+        return fail(ctx, GEV_ERR_ARG, e.what());
+    } catch (const gev::StateError &e) {
+        return fail(ctx, GEV_ERR_STATE, e.what());
+    } catch (const gev::DeviceError &e) {
+        return fail(ctx, GEV_ERR_DEVICE, e.what());
+    } catch (const gev::CapacityError &e) {
+        return fail(ctx, GEV_ERR_CAPACITY, e.what());
+    } catch (const gev::NoMemError &e) {
+        return fail(ctx, GEV_ERR_NOMEM, e.what());
+    } catch (const std::exception &e) {
+        return fail(ctx, GEV_ERR_CUDA, e.what());
+    }
+}
+
+bool supported_N(int N)
+{
+    for (int n : {16, 32, 64, 128, 256, 384, 512, 768})
+        if (N == n) return true;
+    return false;
+}
+
+thread_local std::string g_create_error;
+
+}  // namespace
+
+extern "C" {
+
+const char *gev_version(void) { return "gevolution-b200 1.0 (sm_100a)"; }
+
+int gev_ctx_create(const gev_config *cfg, gev_ctx **out)
+{
+    if (!cfg || !out) return GEV_ERR_ARG;
+    *out = nullptr;
+    if (!supported_N(cfg->N) || (cfg->precision != GEV_FP64 && cfg->precision != GEV_MIXED) || cfg->capacity < 0 ||
+        (cfg->vector_method != GEV_VECTOR_ELLIPTIC && cfg->vector_method != GEV_VECTOR_PARABOLIC)) {
+        g_create_error = "invalid configuration (N must be one of 16,32,64,128,256,384,512,768)";
+        return GEV_ERR_ARG;
+    }
+    auto *c = new gev_ctx;
+    try {
+        if (cfg->precision == GEV_FP64) c->impl.reset(new gev::Ctx<double>(*cfg));
+        else c->impl.reset(new gev::Ctx<float>(*cfg));
+    } catch (const gev::NoMemError &e) {
+        g_create_error = e.what();
+        delete c;
+        return GEV_ERR_NOMEM;
+    } catch (const std::exception &e) {
+        g_create_error = e.what();
+        delete c;
+        return GEV_ERR_CUDA;
+    }
+    *out = c;
+    return GEV_OK;
+}
+
+int gev_ctx_destroy(gev_ctx *ctx)
+{
+    delete ctx;
+    return GEV_OK;
+}
+
+const char *gev_last_error(const gev_ctx *ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+
+int gev_particles_set(gev_ctx *ctx, const double *pos, const double *q, const int64_t *id, int64_t n, double mass)
+{
+    return guarded(ctx, [&](gev::CtxBase &c) { c.particles_set(pos, q, id, n, mass); });
+}
+
+int gev_particles_get(gev_ctx *ctx, double *pos, double *q, int64_t *id, int64_t capacity, int64_t *n_out)
+{
+    return guarded(ctx, [&](gev::CtxBase &c) { c.particles_get(pos, q, id, capacity, n_out); });
+}
+
+int gev_particles_count(const gev_ctx *ctx, int64_t *n_out)
+{
+    if (!ctx || !ctx->impl || !n_out) return GEV_ERR_ARG;
+    *n_out = ctx->impl->particles_count();
+    return GEV_OK;
+}
+
+int gev_field_components(int32_t field)
+{
+    switch (field) {
+    case GEV_FIELD_PHI: case GEV_FIELD_CHI: case GEV_FIELD_SOURCE: return 1;
+    case GEV_FIELD_SIJ: case GEV_FIELD_HIJ_FT: case GEV_FIELD_HIJP_FT: return 6;
+    case GEV_FIELD_BI: case GEV_FIELD_BI_FT: return 3;
+    default: return 0;
+    }
+}
+
+int gev_field_get(gev_ctx *ctx, int32_t field, double *host)
+{
+    return guarded(ctx, [&](gev::CtxBase &c) { c.field_get(field, host); });
+}
+
+int gev_field_set(gev_ctx *ctx, int32_t field, const double *host)
+{
+    return guarded(ctx, [&](gev::CtxBase &c) { c.field_set(field, host); });
+}
+
+int gev_project(gev_ctx *ctx, uint32_t which, double a, double coeff, int32_t use_phi, int32_t accumulate)
+{
+    return guarded(ctx, [&](gev::CtxBase &c) { c.project(which, a, coeff, use_phi, accumulate); });
+}
+
+int gev_solve_phi(gev_ctx *ctx, int32_t prepare, double bgmodel, double coeff, double coeff2, double coeff3,
+                  double poisson_coeff, double modif, double *T00sum, double *phi_hom)
+{
+    return guarded(ctx, [&](gev::CtxBase &c) { c.solve_phi(prepare, bgmodel, coeff, coeff2, coeff3, poisson_coeff, modif, T00sum, phi_hom); });
+}
+
+int gev_solve_chi(gev_ctx *ctx, double coeff, int32_t cycle0, double hubble, double dtau, double dtau_old, double a2dtau)
+{
+    return guarded(ctx, [&](gev::CtxBase &c) { c.solve_chi(coeff, cycle0, hubble, dtau, dtau_old, a2dtau); });
+}
+
+int gev_solve_B(gev_ctx *ctx, double coeff, double modif)
+{
+    return guarded(ctx, [&](gev::CtxBase &c) { c.solve_B(coeff, modif); });
+}
+
+int gev_kick(gev_ctx *ctx, double dtau, double a, double bcoeff, int32_t nfield, double *maxvel)
+{
+    return guarded(ctx, [&](gev::CtxBase &c) {
+        gev::KickDriftParams kp{};
+        kp.dtau_k = dtau; kp.a_k = a; kp.b_k = bcoeff; kp.nfield_k = nfield; kp.do_kick = 1;
+        double v = c.kick_drift(kp);
+        if (maxvel) *maxvel = v;
+    });
+}
+
+int gev_drift(gev_ctx *ctx, double dtau, double a, double bcoeff, int32_t nfield)
+{
+    return guarded(ctx, [&](gev::CtxBase &c) {
+        gev::KickDriftParams kp{};
+        kp.dtau_d = dtau; kp.a_d = a; kp.b_d = bcoeff; kp.nfield_d = nfield; kp.do_drift = 1; kp.do_bin = 1;
+        c.kick_drift(kp);
+    });
+}
+
+int gev_kick_drift(gev_ctx *ctx, double dtau_kick, double a_kick, double bcoeff_kick, int32_t nfield_kick,
+                   double dtau_drift, double a_drift, double bcoeff_drift, int32_t nfield_drift, double *maxvel)
+{
+    return guarded(ctx, [&](gev::CtxBase &c) {
+        gev::KickDriftParams kp{};
+        kp.dtau_k = dtau_kick; kp.a_k = a_kick; kp.b_k = bcoeff_kick; kp.nfield_k = nfield_kick;
+        kp.dtau_d = dtau_drift; kp.a_d = a_drift; kp.b_d = bcoeff_drift; kp.nfield_d = nfield_drift;
+        kp.do_kick = 1; kp.do_drift = 1; kp.do_bin = 1;
+        double v = c.kick_drift(kp);
+        if (maxvel) *maxvel = v;
+    });
+}
+
+int gev_power_spectrum(gev_ctx *ctx, int32_t numbins, double kmax, double *kbin, double *power, double *kscatter,
+                       double *pscatter, int32_t *occupation)
+{
+    if (!kbin || !power || !kscatter || !pscatter || !occupation) return fail(ctx, GEV_ERR_ARG, "null output array");
+    return guarded(ctx, [&](gev::CtxBase &c) { c.power_spectrum(numbins, kmax, kbin, power, kscatter, pscatter, occupation); });
+}
+
+int gev_lightcone(gev_ctx *ctx, const gev_lightcone_args *lc, double tau, double dtau, double dtau_old, double a,
+                  double dadtau, int64_t capacity, float *pos, float *vel, int64_t *ids, int64_t *n_out)
+{
+    if (!lc || !n_out || (capacity > 0 && (!pos || !vel || !ids))) return fail(ctx, GEV_ERR_ARG, "null argument");
+    return guarded(ctx, [&](gev::CtxBase &c) { c.lightcone(*lc, tau, dtau, dtau_old, a, dadtau, capacity, pos, vel, ids, n_out); });
+}
+
+double gev_hconf(double a, double fourpiG, const gev_cosmo *cosmo) { return gev::hconf(a, fourpiG, *cosmo); }
+
+void gev_rungekutta4bg(double *a, double fourpiG, const gev_cosmo *cosmo, double dtau) { gev::rk4bg(*a, fourpiG, *cosmo, dtau); }
+
+double gev_particle_horizon(double a, double fourpiG, const gev_cosmo *cosmo) { return gev::particle_horizon(a, fourpiG, *cosmo); }
+
+// One cycle of main.cu:608-1317 (GR, CDM, elliptic or parabolic B), no outputs.
+int gev_step(gev_ctx *ctx, const gev_cosmo *cosmo, gev_state *s)
+{
+    if (!cosmo || !s) return fail(ctx, GEV_ERR_ARG, "null argument");
+    return guarded(ctx, [&](gev::CtxBase &c) {
+        const gev_cosmo &cm = *cosmo;
+        const int N = c.cfg.N;
+        const double dx = 1.0 / N;
+        double a = s->a;
+        // T00 and Tij with the previous phi (main.cu:623, :756)
+        c.project(GEV_PROJ_T00 | GEV_PROJ_TIJ, a, 1.0, 1, 0);
+        // phi (main.cu:719-809)
+        if (s->dtau_old > 0.) {
+            const double H = gev::hconf(a, cm.fourpiG, cm);
+            double sum = 0.0, ph = 0.0;
+            c.solve_phi(1, cm.Omega_m, 3. * H * dx * dx / s->dtau_old, cm.fourpiG * dx * dx / a, 3. * H * H * dx * dx,
+                        1. / (dx * dx), 3. * H / s->dtau_old, &sum, &ph);
+            s->T00hom = sum / ((double)N * N * N);
+            s->phi_hom = ph;
+        }
+        // chi, h_ij (main.cu:820-966)
+        const double H = gev::hconf(a, cm.fourpiG, cm);
+        c.solve_chi(2. * cm.fourpiG * dx * dx / a, s->cycle == 0, H, s->dtau, s->dtau_old, a * a * s->dtau_old);
+        // B elliptic with the new phi (main.cu:836-955)
+        if (c.cfg.vector_method == GEV_VECTOR_ELLIPTIC) {
+            c.project(GEV_PROJ_T0I, a, 1.0, 1, 0);
+            c.solve_B(cm.fourpiG * dx * dx, 0.);
+        }
+        // kick, background half step, drift, background half step (main.cu:1225-1283)
+        gev::KickDriftParams kp{};
+        kp.do_kick = 1; kp.do_drift = 1; kp.do_bin = 1;
+        kp.dtau_k = 0.5 * (s->dtau + s->dtau_old);
+        kp.a_k = a;
+        kp.b_k = a * a * N;
+        kp.nfield_k = (1. / a < cm.z_relax + 1.) ? 3 : 2;
+        gev::rk4bg(a, cm.fourpiG, cm, 0.5 * s->dtau);
+        kp.dtau_d = s->dtau;
+        kp.a_d = a;
+        kp.b_d = a * a * N;
+        kp.nfield_d = (1. / a < cm.z_relax + 1.) ? 3 : 0;
+        double mv = c.kick_drift(kp);
+        gev::rk4bg(a, cm.fourpiG, cm, 0.5 * s->dtau);
+        s->maxvel = mv / std::sqrt(mv * mv + 1.0);
+        // step control (main.cu:1286-1310)
+        s->tau += s->dtau;
+        s->dtau_old = s->dtau;
+        const double H2 = gev::hconf(a, cm.fourpiG, cm);
+        s->dtau = (cm.Cf * dx < cm.steplimit / H2) ? cm.Cf * dx : cm.steplimit / H2;
+        s->a = a;
+        s->cycle++;
+    });
+}
+
+int gev_synchronize(gev_ctx *ctx)
+{
+    return guarded(ctx, [&](gev::CtxBase &c) { c.sync(); });
+}
+
+void *gev_stream(gev_ctx *ctx) { return (ctx && ctx->impl) ? (void *)ctx->impl->stream() : nullptr; }
+
+}  // extern "C"

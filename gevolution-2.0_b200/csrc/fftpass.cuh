@@ -1,0 +1,430 @@
+// fftpass.cuh -- pencil passes of the 3-D real-to-complex transforms with the
+// reference's pointwise physics fused into their load and solve stages.
+//
+// Fourier layout: kx + P*(ky + N*kz), P = N/2 + 1 (half spectrum along x).
+//   fx_fwd : R2C along x for T rows (y0..y0+T-1, z); fused prepareFTsource
+//   fy     : complex FFT along y for T kx-columns at one z (in place)
+//   fz     : FFT along z, pointwise Fourier-space solver, inverse FFT along z,
+//            for T kx-columns at one y and all components of the solve
+//   fx_inv : C2R along x for T rows
+#pragma once
+
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace gev {
+
+// ---------------------------------------------------------------------------
+// fused source preparation (PHINONLINEAR), evaluated in FP64
+// ---------------------------------------------------------------------------
+// FX_COPY, FX_PREP_T00, FX_PREP_TIJ: common.cuh
+
+template <class R> struct FxArgs {
+    const R *in;          // field (component plane) to transform
+    const R *phi;
+    const R *chi;
+    double bg, c, c2, c3; // prepareFTsource_T00 params (bgmodel, coeff, coeff2, coeff3) / Tij coeff in c
+    int comp0;            // first Tij component of the batch (gridDim.z = number of components)
+    typename CT<R>::C *out;
+    double *partial;      // per-block partial sums of the source (FX_PREP_T00)
+};
+
+template <class R>
+__device__ __forceinline__ double ld(const R *f, int N, int x, int y, int z)
+{
+    return (double)f[sidx(N, wrapi(x, N), wrapi(y, N), wrapi(z, N))];
+}
+
+// prepareFTsource_T00: gevolution.hpp:160-171
+template <class R>
+__device__ __forceinline__ double prep_t00(const FxArgs<R> &a, int N, int x, int y, int z, double &src)
+{
+    int64_t i = sidx(N, x, y, z);
+    double s = (double)a.in[i];
+    double ph = (double)a.phi[i];
+    src = s;
+    double r = a.c2 * (s - a.bg);
+    r *= 1.0 - 2.0 * ph * (1.0 - ph);
+    double g;
+    g = ld(a.phi, N, x - 1, y, z) - ld(a.phi, N, x + 1, y, z); r += 0.125 * g * g;
+    g = ld(a.phi, N, x, y - 1, z) - ld(a.phi, N, x, y + 1, z); r += 0.125 * g * g;
+    g = ld(a.phi, N, x, y, z - 1) - ld(a.phi, N, x, y, z + 1); r += 0.125 * g * g;
+    r += (a.c3 * (1.0 - 3.0 * ph) - a.c) * ph - a.c3 * (double)a.chi[i];
+    return r;
+}
+
+// prepareFTsource_Tij for one symmetric component c (00,01,02,11,12,22): gevolution.hpp:64-107
+template <class R>
+__device__ __forceinline__ double prep_tij(const R *T, const R *phi, double coeff, int c, int N, int x, int y, int z)
+{
+    int64_t i = sidx(N, x, y, z);
+    double t = (double)T[i];
+    const int ai = (c == 0 || c == 1 || c == 2) ? 0 : (c == 5 ? 2 : 1);
+    const int aj = (c == 0) ? 0 : (c == 1 ? 1 : ((c == 2 || c == 4 || c == 5) ? 2 : 1));
+    int ei[3] = {ai == 0, ai == 1, ai == 2}, ej[3] = {aj == 0, aj == 1, aj == 2};
+    if (ai == aj) {
+        double g = ld(phi, N, x + ei[0], y + ei[1], z + ei[2]) - ld(phi, N, x - ei[0], y - ei[1], z - ei[2]);
+        return 0.5 * g * g + coeff * t;
+    }
+    double p0 = (double)phi[i];
+    double pi_ = ld(phi, N, x + ei[0], y + ei[1], z + ei[2]);
+    double pj = ld(phi, N, x + ej[0], y + ej[1], z + ej[2]);
+    double pij = ld(phi, N, x + ei[0] + ej[0], y + ei[1] + ej[1], z + ei[2] + ej[2]);
+    return pi_ * pj - p0 * pij + 0.5 * (p0 * p0 - pi_ * pi_ - pj * pj + pij * pij) + coeff * t;
+}
+
+// ---------------------------------------------------------------------------
+// x pass, forward: real rows -> half spectrum.  grid (N/T, N, ncomp)
+// ---------------------------------------------------------------------------
+template <class R, int N, int T, int NT, int MODE>
+__global__ void __launch_bounds__(NT) k_fx_fwd(FxArgs<R> a, int64_t in_stride, int64_t out_stride,
+                                               const typename CT<R>::C *__restrict__ tw_half,
+                                               const typename CT<R>::C *__restrict__ tw_full)
+{
+    using C = typename CT<R>::C;
+    constexpr int M = N / 2, P = N / 2 + 1, LD = T + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *buf = reinterpret_cast<C *>(smem_raw);
+    __shared__ double red[NT / 32];
+
+    const int y0 = blockIdx.x * T, z = blockIdx.y, comp = blockIdx.z;
+    const R *in = a.in + (int64_t)comp * in_stride;
+    C *out = a.out + (int64_t)comp * out_stride;
+    double lsum = 0.0;
+
+    for (int idx = threadIdx.x; idx < M * T; idx += NT) {
+        int n = idx % M, t = idx / M, y = y0 + t;
+        R v0, v1;
+        if constexpr (MODE == FX_COPY) {
+            const R *row = in + sidx(N, 0, y, z);
+            v0 = row[2 * n];
+            v1 = row[2 * n + 1];
+        } else if constexpr (MODE == FX_PREP_T00) {
+            double s0, s1;
+            v0 = (R)prep_t00(a, N, 2 * n, y, z, s0);
+            v1 = (R)prep_t00(a, N, 2 * n + 1, y, z, s1);
+            lsum += s0 + s1;
+        } else {
+            v0 = (R)prep_tij(in, a.phi, a.c, a.comp0 + comp, N, 2 * n, y, z);
+            v1 = (R)prep_tij(in, a.phi, a.c, a.comp0 + comp, N, 2 * n + 1, y, z);
+        }
+        buf[n * LD + t] = mk(v0, v1);
+    }
+    __syncthreads();
+    fft_lines<M, -1, T, NT>(buf, LD, tw_half);
+
+    for (int idx = threadIdx.x; idx < P * T; idx += NT) {
+        int k = idx % P, t = idx / P, y = y0 + t;
+        C zk = buf[(k == M ? 0 : k) * LD + t];
+        C zm = buf[(k == 0 ? 0 : M - k) * LD + t];
+        zm.y = -zm.y;                                  // conj(Z[M-k])
+        C ze = cscale(cadd(zk, zm), R(0.5));
+        C d = csub(zk, zm);
+        C zo = mk(R(0.5) * d.y, R(-0.5) * d.x);        // (zk - conj(zm)) / (2i)
+        C w = __ldg(tw_full + k);
+        out[k + (int64_t)P * (y + (int64_t)N * z)] = cadd(ze, cmul(w, zo));
+    }
+
+    if constexpr (MODE == FX_PREP_T00) {
+        for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = lsum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = 0.0;
+            for (int w = 0; w < NT / 32; w++) s += red[w];
+            a.partial[blockIdx.x + gridDim.x * blockIdx.y] = s;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// y pass (in place), complex.  grid (ceil(P/T), N, ncomp)
+// ---------------------------------------------------------------------------
+template <class R, int N, int T, int NT, int S>
+__global__ void __launch_bounds__(NT) k_fy(typename CT<R>::C *data, int64_t stride,
+                                           const typename CT<R>::C *__restrict__ tw)
+{
+    using C = typename CT<R>::C;
+    constexpr int P = N / 2 + 1, LD = T + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *buf = reinterpret_cast<C *>(smem_raw);
+    const int kx0 = blockIdx.x * T, z = blockIdx.y;
+    C *d = data + (int64_t)blockIdx.z * stride;
+    for (int idx = threadIdx.x; idx < N * T; idx += NT) {
+        int t = idx % T, n = idx / T, kx = kx0 + t;
+        buf[n * LD + t] = (kx < P) ? d[kx + (int64_t)P * (n + (int64_t)N * z)] : mk(R(0), R(0));
+    }
+    __syncthreads();
+    fft_lines<N, S, T, NT>(buf, LD, tw);
+    for (int idx = threadIdx.x; idx < N * T; idx += NT) {
+        int t = idx % T, n = idx / T, kx = kx0 + t;
+        if (kx < P) d[kx + (int64_t)P * (n + (int64_t)N * z)] = buf[n * LD + t];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// x pass, inverse: half spectrum -> real rows (imaginary parts of the kx = 0
+// and kx = N/2 entries do not contribute).  grid (N/T, N, ncomp)
+// ---------------------------------------------------------------------------
+template <class R, int N, int T, int NT>
+__global__ void __launch_bounds__(NT) k_fx_inv(const typename CT<R>::C *in, int64_t in_stride, R *out,
+                                               int64_t out_stride,
+                                               const typename CT<R>::C *__restrict__ tw_half,
+                                               const typename CT<R>::C *__restrict__ tw_full)
+{
+    using C = typename CT<R>::C;
+    constexpr int M = N / 2, P = N / 2 + 1, LD = T + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *buf = reinterpret_cast<C *>(smem_raw);
+    const int y0 = blockIdx.x * T, z = blockIdx.y;
+    const C *src = in + (int64_t)blockIdx.z * in_stride;
+    R *dst = out + (int64_t)blockIdx.z * out_stride;
+    for (int idx = threadIdx.x; idx < M * T; idx += NT) {
+        int k = idx % M, t = idx / M, y = y0 + t;
+        const C *row = src + (int64_t)P * (y + (int64_t)N * z);
+        C A = row[k], B = row[M - k];
+        if (k == 0) { A.y = R(0); B.y = R(0); }
+        B.y = -B.y;
+        C w = __ldg(tw_full + k);
+        w.y = -w.y;                                    // exp(+2 pi i k / N)
+        C dd = cmul(csub(A, B), w);
+        C s = cadd(A, B);
+        buf[k * LD + t] = mk(s.x - dd.y, s.y + dd.x);  // (A+B) + i (A-B) w
+    }
+    __syncthreads();
+    fft_lines<M, 1, T, NT>(buf, LD, tw_half);
+    for (int idx = threadIdx.x; idx < M * T; idx += NT) {
+        int n = idx % M, t = idx / M, y = y0 + t;
+        C v = buf[n * LD + t];
+        R *row = dst + sidx(N, 0, y, z);
+        row[2 * n] = v.x;
+        row[2 * n + 1] = v.y;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// z pass with the Fourier-space solvers (gevolution.hpp:251-852).  All solver
+// arithmetic is FP64; k tables hold gridk2[i] = (2N sin(pi i/N))^2 and
+// kshift[i] = 2N sin(pi i/N) exp(-i pi i/N) (gevolution.hpp:269-275).
+// ---------------------------------------------------------------------------
+// OP_POISSON, OP_SCALAR, OP_VECTOR, OP_BIN and the EXTRA_* flags: common.cuh
+// optional extras of OP_SCALAR
+
+template <class R> struct FzArgs {
+    typename CT<R>::C *data;   // component planes (stride nk)
+    int64_t stride;
+    const double *k2;          // gridk2[N]
+    const double2 *ks;         // kshift[N]
+    double p0, p1, p2, p3;     // op parameters
+    int extra;
+    typename CT<R>::C *hij;    // tensor state (6 planes) / B state (3 planes)
+    typename CT<R>::C *hijp;
+    typename CT<R>::C *bstate;
+    double *phi_hom;           // k = 0 mode after the Poisson solve
+    double *bins;              // OP_BIN: 4*numbins accumulators (k, k^2, P, P^2)
+    unsigned long long *occ;   // OP_BIN: mode counts
+};
+
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ double2 zadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 zsub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 zsc(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ double2 zcj(double2 a) { return make_double2(a.x, -a.y); }
+template <class C> __device__ __forceinline__ double2 z2d(C a) { return make_double2((double)a.x, (double)a.y); }
+
+// transverse-traceless numerators of projectFTtensor (gevolution.hpp:744-769)
+__device__ __forceinline__ void tt_num(const double *g, const double2 *k, double k2, const double2 *S, double2 *o)
+{
+    double2 Sxx = S[0], Sxy = S[1], Sxz = S[2], Syy = S[3], Syz = S[4], Szz = S[5];
+    o[0] = zadd(zadd(zsc(zadd(zsc(Sxx, g[0] - k2), zsc(zmul(k[0], zadd(zmul(k[1], Sxy), zmul(k[2], Sxz))), 2.0)), g[0] - k2),
+                     zsc(Syy, (g[0] + k2) * (g[1] + k2) - 2.0 * k2 * k2)),
+                zadd(zsc(Szz, (g[0] + k2) * (g[2] + k2) - 2.0 * k2 * k2), zsc(zmul(zmul(k[1], k[2]), Syz), 2.0 * (g[0] + k2))));
+    o[1] = zadd(zadd(zsc(Sxy, 2.0 * (g[0] - k2) * (g[1] - k2)), zsc(zmul(zmul(zcj(k[0]), zcj(k[1])), Szz), g[2] + k2)),
+                zadd(zsc(zmul(zcj(k[1]), zadd(zmul(zcj(k[0]), Sxx), zsc(zmul(k[2], Sxz), 2.0))), g[0] - k2),
+                     zsc(zmul(zcj(k[0]), zadd(zmul(zcj(k[1]), Syy), zsc(zmul(k[2], Syz), 2.0))), g[1] - k2)));
+    o[2] = zadd(zadd(zsc(Sxz, 2.0 * (g[0] - k2) * (g[2] - k2)), zsc(zmul(zmul(zcj(k[0]), zcj(k[2])), Syy), g[1] + k2)),
+                zadd(zsc(zmul(zcj(k[2]), zadd(zmul(zcj(k[0]), Sxx), zsc(zmul(k[1], Sxy), 2.0))), g[0] - k2),
+                     zsc(zmul(zcj(k[0]), zadd(zmul(zcj(k[2]), Szz), zsc(zmul(k[1], Syz), 2.0))), g[2] - k2)));
+    o[3] = zadd(zadd(zsc(zadd(zsc(Syy, g[1] - k2), zsc(zmul(k[1], zadd(zmul(k[0], Sxy), zmul(k[2], Syz))), 2.0)), g[1] - k2),
+                     zsc(Sxx, (g[1] + k2) * (g[0] + k2) - 2.0 * k2 * k2)),
+                zadd(zsc(Szz, (g[1] + k2) * (g[2] + k2) - 2.0 * k2 * k2), zsc(zmul(zmul(k[0], k[2]), Sxz), 2.0 * (g[1] + k2))));
+    o[4] = zadd(zadd(zsc(Syz, 2.0 * (g[1] - k2) * (g[2] - k2)), zsc(zmul(zmul(zcj(k[1]), zcj(k[2])), Sxx), g[0] + k2)),
+                zadd(zsc(zmul(zcj(k[2]), zadd(zmul(zcj(k[1]), Syy), zsc(zmul(k[0], Sxy), 2.0))), g[1] - k2),
+                     zsc(zmul(zcj(k[1]), zadd(zmul(zcj(k[2]), Szz), zsc(zmul(k[0], Sxz), 2.0))), g[2] - k2)));
+    o[5] = zadd(zadd(zsc(zadd(zsc(Szz, g[2] - k2), zsc(zmul(k[2], zadd(zmul(k[0], Sxz), zmul(k[1], Syz))), 2.0)), g[2] - k2),
+                     zsc(Sxx, (g[2] + k2) * (g[0] + k2) - 2.0 * k2 * k2)),
+                zadd(zsc(Syy, (g[2] + k2) * (g[1] + k2) - 2.0 * k2 * k2), zsc(zmul(zmul(k[0], k[1]), Sxy), 2.0 * (g[2] + k2))));
+}
+
+template <int OP, int EXTRA> struct OpShape {
+    static constexpr int CIN = (OP == OP_POISSON || OP == OP_BIN) ? 1 : (OP == OP_SCALAR ? 6 : 3);
+    static constexpr int COUT = (OP == OP_BIN) ? 0 : ((OP == OP_POISSON) ? 1 : (OP == OP_SCALAR ? ((EXTRA & EXTRA_VECTOR_EVOLVE) ? 4 : 1) : 3));
+};
+
+// Element-wise solver for one (kx, ky, kz): reads CIN values from v, writes
+// COUT values back into v[0..COUT-1].
+template <class R, int OP, int EXTRA>
+__device__ __forceinline__ void fz_apply(const FzArgs<R> &a, int N, int kx, int ky, int kz, int64_t kidx, double2 *v)
+{
+    using C = typename CT<R>::C;
+    const double g[3] = {__ldg(a.k2 + kx), __ldg(a.k2 + ky), __ldg(a.k2 + kz)};
+    const double2 k[3] = {__ldg(a.ks + kx), __ldg(a.ks + ky), __ldg(a.ks + kz)};
+    const double k2 = g[0] + g[1] + g[2];
+    if constexpr (OP == OP_BIN) {
+        // extractCrossSpectrum binning, KTYPE_LINEAR with CIC deconvolution
+        // (tools.hpp:105-215); p0 = numbins, p1 = kmax
+        if (kx == 0 && ky == 0 && kz == 0) return;
+        const int weight = (kx == 0 || (kx == N / 2 && (N % 2) == 0)) ? 1 : 2;
+        auto lin = [&](int i) { double t = 2.0 * 3.14159265358979323846 * (double)(i <= N / 2 ? i : N - i); return t * t; };
+        auto snc = [&](int i) {
+            int j = i <= N / 2 ? i : N - i;
+            if (j == 0) return 1.0;
+            return sin(3.14159265358979323846 * (double)(float)j / (double)(float)N) * (double)(float)N / (3.14159265358979323846 * (double)(float)j);
+        };
+        double kk2 = lin(kx) + lin(ky) + lin(kz);
+        double s = snc(kx) * snc(ky) * snc(kz);
+        s *= s;
+        double pw = v[0].x * v[0].x + v[0].y * v[0].y;
+        double sk = sqrt(kk2);
+        int nb = (int)a.p0;
+        int bin = (int)floor((double)nb * sk / a.p1);
+        if (bin < nb) {
+            atomicAdd(a.bins + bin, weight * sk);
+            atomicAdd(a.bins + nb + bin, weight * kk2);
+            atomicAdd(a.bins + 2 * nb + bin, weight * pw * kk2 * sk / s);
+            atomicAdd(a.bins + 3 * nb + bin, weight * pw * pw * kk2 * kk2 * kk2 / s / s);
+            atomicAdd(a.occ + bin, (unsigned long long)weight);
+        }
+    } else if constexpr (OP == OP_POISSON) {
+        // solveModifiedPoissonFT: gevolution.hpp:806-852; p0 = coeff / (-N^3), p1 = modif
+        double den = k2 + a.p1;
+        v[0] = (den != 0.0) ? zsc(v[0], a.p0 / den) : make_double2(0.0, 0.0);
+        if (kx == 0 && ky == 0 && kz == 0) {
+            if (a.p1 == 0.0) v[0] = make_double2(0.0, 0.0);
+            if (a.phi_hom) *a.phi_hom = v[0].x;
+        }
+    } else if constexpr (OP == OP_VECTOR) {
+        // projectFTvector: gevolution.hpp:449-515; p0 = coeff, p1 = modif
+        if (k2 > 0.0) {
+            double2 tmp = zsc(zadd(zadd(zmul(k[0], v[0]), zmul(k[1], v[1])), zmul(k[2], v[2])), 1.0 / k2);
+            double f = 4.0 * a.p0 / (k2 + a.p1);
+            for (int c = 0; c < 3; c++) v[c] = zsc(zsub(v[c], zmul(zcj(k[c]), tmp)), f);
+        } else {
+            v[0] = v[1] = v[2] = make_double2(0.0, 0.0);
+        }
+    } else {
+        // projectFTscalar: gevolution.hpp:251-340 (add = 0)
+        double2 S[6] = {v[0], v[1], v[2], v[3], v[4], v[5]};
+        double2 chi = make_double2(0.0, 0.0);
+        if (k2 > 0.0) {
+            chi = zadd(zadd(zsc(S[0], g[1] + g[2] - 2.0 * g[0]), zsc(S[3], g[0] + g[2] - 2.0 * g[1])), zsc(S[5], g[0] + g[1] - 2.0 * g[2]));
+            chi = zsub(chi, zsc(zmul(zmul(k[0], k[1]), S[1]), 6.0));
+            chi = zsub(chi, zsc(zmul(zmul(k[0], k[2]), S[2]), 6.0));
+            chi = zsub(chi, zsc(zmul(zmul(k[1], k[2]), S[4]), 6.0));
+            chi = zsc(chi, 1.0 / (2.0 * k2 * k2 * N));
+        }
+        if constexpr ((EXTRA & EXTRA_TENSOR_PROJECT) != 0) {
+            // projectFTtensor: gevolution.hpp:693-787
+            double2 o[6];
+            if (k2 > 0.0) {
+                tt_num(g, k, k2, S, o);
+                double k6 = k2 * k2 * k2 * N;
+                for (int c = 0; c < 6; c++) a.hij[c * a.stride + kidx] = mk(R(o[c].x / k6), R(o[c].y / k6));
+            } else {
+                for (int c = 0; c < 6; c++) a.hij[c * a.stride + kidx] = mk(R(0), R(0));
+            }
+        }
+        if constexpr ((EXTRA & EXTRA_TENSOR_EVOLVE) != 0) {
+            // evolveFTtensor: gevolution.hpp:537-674; p0 = hubble, p1 = dtau, p2 = dtau_old
+            const double dm = 0.5 * (a.p2 + a.p1), opd = 1.0 + a.p0 * dm, omd = 1.0 - a.p0 * dm;
+            const double k4 = k2 * k2 * N;
+            double2 h[6], hp[6], o[6];
+            for (int c = 0; c < 6; c++) { h[c] = z2d(a.hij[c * a.stride + kidx]); hp[c] = z2d(a.hijp[c * a.stride + kidx]); }
+            if (k2 * dm * dm < 1.0) {
+                for (int c = 0; c < 6; c++) h[c] = zadd(h[c], zsc(hp[c], a.p2));
+                if (k2 > 0.0) {
+                    tt_num(g, k, k2, S, o);
+                    for (int c = 0; c < 6; c++) hp[c] = zsc(zadd(zsc(hp[c], omd), zsc(zsub(zsc(o[c], 1.0 / k4), zsc(h[c], k2)), dm)), 1.0 / opd);
+                } else {
+                    double2 tr = zadd(zadd(S[0], S[3]), S[5]);
+                    double2 Sm[6] = {zsub(S[0], zsc(tr, 1.0 / 3.0)), S[1], S[2], zsub(S[3], zsc(tr, 1.0 / 3.0)), S[4], zsub(S[5], zsc(tr, 1.0 / 3.0))};
+                    for (int c = 0; c < 6; c++) hp[c] = zsc(zadd(zsc(hp[c], omd), zsc(Sm[c], 2.0 * dm / N)), 1.0 / opd);
+                }
+            } else {
+                tt_num(g, k, k2, S, o);
+                for (int c = 0; c < 6; c++) {
+                    hp[c] = make_double2(0.0, 0.0);
+                    h[c] = zsc(zadd(zsc(o[c], a.p2 / k4), zsc(h[c], 2.0 * a.p0)), 1.0 / (k2 * a.p2 + 2.0 * a.p0));
+                }
+            }
+            for (int c = 0; c < 6; c++) {
+                a.hij[c * a.stride + kidx] = mk(R(h[c].x), R(h[c].y));
+                a.hijp[c * a.stride + kidx] = mk(R(hp[c].x), R(hp[c].y));
+            }
+        }
+        if constexpr ((EXTRA & EXTRA_VECTOR_EVOLVE) != 0) {
+            // evolveFTvector: gevolution.hpp:359-429; p3 = a^2 dtau
+            double2 B[3];
+            for (int c = 0; c < 3; c++) B[c] = z2d(a.bstate[c * a.stride + kidx]);
+            double k4 = k2 * k2;
+            if (k4 > 0.0) {
+                double2 fac = make_double2(0.0, -2.0 * a.p3 / k4);
+                B[0] = zadd(B[0], zmul(fac, zadd(zmul(zcj(k[0]), zsub(zsub(zsub(zsc(S[0], g[1] + g[2]), zsc(S[3], g[1])), zsc(S[5], g[2])), zsc(zmul(zmul(k[1], k[2]), S[4]), 2.0))),
+                                                 zsc(zadd(zmul(k[1], S[1]), zmul(k[2], S[2])), g[1] + g[2] - g[0]))));
+                B[1] = zadd(B[1], zmul(fac, zadd(zmul(zcj(k[1]), zsub(zsub(zsub(zsc(S[3], g[0] + g[2]), zsc(S[0], g[0])), zsc(S[5], g[2])), zsc(zmul(zmul(k[0], k[2]), S[2]), 2.0))),
+                                                 zsc(zadd(zmul(k[0], S[1]), zmul(k[2], S[4])), g[0] + g[2] - g[1]))));
+                B[2] = zadd(B[2], zmul(fac, zadd(zmul(zcj(k[2]), zsub(zsub(zsub(zsc(S[5], g[0] + g[1]), zsc(S[0], g[0])), zsc(S[3], g[1])), zsc(zmul(zmul(k[0], k[1]), S[1]), 2.0))),
+                                                 zsc(zadd(zmul(k[0], S[2]), zmul(k[1], S[4])), g[0] + g[1] - g[2]))));
+            } else {
+                B[0] = B[1] = B[2] = make_double2(0.0, 0.0);
+            }
+            for (int c = 0; c < 3; c++) {
+                a.bstate[c * a.stride + kidx] = mk(R(B[c].x), R(B[c].y));
+                v[1 + c] = B[c];
+            }
+        }
+        v[0] = chi;
+    }
+}
+
+// grid (ceil(P/T), N); T kx-columns at one ky, all CIN components of the solve.
+template <class R, int N, int T, int NT, int OP, int EXTRA>
+__global__ void __launch_bounds__(NT) k_fz(FzArgs<R> a, const typename CT<R>::C *__restrict__ tw)
+{
+    using C = typename CT<R>::C;
+    constexpr int P = N / 2 + 1;
+    constexpr int CIN = OpShape<OP, EXTRA>::CIN, COUT = OpShape<OP, EXTRA>::COUT;
+    constexpr int LD = CIN * T + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *buf = reinterpret_cast<C *>(smem_raw);
+    const int kx0 = blockIdx.x * T, ky = blockIdx.y;
+
+    for (int idx = threadIdx.x; idx < N * CIN * T; idx += NT) {
+        int t = idx % T, r = idx / T, c = r % CIN, n = r / CIN, kx = kx0 + t;
+        buf[n * LD + c * T + t] = (kx < P) ? a.data[c * a.stride + kx + (int64_t)P * (ky + (int64_t)N * n)] : mk(R(0), R(0));
+    }
+    __syncthreads();
+    fft_lines<N, -1, CIN * T, NT>(buf, LD, tw);
+
+    for (int idx = threadIdx.x; idx < N * T; idx += NT) {
+        int t = idx % T, n = idx / T, kx = kx0 + t;
+        if (kx >= P) continue;
+        double2 v[6];
+#pragma unroll
+        for (int c = 0; c < CIN; c++) v[c] = z2d(buf[n * LD + c * T + t]);
+        int64_t kidx = kx + (int64_t)P * (ky + (int64_t)N * n);
+        fz_apply<R, OP, EXTRA>(a, N, kx, ky, n, kidx, v);
+#pragma unroll
+        for (int c = 0; c < COUT; c++) buf[n * LD + c * T + t] = mk(R(v[c].x), R(v[c].y));
+    }
+    if constexpr (COUT > 0) {
+        __syncthreads();
+        fft_lines<N, 1, COUT * T, NT>(buf, LD, tw);
+        for (int idx = threadIdx.x; idx < N * COUT * T; idx += NT) {
+            int t = idx % T, r = idx / T, c = r % COUT, n = r / COUT, kx = kx0 + t;
+            if (kx < P) a.data[c * a.stride + kx + (int64_t)P * (ky + (int64_t)N * n)] = buf[n * LD + c * T + t];
+        }
+    }
+}
+
+}  // namespace gev

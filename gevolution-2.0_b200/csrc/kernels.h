@@ -1,0 +1,100 @@
+// kernels.h -- host-side launchers of the sm_100a kernels (one translation
+// unit per family: deposit.cu, particles_k.cu, solve.cu, lightcone.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+#include "particles.cuh"
+
+namespace gev {
+
+enum { DEP_T00 = 0, DEP_TIJ = 1, DEP_T00_TIJ = 2, DEP_T0I = 3 };
+
+template <class R> struct DepOut { R *p[7]; };
+
+template <class R>
+void launch_deposit(int kind, bool use_phi, const PView<R> &p, const uint32_t *bstart, int N, const R *phi,
+                    const DepOut<R> &out, double a, double m00, double mij, int accumulate, cudaStream_t st);
+
+// ---- particles ----
+struct KickDriftParams {
+    double dtau_k, a_k, b_k;  // kick: dtau, a, a^2 N
+    int nfield_k;
+    double dtau_d, a_d, b_d;  // drift
+    int nfield_d;
+    int do_kick, do_drift, do_bin;
+};
+
+template <class R>
+void launch_kick_drift(const PView<R> &p, const uint32_t *bstart, int N, const R *phi, const R *chi, const R *Bi,
+                       int64_t n3, const KickDriftParams &kp, uint32_t *counts, uint32_t *bucket, uint32_t *rank,
+                       unsigned long long *vmax_bits, int *err, cudaStream_t st);
+
+template <class R>
+void launch_load_particles(PView<R> p, const double *pos, const double *q, const int64_t *id, int64_t n, int N,
+                           int *err, cudaStream_t st);
+template <class R>
+void launch_store_particles(const PView<R> &p, double *pos, double *q, int64_t *id, int64_t n, int N,
+                            cudaStream_t st);
+template <class R>
+void launch_bin_count(const PView<R> &p, int N, uint32_t *counts, uint32_t *bucket, uint32_t *rank, cudaStream_t st);
+void launch_scan(const uint32_t *counts, uint32_t *start, int64_t nb, uint32_t *block_sums, cudaStream_t st);
+template <class R>
+void launch_scatter(const PView<R> &src, PView<R> dst, const uint32_t *bstart, const uint32_t *bucket,
+                    const uint32_t *rank, cudaStream_t st);
+
+void launch_reduce_sum(const double *partial, int64_t n, double *out, cudaStream_t st);
+
+// ---- Fourier passes ----
+template <class R> struct FftTables {
+    const typename CT<R>::C *tw_full;   // exp(-2 pi i k / N), k < N
+    const typename CT<R>::C *tw_half;   // exp(-2 pi i k / (N/2)), k < N/2
+    const double *k2;                   // gridk2
+    const double2 *ks;                  // kshift
+};
+
+template <class R>
+void fx_forward(int N, int mode, const R *in, int64_t in_stride, int ncomp, int comp0, const R *phi, const R *chi,
+                double bg, double c, double c2, double c3, typename CT<R>::C *out, int64_t out_stride,
+                double *partial, const FftTables<R> &tb, cudaStream_t st);
+template <class R>
+void fy_pass(int N, int sign, typename CT<R>::C *data, int64_t stride, int ncomp, const FftTables<R> &tb,
+             cudaStream_t st);
+template <class R>
+void fx_inverse(int N, const typename CT<R>::C *in, int64_t in_stride, R *out, int64_t out_stride, int ncomp,
+                const FftTables<R> &tb, cudaStream_t st);
+
+struct FzParams {
+    int op, extra;
+    double p0, p1, p2, p3;
+    double *phi_hom;
+    double *bins;
+    unsigned long long *occ;
+};
+template <class R>
+void fz_pass(int N, const FzParams &fp, typename CT<R>::C *data, int64_t stride, typename CT<R>::C *hij,
+             typename CT<R>::C *hijp, typename CT<R>::C *bstate, const FftTables<R> &tb, cudaStream_t st);
+int fx_rows_per_block(int N, bool fp64);   // T of the x passes (partial-sum count = N*N/T)
+
+// ---- lightcone ----
+struct LcKernelArgs {
+    double vtx[64][3];      // periodic images of the vertex that can intersect the shell
+    double lc_vertex[3];    // the lightcone's own vertex (output positions are relative to it)
+    int nvtx;
+    double direction[3];
+    double opening;
+    double inner, outer, dist;
+    double dtau, dtau_old, a, dadtau, boxsize;
+    int tracer_factor;
+    const int64_t *backlog;
+    int64_t backlog_n;
+    int64_t capacity;
+};
+template <class R>
+void launch_lightcone(const PView<R> &p, int N, const R *phi, const LcKernelArgs &la, float *pos, float *vel,
+                      int64_t *ids, unsigned long long *count, int64_t *prelog, unsigned long long *prelog_count,
+                      int64_t prelog_cap, int *err, cudaStream_t st);
+
+}  // namespace gev

@@ -1,0 +1,130 @@
+// lightcone.cu -- particle lightcone crossing for one shell and one cycle.
+//
+// One thread per particle, one pass: the shell and cone test of
+// count_tracer_particles / buffer_tracer_particles
+// (Particles_gevolution.hpp:1271-1345, :1381-1466) against the periodic images
+// of the vertex, the ID-backlog de-duplication of the check zone
+// (count_lightcone_duplicate_ids / mark_lightcone_kept_particles, :1468-1510),
+// the interpolation to the crossing time (bufferTracerParticle with
+// EXACT_OUTPUT_REDSHIFTS, :500-560) and the logging of IDs near the inner
+// edge for the next cycle's backlog.  Slots come from one atomic counter; the
+// output order is not significant (the reference's is not either).
+#include "common.cuh"
+#include "kernels.h"
+#include "particles.cuh"
+
+namespace gev {
+
+constexpr double LC_IDCHECK_ZONE = 0.05;            // metadata.hpp:38-40
+constexpr double LC_GADGET_VEL = 3.335640952e-6;    // GADGET_VELOCITY_CONVERSION, metadata.hpp
+
+__device__ __forceinline__ bool backlog_contains(const int64_t *b, int64_t n, int64_t id)
+{
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        int64_t mid = lo + (hi - lo) / 2;
+        if (b[mid] < id) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo < n && b[lo] == id;
+}
+
+template <class R>
+__device__ __forceinline__ double gphi(const R *phi, int N, int x, int y, int z)
+{
+    return (double)phi[sidx(N, wrapi(x, N), wrapi(y, N), wrapi(z, N))];
+}
+
+template <class R>
+__global__ void k_lightcone(PView<R> p, int N, const R *__restrict__ phi, LcKernelArgs la, float *opos, float *ovel,
+                            int64_t *oid, unsigned long long *count, int64_t *prelog,
+                            unsigned long long *prelog_count, int64_t prelog_cap, int *err)
+{
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const int64_t id = p.id[i];
+    if (la.tracer_factor > 1 && id % la.tracer_factor != 0) return;
+    const uint32_t cell = p.cell[i];
+    if ((int64_t)cell >= (int64_t)N * N * N) { atomicOr(err, ERR_BAD_CELL); return; }
+    const int c[3] = {(int)(cell % (uint32_t)N), (int)((cell / (uint32_t)N) % (uint32_t)N), (int)(cell / ((uint32_t)N * (uint32_t)N))};
+    const double fr[3] = {p.off[i], p.off[p.cap + i], p.off[2 * p.cap + i]};
+    const double x[3] = {(c[0] + fr[0]) / N, (c[1] + fr[1]) / N, (c[2] + fr[2]) / N};
+    const double q[3] = {(double)p.q[i], (double)p.q[p.cap + i], (double)p.q[2 * p.cap + i]};
+
+    for (int v = 0; v < la.nvtx; v++) {
+        const double *V = la.vtx[v];
+        double r[3] = {x[0] - V[0], x[1] - V[1], x[2] - V[2]};
+        double d = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+        if (!(d >= la.inner && d < la.outer)) continue;
+        if (!(la.opening == -1. || (r[0] * la.direction[0] + r[1] * la.direction[1] + r[2] * la.direction[2]) / d > la.opening)) continue;
+
+        // check zone near the outer edge: drop IDs written in the previous cycle
+        if (la.outer - d <= 2. * LC_IDCHECK_ZONE * la.dtau_old && backlog_contains(la.backlog, la.backlog_n, id)) return;
+
+        double vlos = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + la.a * (la.a + la.dtau_old * la.dadtau));
+        vlos = (q[0] * r[0] + q[1] * r[1] + q[2] * r[2]) / d / vlos;
+        const double dtau_pos = (la.dist - d) / (1. + vlos);
+        const double dtau_vel = dtau_pos + 0.5 * la.dtau_old;
+        const double at = la.a + dtau_pos * la.dadtau;
+
+        // bufferTracerParticle (EXACT_OUTPUT_REDSHIFTS)
+        double phip = 0., g[3] = {0., 0., 0.};
+        if (phi) {
+            double w[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                w[k] = (((k >> 2) & 1) ? fr[0] : 1. - fr[0]) * (((k >> 1) & 1) ? fr[1] : 1. - fr[1]) * ((k & 1) ? fr[2] : 1. - fr[2]);
+            double P[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) P[k] = gphi(phi, N, c[0] + ((k >> 2) & 1), c[1] + ((k >> 1) & 1), c[2] + (k & 1));
+#pragma unroll
+            for (int k = 0; k < 8; k++) phip += w[k] * P[k];
+            // P[4bx+2by+bz]
+            g[0] = (1 - fr[1]) * (1 - fr[2]) * (P[4] - P[0]) + fr[1] * (1 - fr[2]) * (P[6] - P[2]) + (1 - fr[1]) * fr[2] * (P[5] - P[1]) + fr[1] * fr[2] * (P[7] - P[3]);
+            g[1] = (1 - fr[0]) * (1 - fr[2]) * (P[2] - P[0]) + fr[0] * (1 - fr[2]) * (P[6] - P[4]) + (1 - fr[0]) * fr[2] * (P[3] - P[1]) + fr[0] * fr[2] * (P[7] - P[5]);
+            g[2] = (1 - fr[0]) * (1 - fr[1]) * (P[1] - P[0]) + fr[0] * (1 - fr[1]) * (P[5] - P[4]) + (1 - fr[0]) * fr[1] * (P[3] - P[2]) + fr[0] * fr[1] * (P[7] - P[6]);
+        }
+        double q2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+        double f1 = q2 + at * at, f2 = sqrt(f1), f0 = q2 + f1;
+        f1 = 1. + (4. - f0 / f1) * phip;
+        const double rescale_vel = 1. / sqrt(at) / LC_GADGET_VEL;
+
+        unsigned long long slot = atomicAdd(count, 1ull);
+        if (slot < (unsigned long long)la.capacity) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                float pos_offset = (float)(la.lc_vertex[k] - V[k]);
+                opos[3 * slot + k] = ((float)(x[k] + dtau_pos * q[k] * f1 / f2) + pos_offset) * (float)la.boxsize;
+                ovel[3 * slot + k] = (float)((q[k] - dtau_vel * f0 * g[k] * (double)N / f2) * rescale_vel) / (float)at;
+            }
+            oid[slot] = id;
+        } else {
+            atomicOr(err, ERR_LC_OVERFLOW);
+        }
+        if (d - la.inner < 2. * LC_IDCHECK_ZONE * la.dtau) {
+            unsigned long long ls = atomicAdd(prelog_count, 1ull);
+            if (ls < (unsigned long long)prelog_cap) prelog[ls] = id;
+            else atomicOr(err, ERR_LC_OVERFLOW);
+        }
+        return;
+    }
+}
+
+template <class R>
+void launch_lightcone(const PView<R> &p, int N, const R *phi, const LcKernelArgs &la, float *pos, float *vel,
+                      int64_t *ids, unsigned long long *count, int64_t *prelog, unsigned long long *prelog_count,
+                      int64_t prelog_cap, int *err, cudaStream_t st)
+{
+    if (p.n > 0)
+        k_lightcone<R><<<cdiv(p.n, 256), 256, 0, st>>>(p, N, phi, la, pos, vel, ids, count, prelog, prelog_count,
+                                                      prelog_cap, err);
+}
+
+template void launch_lightcone<float>(const PView<float> &, int, const float *, const LcKernelArgs &, float *, float *,
+                                      int64_t *, unsigned long long *, int64_t *, unsigned long long *, int64_t, int *,
+                                      cudaStream_t);
+template void launch_lightcone<double>(const PView<double> &, int, const double *, const LcKernelArgs &, float *,
+                                       float *, int64_t *, unsigned long long *, int64_t *, unsigned long long *,
+                                       int64_t, int *, cudaStream_t);
+
+}  // namespace gev

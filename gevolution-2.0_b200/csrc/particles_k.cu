@@ -1,0 +1,439 @@
+// particles_k.cu -- geodesic kick + drift, tile re-bucketing, particle I/O.
+//
+// Kick and drift follow update_q (gevolution.hpp:888-1011, GRADIENT_ORDER 2)
+// and update_pos (:1162-1232) term by term in FP64.  One CTA handles one
+// tile's particles and stages phi, chi and B_i over the tile plus the stencil
+// reach ([-1, 10)^3 relative to the tile origin) in shared memory, so every
+// gather is a shared-memory read.  The drift moves the cell index and the FP64
+// in-cell offset and assigns the particle its new bucket; a warp-aggregated
+// counter gives it a slot, and launch_scatter moves it into bucket order after
+// an exclusive scan of the bucket counts (the re-binning that LATfield2's
+// moveParticles does into its row buffers).
+#include "common.cuh"
+#include "kernels.h"
+#include "particles.cuh"
+
+namespace gev {
+
+constexpr int KD_NT = 256;
+constexpr int KD_W = 11;   // staged extent per axis
+
+template <class R>
+__device__ __forceinline__ double SF(const R *s, int rx, int ry, int rz, int dx, int dy, int dz)
+{
+    return (double)s[(rx + 1 + dx) + KD_W * ((ry + 1 + dy) + KD_W * (rz + 1 + dz))];
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt()
+{
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// slot within bucket b, warp-aggregated (order inside a bucket is not significant)
+__device__ __forceinline__ uint32_t bucket_slot(uint32_t b, uint32_t *counts)
+{
+    unsigned act = __activemask();
+    unsigned peers = __match_any_sync(act, b);
+    int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&counts[b], (uint32_t)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    return base + (uint32_t)__popc(peers & lanemask_lt());
+}
+
+template <class R>
+__global__ void __launch_bounds__(KD_NT) k_kick_drift(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt,
+                                                      const R *__restrict__ phi, const R *__restrict__ chi,
+                                                      const R *__restrict__ Bi, int64_t n3, KickDriftParams kp,
+                                                      uint32_t *counts, uint32_t *bucket, uint32_t *rank,
+                                                      unsigned long long *vmax_bits, int *err)
+{
+    extern __shared__ __align__(16) unsigned char kd_smem[];
+    R(*sf)[KD_W * KD_W * KD_W] = reinterpret_cast<R(*)[KD_W * KD_W * KD_W]>(kd_smem);
+    __shared__ double wmax[KD_NT / 32];
+    const int tile = blockIdx.x;
+    const int tx = tile % nt, ty = (tile / nt) % nt, tz = tile / (nt * nt);
+    const int x0 = tx * 8, y0 = ty * 8, z0 = tz * 8;
+
+    const bool need_phi = kp.do_kick || (kp.do_drift && kp.nfield_d >= 1);
+    const bool need_chi = (kp.do_kick && kp.nfield_k >= 2) || (kp.do_drift && kp.nfield_d >= 2);
+    const bool need_B = (kp.do_kick && kp.nfield_k >= 3) || (kp.do_drift && kp.nfield_d >= 3);
+    for (int i = threadIdx.x; i < KD_W * KD_W * KD_W; i += KD_NT) {
+        int vx = i % KD_W - 1, vy = (i / KD_W) % KD_W - 1, vz = i / (KD_W * KD_W) - 1;
+        int64_t g = sidx(N, wrapi(x0 + vx, N), wrapi(y0 + vy, N), wrapi(z0 + vz, N));
+        if (need_phi) sf[0][i] = phi[g];
+        if (need_chi) sf[1][i] = chi[g];
+        if (need_B) { sf[2][i] = Bi[g]; sf[3][i] = Bi[n3 + g]; sf[4][i] = Bi[2 * n3 + g]; }
+    }
+    __syncthreads();
+    const R *P_ = sf[0], *X_ = sf[1], *B0 = sf[2], *B1 = sf[3], *B2 = sf[4];
+
+    const uint32_t lo = bstart[8 * tile], hi = bstart[8 * tile + 8];
+    double lmax = 0.0;
+    for (uint32_t base = lo; base < hi; base += KD_NT) {
+        uint32_t i = base + threadIdx.x;
+        if (i >= hi) continue;
+        uint32_t cell = p.cell[i];
+        int cx = (int)(cell % (uint32_t)N), cy = (int)((cell / (uint32_t)N) % (uint32_t)N), cz = (int)(cell / ((uint32_t)N * (uint32_t)N));
+        int rx = cx - x0, ry = cy - y0, rz = cz - z0;
+        // a particle outside this tile means the bucket order is stale: flag it, leave it
+        // unmoved (never read outside the stage) and still give it a bucket slot
+        const bool ok = !(rx < 0 || rx > 7 || ry < 0 || ry > 7 || rz < 0 || rz > 7);
+        if (!ok) atomicOr(err, ERR_BAD_CELL);
+        if (!ok) { rx = ry = rz = 0; cx = x0; cy = y0; cz = z0; }
+        double d[3] = {p.off[i], p.off[p.cap + i], p.off[2 * p.cap + i]};
+        double v[3] = {(double)p.q[i], (double)p.q[p.cap + i], (double)p.q[2 * p.cap + i]};
+        double w8[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            w8[k] = (((k >> 2) & 1) ? d[0] : 1.0 - d[0]) * (((k >> 1) & 1) ? d[1] : 1.0 - d[1]) * ((k & 1) ? d[2] : 1.0 - d[2]);
+
+        if (kp.do_kick && ok) {
+            // update_q, gevolution.hpp:888-1011
+            const double a = kp.a_k;
+            double gradphi[3];
+            double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+            double e2 = v2 + a * a;
+            double phiint = 0.0;
+#pragma unroll
+            for (int k = 0; k < 8; k++) phiint += w8[k] * SF(P_, rx, ry, rz, (k >> 2) & 1, (k >> 1) & 1, k & 1);
+            phiint /= e2;
+            phiint = 4. * phiint * v2 + (1. + a * a * phiint) * (v2 + e2) / e2;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const int ex = c == 0, ey = c == 1, ez = c == 2;
+                double g = 0.0;
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    int bx = (k >> 2) & 1, by = (k >> 1) & 1, bz = k & 1;
+                    g += 0.5 * w8[k] * (SF(P_, rx, ry, rz, bx + ex, by + ey, bz + ez) - SF(P_, rx, ry, rz, bx - ex, by - ey, bz - ez));
+                }
+                gradphi[c] = g * phiint;
+            }
+            if (kp.nfield_k >= 2) {
+                gradphi[0] -= (1 - d[1]) * (1 - d[2]) * (SF(X_, rx, ry, rz, 1, 0, 0) - SF(X_, rx, ry, rz, 0, 0, 0));
+                gradphi[1] -= (1 - d[0]) * (1 - d[2]) * (SF(X_, rx, ry, rz, 0, 1, 0) - SF(X_, rx, ry, rz, 0, 0, 0));
+                gradphi[2] -= (1 - d[0]) * (1 - d[1]) * (SF(X_, rx, ry, rz, 0, 0, 1) - SF(X_, rx, ry, rz, 0, 0, 0));
+                gradphi[0] -= d[1] * (1 - d[2]) * (SF(X_, rx, ry, rz, 1, 1, 0) - SF(X_, rx, ry, rz, 0, 1, 0));
+                gradphi[1] -= d[0] * (1 - d[2]) * (SF(X_, rx, ry, rz, 1, 1, 0) - SF(X_, rx, ry, rz, 1, 0, 0));
+                gradphi[2] -= d[0] * (1 - d[1]) * (SF(X_, rx, ry, rz, 1, 0, 1) - SF(X_, rx, ry, rz, 1, 0, 0));
+                gradphi[0] -= (1 - d[1]) * d[2] * (SF(X_, rx, ry, rz, 1, 0, 1) - SF(X_, rx, ry, rz, 0, 0, 1));
+                gradphi[1] -= (1 - d[0]) * d[2] * (SF(X_, rx, ry, rz, 0, 1, 1) - SF(X_, rx, ry, rz, 0, 0, 1));
+                gradphi[2] -= (1 - d[0]) * d[1] * (SF(X_, rx, ry, rz, 0, 1, 1) - SF(X_, rx, ry, rz, 0, 1, 0));
+                gradphi[0] -= d[1] * d[2] * (SF(X_, rx, ry, rz, 1, 1, 1) - SF(X_, rx, ry, rz, 0, 1, 1));
+                gradphi[1] -= d[0] * d[2] * (SF(X_, rx, ry, rz, 1, 1, 1) - SF(X_, rx, ry, rz, 1, 0, 1));
+                gradphi[2] -= d[0] * d[1] * (SF(X_, rx, ry, rz, 1, 1, 1) - SF(X_, rx, ry, rz, 1, 1, 0));
+            }
+            e2 = sqrt(e2);
+            if (kp.nfield_k >= 3) {
+                // gevolution.hpp:970-993
+                double pg[3];
+                pg[0] = ((1 - d[2]) * (SF(B1, rx, ry, rz, 1, 0, 0) - SF(B1, rx, ry, rz, 0, 0, 0)) + d[2] * (SF(B1, rx, ry, rz, 1, 0, 1) - SF(B1, rx, ry, rz, 0, 0, 1))) * v[1];
+                pg[0] += ((1 - d[1]) * (SF(B2, rx, ry, rz, 1, 0, 0) - SF(B2, rx, ry, rz, 0, 0, 0)) + d[1] * (SF(B2, rx, ry, rz, 1, 1, 0) - SF(B2, rx, ry, rz, 0, 1, 0))) * v[2];
+                pg[0] += (1 - d[1]) * (1 - d[2]) * ((d[0] - 1) * SF(B0, rx, ry, rz, -1, 0, 0) + (1 - 2 * d[0]) * SF(B0, rx, ry, rz, 0, 0, 0) + d[0] * SF(B0, rx, ry, rz, 1, 0, 0)) * v[0];
+                pg[0] += d[1] * (1 - d[2]) * ((d[0] - 1) * SF(B0, rx, ry, rz, -1, 1, 0) + (1 - 2 * d[0]) * SF(B0, rx, ry, rz, 0, 1, 0) + d[0] * SF(B0, rx, ry, rz, 1, 1, 0)) * v[0];
+                pg[0] += (1 - d[1]) * d[2] * ((d[0] - 1) * SF(B0, rx, ry, rz, -1, 0, 1) + (1 - 2 * d[0]) * SF(B0, rx, ry, rz, 0, 0, 1) + d[0] * SF(B0, rx, ry, rz, 1, 0, 1)) * v[0];
+                pg[0] += d[1] * d[2] * ((d[0] - 1) * SF(B0, rx, ry, rz, -1, 1, 1) + (1 - 2 * d[0]) * SF(B0, rx, ry, rz, 0, 1, 1) + d[0] * SF(B0, rx, ry, rz, 1, 1, 1)) * v[0];
+
+                pg[1] = ((1 - d[0]) * (SF(B2, rx, ry, rz, 0, 1, 0) - SF(B2, rx, ry, rz, 0, 0, 0)) + d[0] * (SF(B2, rx, ry, rz, 1, 1, 0) - SF(B2, rx, ry, rz, 1, 0, 0))) * v[2];
+                pg[1] += ((1 - d[2]) * (SF(B0, rx, ry, rz, 0, 1, 0) - SF(B0, rx, ry, rz, 0, 0, 0)) + d[2] * (SF(B0, rx, ry, rz, 0, 1, 1) - SF(B0, rx, ry, rz, 0, 0, 1))) * v[0];
+                pg[1] += (1 - d[0]) * (1 - d[2]) * ((d[1] - 1) * SF(B1, rx, ry, rz, 0, -1, 0) + (1 - 2 * d[1]) * SF(B1, rx, ry, rz, 0, 0, 0) + d[1] * SF(B1, rx, ry, rz, 0, 1, 0)) * v[1];
+                pg[1] += d[0] * (1 - d[2]) * ((d[1] - 1) * SF(B1, rx, ry, rz, 1, -1, 0) + (1 - 2 * d[1]) * SF(B1, rx, ry, rz, 1, 0, 0) + d[1] * SF(B1, rx, ry, rz, 1, 1, 0)) * v[1];
+                pg[1] += (1 - d[0]) * d[2] * ((d[1] - 1) * SF(B1, rx, ry, rz, 0, -1, 1) + (1 - 2 * d[1]) * SF(B1, rx, ry, rz, 0, 0, 1) + d[1] * SF(B1, rx, ry, rz, 0, 1, 1)) * v[1];
+                pg[1] += d[0] * d[2] * ((d[1] - 1) * SF(B1, rx, ry, rz, 1, -1, 1) + (1 - 2 * d[1]) * SF(B1, rx, ry, rz, 1, 0, 1) + d[1] * SF(B1, rx, ry, rz, 1, 1, 1)) * v[1];
+
+                pg[2] = ((1 - d[1]) * (SF(B0, rx, ry, rz, 0, 0, 1) - SF(B0, rx, ry, rz, 0, 0, 0)) + d[1] * (SF(B0, rx, ry, rz, 0, 1, 1) - SF(B0, rx, ry, rz, 0, 1, 0))) * v[0];
+                pg[2] += ((1 - d[0]) * (SF(B1, rx, ry, rz, 0, 0, 1) - SF(B1, rx, ry, rz, 0, 0, 0)) + d[0] * (SF(B1, rx, ry, rz, 1, 0, 1) - SF(B1, rx, ry, rz, 1, 0, 0))) * v[1];
+                pg[2] += (1 - d[0]) * (1 - d[1]) * ((d[2] - 1) * SF(B2, rx, ry, rz, 0, 0, -1) + (1 - 2 * d[2]) * SF(B2, rx, ry, rz, 0, 0, 0) + d[2] * SF(B2, rx, ry, rz, 0, 0, 1)) * v[2];
+                pg[2] += d[0] * (1 - d[1]) * ((d[2] - 1) * SF(B2, rx, ry, rz, 1, 0, -1) + (1 - 2 * d[2]) * SF(B2, rx, ry, rz, 1, 0, 0) + d[2] * SF(B2, rx, ry, rz, 1, 0, 1)) * v[2];
+                pg[2] += (1 - d[0]) * d[1] * ((d[2] - 1) * SF(B2, rx, ry, rz, 0, 1, -1) + (1 - 2 * d[2]) * SF(B2, rx, ry, rz, 0, 1, 0) + d[2] * SF(B2, rx, ry, rz, 0, 1, 1)) * v[2];
+                pg[2] += d[0] * d[1] * ((d[2] - 1) * SF(B2, rx, ry, rz, 1, 1, -1) + (1 - 2 * d[2]) * SF(B2, rx, ry, rz, 1, 1, 0) + d[2] * SF(B2, rx, ry, rz, 1, 1, 1)) * v[2];
+#pragma unroll
+                for (int c = 0; c < 3; c++) gradphi[c] += pg[c] / kp.b_k / e2;
+            }
+            v2 = 0.0;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                v[c] -= kp.dtau_k * e2 * gradphi[c] * (double)N;
+                v2 += v[c] * v[c];
+            }
+            lmax = fmax(lmax, v2 / a / a);
+#pragma unroll
+            for (int c = 0; c < 3; c++) p.q[c * p.cap + i] = (R)v[c];
+        }
+
+        if (kp.do_drift && ok) {
+            // update_pos, gevolution.hpp:1162-1232 (drift uses the kicked momentum,
+            // rounded to the storage precision as the reference stores it first)
+#pragma unroll
+            for (int c = 0; c < 3; c++) v[c] = (double)p.q[c * p.cap + i];
+            const double a = kp.a_d;
+            double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+            double e2 = v2 + a * a;
+            double ph = 0.0, ch = 0.0;
+            if (kp.nfield_d >= 1) {
+#pragma unroll
+                for (int k = 0; k < 8; k++) ph += w8[k] * SF(P_, rx, ry, rz, (k >> 2) & 1, (k >> 1) & 1, k & 1);
+            }
+            if (kp.nfield_d >= 2) {
+#pragma unroll
+                for (int k = 0; k < 8; k++) ch += w8[k] * SF(X_, rx, ry, rz, (k >> 2) & 1, (k >> 1) & 1, k & 1);
+            }
+            v2 = (1. + (3. - v2 / e2) * ph - ch) / sqrt(e2);
+            double dp[3] = {v[0] * v2, v[1] * v2, v[2] * v2};
+            if (kp.nfield_d >= 3) {
+                double b0 = SF(B0, rx, ry, rz, 0, 0, 0) * (1 - d[1]) * (1 - d[2]) + SF(B0, rx, ry, rz, 0, 1, 0) * d[1] * (1 - d[2]) +
+                            SF(B0, rx, ry, rz, 0, 0, 1) * (1 - d[1]) * d[2] + SF(B0, rx, ry, rz, 0, 1, 1) * d[1] * d[2];
+                double b1 = SF(B1, rx, ry, rz, 0, 0, 0) * (1 - d[0]) * (1 - d[2]) + SF(B1, rx, ry, rz, 1, 0, 0) * d[0] * (1 - d[2]) +
+                            SF(B1, rx, ry, rz, 0, 0, 1) * (1 - d[0]) * d[2] + SF(B1, rx, ry, rz, 1, 0, 1) * d[0] * d[2];
+                double b2 = SF(B2, rx, ry, rz, 0, 0, 0) * (1 - d[0]) * (1 - d[1]) + SF(B2, rx, ry, rz, 1, 0, 0) * d[0] * (1 - d[1]) +
+                            SF(B2, rx, ry, rz, 0, 1, 0) * (1 - d[0]) * d[1] + SF(B2, rx, ry, rz, 1, 1, 0) * d[0] * d[1];
+                dp[0] += b0 / kp.b_d;
+                dp[1] += b1 / kp.b_d;
+                dp[2] += b2 / kp.b_d;
+            }
+            int cc[3] = {cx, cy, cz};
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                double o = d[c] + kp.dtau_d * dp[c] * (double)N;   // box units -> cell units
+                if (!isfinite(o)) { atomicOr(err, ERR_NONFINITE); o = d[c]; }
+                double s = floor(o);
+                o -= s;
+                if (o >= 1.0) { o = 0.0; s += 1.0; }
+                long long sh = (long long)s;
+                long long nc = ((long long)cc[c] + sh) % N;
+                if (nc < 0) nc += N;
+                cc[c] = (int)nc;
+                p.off[c * p.cap + i] = o;
+            }
+            cx = cc[0]; cy = cc[1]; cz = cc[2];
+            p.cell[i] = (uint32_t)sidx(N, cx, cy, cz);
+        }
+        if (kp.do_bin) {
+            uint32_t b = bucket_of_cell(N, nt, cx, cy, cz);
+            bucket[i] = b;
+            rank[i] = bucket_slot(b, counts);
+        }
+    }
+
+    for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = lmax;
+    __syncthreads();
+    if (threadIdx.x == 0 && kp.do_kick) {
+        double m = 0.0;
+        for (int w = 0; w < KD_NT / 32; w++) m = fmax(m, wmax[w]);
+        atomicMax(vmax_bits, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+template <class R>
+void launch_kick_drift(const PView<R> &p, const uint32_t *bstart, int N, const R *phi, const R *chi, const R *Bi,
+                       int64_t n3, const KickDriftParams &kp, uint32_t *counts, uint32_t *bucket, uint32_t *rank,
+                       unsigned long long *vmax_bits, int *err, cudaStream_t st)
+{
+    int nt = N / 8;
+    const size_t smem = 5 * KD_W * KD_W * KD_W * sizeof(R);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_kick_drift<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_set = true;
+    }
+    k_kick_drift<R><<<(unsigned)nt * nt * nt, KD_NT, smem, st>>>(p, bstart, N, nt, phi, chi, Bi, n3, kp, counts,
+                                                                bucket, rank, vmax_bits, err);
+}
+
+// ---- particle I/O: host layout (box-unit positions, AoS triples) <-> cell + offset ----
+template <class R>
+__global__ void k_load_particles(PView<R> p, const double *pos, const double *q, const int64_t *id, int64_t n, int N,
+                                 int *err)
+{
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        double x = pos[3 * i + k];
+        if (!isfinite(x)) { atomicOr(err, ERR_NONFINITE); x = 0.0; }
+        x -= floor(x);
+        double s = x * N;
+        double f = floor(s);
+        double o = s - f;
+        int ci = (int)f;
+        if (ci >= N) { ci = N - 1; o = 1.0 - 1e-16; }
+        if (ci < 0) { ci = 0; o = 0.0; }
+        c[k] = ci;
+        p.off[k * p.cap + i] = o;
+        p.q[k * p.cap + i] = (R)q[3 * i + k];
+    }
+    p.cell[i] = (uint32_t)sidx(N, c[0], c[1], c[2]);
+    p.id[i] = id ? id[i] : i;
+}
+
+template <class R>
+__global__ void k_store_particles(PView<R> p, double *pos, double *q, int64_t *id, int64_t n, int N)
+{
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t cell = p.cell[i];
+    int c[3] = {(int)(cell % (uint32_t)N), (int)((cell / (uint32_t)N) % (uint32_t)N), (int)(cell / ((uint32_t)N * (uint32_t)N))};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        if (pos) pos[3 * i + k] = ((double)c[k] + p.off[k * p.cap + i]) / (double)N;
+        if (q) q[3 * i + k] = (double)p.q[k * p.cap + i];
+    }
+    if (id) id[i] = p.id[i];
+}
+
+template <class R>
+void launch_load_particles(PView<R> p, const double *pos, const double *q, const int64_t *id, int64_t n, int N,
+                           int *err, cudaStream_t st)
+{
+    if (n > 0) k_load_particles<R><<<cdiv(n, 256), 256, 0, st>>>(p, pos, q, id, n, N, err);
+}
+
+template <class R>
+void launch_store_particles(const PView<R> &p, double *pos, double *q, int64_t *id, int64_t n, int N,
+                            cudaStream_t st)
+{
+    if (n > 0) k_store_particles<R><<<cdiv(n, 256), 256, 0, st>>>(p, pos, q, id, n, N);
+}
+
+template <class R>
+__global__ void k_bin_count(PView<R> p, int N, int nt, uint32_t *counts, uint32_t *bucket, uint32_t *rank)
+{
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    uint32_t cell = p.cell[i];
+    if ((int64_t)cell >= (int64_t)N * N * N) cell = 0;   // loaded cells are always in range; never index past the counts
+    int cx = (int)(cell % (uint32_t)N), cy = (int)((cell / (uint32_t)N) % (uint32_t)N), cz = (int)(cell / ((uint32_t)N * (uint32_t)N));
+    uint32_t b = bucket_of_cell(N, nt, cx, cy, cz);
+    bucket[i] = b;
+    rank[i] = bucket_slot(b, counts);
+}
+
+template <class R>
+void launch_bin_count(const PView<R> &p, int N, uint32_t *counts, uint32_t *bucket, uint32_t *rank, cudaStream_t st)
+{
+    if (p.n > 0) k_bin_count<R><<<cdiv(p.n, 256), 256, 0, st>>>(p, N, N / 8, counts, bucket, rank);
+}
+
+// ---- exclusive scan of bucket counts: start[0..nb] ----
+constexpr int SCAN_NT = 1024;
+
+__global__ void k_scan_blocks(const uint32_t *counts, uint32_t *start, int64_t nb, uint32_t *block_sums)
+{
+    __shared__ uint32_t s[SCAN_NT];
+    int64_t i = blockIdx.x * (int64_t)SCAN_NT + threadIdx.x;
+    uint32_t v = (i < nb) ? counts[i] : 0u;
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < SCAN_NT; o <<= 1) {
+        uint32_t t = (threadIdx.x >= (unsigned)o) ? s[threadIdx.x - o] : 0u;
+        __syncthreads();
+        s[threadIdx.x] += t;
+        __syncthreads();
+    }
+    if (i < nb) start[i] = s[threadIdx.x] - v;
+    if (threadIdx.x == SCAN_NT - 1) block_sums[blockIdx.x] = s[threadIdx.x];
+}
+
+__global__ void k_scan_sums(uint32_t *block_sums, int64_t nblk, uint32_t *start, int64_t nb)
+{
+    __shared__ uint32_t s[SCAN_NT];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int64_t b0 = 0; b0 < nblk; b0 += SCAN_NT) {
+        int64_t i = b0 + threadIdx.x;
+        uint32_t v = (i < nblk) ? block_sums[i] : 0u;
+        s[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < SCAN_NT; o <<= 1) {
+            uint32_t t = (threadIdx.x >= (unsigned)o) ? s[threadIdx.x - o] : 0u;
+            __syncthreads();
+            s[threadIdx.x] += t;
+            __syncthreads();
+        }
+        if (i < nblk) block_sums[i] = carry + s[threadIdx.x] - v;
+        __syncthreads();
+        if (threadIdx.x == SCAN_NT - 1) carry += s[threadIdx.x];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) start[nb] = carry;
+}
+
+__global__ void k_scan_add(uint32_t *start, int64_t nb, const uint32_t *block_sums)
+{
+    int64_t i = blockIdx.x * (int64_t)SCAN_NT + threadIdx.x;
+    if (i < nb) start[i] += block_sums[blockIdx.x];
+}
+
+void launch_scan(const uint32_t *counts, uint32_t *start, int64_t nb, uint32_t *block_sums, cudaStream_t st)
+{
+    int64_t nblk = (nb + SCAN_NT - 1) / SCAN_NT;
+    k_scan_blocks<<<(unsigned)nblk, SCAN_NT, 0, st>>>(counts, start, nb, block_sums);
+    k_scan_sums<<<1, SCAN_NT, 0, st>>>(block_sums, nblk, start, nb);
+    k_scan_add<<<(unsigned)nblk, SCAN_NT, 0, st>>>(start, nb, block_sums);
+}
+
+template <class R>
+__global__ void k_scatter(PView<R> src, PView<R> dst, const uint32_t *bstart, const uint32_t *bucket, const uint32_t *rank)
+{
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= src.n) return;
+    uint32_t j = bstart[bucket[i]] + rank[i];
+    if ((int64_t)j >= src.n) return;   // inconsistent counts: never write out of range
+    dst.cell[j] = src.cell[i];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        dst.off[k * dst.cap + j] = src.off[k * src.cap + i];
+        dst.q[k * dst.cap + j] = src.q[k * src.cap + i];
+    }
+    dst.id[j] = src.id[i];
+}
+
+template <class R>
+void launch_scatter(const PView<R> &src, PView<R> dst, const uint32_t *bstart, const uint32_t *bucket,
+                    const uint32_t *rank, cudaStream_t st)
+{
+    if (src.n > 0) k_scatter<R><<<cdiv(src.n, 256), 256, 0, st>>>(src, dst, bstart, bucket, rank);
+}
+
+// deterministic sum of per-block partials (fixed order)
+__global__ void k_reduce_sum(const double *partial, int64_t n, double *out)
+{
+    __shared__ double s[1024];
+    double v = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += 1024) v += partial[i];
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 512; o > 0; o >>= 1) {
+        if (threadIdx.x < (unsigned)o) s[threadIdx.x] += s[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = s[0];
+}
+
+void launch_reduce_sum(const double *partial, int64_t n, double *out, cudaStream_t st)
+{
+    k_reduce_sum<<<1, 1024, 0, st>>>(partial, n, out);
+}
+
+#define GEV_INST(R)                                                                                                   \
+    template void launch_kick_drift<R>(const PView<R> &, const uint32_t *, int, const R *, const R *, const R *,     \
+                                       int64_t, const KickDriftParams &, uint32_t *, uint32_t *, uint32_t *,          \
+                                       unsigned long long *, int *, cudaStream_t);                                    \
+    template void launch_load_particles<R>(PView<R>, const double *, const double *, const int64_t *, int64_t, int,  \
+                                           int *, cudaStream_t);                                                      \
+    template void launch_store_particles<R>(const PView<R> &, double *, double *, int64_t *, int64_t, int,           \
+                                            cudaStream_t);                                                            \
+    template void launch_bin_count<R>(const PView<R> &, int, uint32_t *, uint32_t *, uint32_t *, cudaStream_t);       \
+    template void launch_scatter<R>(const PView<R> &, PView<R>, const uint32_t *, const uint32_t *, const uint32_t *, \
+                                    cudaStream_t);
+GEV_INST(float)
+GEV_INST(double)
+#undef GEV_INST
+
+}  // namespace gev

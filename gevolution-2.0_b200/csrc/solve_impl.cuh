@@ -1,0 +1,158 @@
+// solve_impl.cuh -- launchers of the pencil passes for every supported grid
+// size; included once per precision (solve_f32.cu, solve_f64.cu).
+#pragma once
+
+#include <stdexcept>
+
+#include "fftpass.cuh"
+#include "kernels.h"
+
+namespace gev {
+
+template <class R> struct PassCfg {
+    static constexpr int TX = sizeof(R) == 4 ? 16 : 8;   // rows per x-pass CTA
+    static constexpr int TY = sizeof(R) == 4 ? 16 : 8;   // columns per y-pass CTA
+    static constexpr int TZ1 = sizeof(R) == 4 ? 16 : 8;  // Poisson
+    static constexpr int TZ3 = sizeof(R) == 4 ? 8 : 4;   // vector
+    static constexpr int TZ6 = sizeof(R) == 4 ? 4 : 2;   // scalar / tensor
+};
+
+template <class K> inline void set_smem(K kernel, size_t bytes)
+{
+    if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+#define GEV_SWITCH_N(N, CALL)                          \
+    switch (N) {                                       \
+    case 16: { constexpr int NN = 16; CALL; } break;   \
+    case 32: { constexpr int NN = 32; CALL; } break;   \
+    case 64: { constexpr int NN = 64; CALL; } break;   \
+    case 128: { constexpr int NN = 128; CALL; } break; \
+    case 256: { constexpr int NN = 256; CALL; } break; \
+    case 384: { constexpr int NN = 384; CALL; } break; \
+    case 512: { constexpr int NN = 512; CALL; } break; \
+    case 768: { constexpr int NN = 768; CALL; } break; \
+    default: throw std::runtime_error("unsupported grid size"); \
+    }
+
+template <class R, int N, int MODE>
+void fx_fwd_n(const FxArgs<R> &a, int ncomp, int64_t in_stride, int64_t out_stride, const FftTables<R> &tb, cudaStream_t st)
+{
+    using C = typename CT<R>::C;
+    constexpr int T = PassCfg<R>::TX, NT = 256;
+    size_t smem = (size_t)(N / 2) * (T + 1) * sizeof(C);
+    auto k = k_fx_fwd<R, N, T, NT, MODE>;
+    set_smem(k, smem);
+    k<<<dim3(N / T, N, ncomp), NT, smem, st>>>(a, in_stride, out_stride, tb.tw_half, tb.tw_full);
+}
+
+template <class R>
+void fx_forward(int N, int mode, const R *in, int64_t in_stride, int ncomp, int comp0, const R *phi, const R *chi,
+                double bg, double c, double c2, double c3, typename CT<R>::C *out, int64_t out_stride,
+                double *partial, const FftTables<R> &tb, cudaStream_t st)
+{
+    FxArgs<R> a;
+    a.in = in; a.phi = phi; a.chi = chi;
+    a.bg = bg; a.c = c; a.c2 = c2; a.c3 = c3;
+    a.comp0 = comp0; a.out = out; a.partial = partial;
+    if (mode == FX_COPY) { GEV_SWITCH_N(N, (fx_fwd_n<R, NN, FX_COPY>(a, ncomp, in_stride, out_stride, tb, st))) }
+    else if (mode == FX_PREP_T00) { GEV_SWITCH_N(N, (fx_fwd_n<R, NN, FX_PREP_T00>(a, ncomp, in_stride, out_stride, tb, st))) }
+    else { GEV_SWITCH_N(N, (fx_fwd_n<R, NN, FX_PREP_TIJ>(a, ncomp, in_stride, out_stride, tb, st))) }
+}
+
+template <class R, int N, int S>
+void fy_n(typename CT<R>::C *data, int64_t stride, int ncomp, const FftTables<R> &tb, cudaStream_t st)
+{
+    using C = typename CT<R>::C;
+    constexpr int T = PassCfg<R>::TY, NT = (N >= 256) ? 512 : 256;
+    size_t smem = (size_t)N * (T + 1) * sizeof(C);
+    auto k = k_fy<R, N, T, NT, S>;
+    set_smem(k, smem);
+    k<<<dim3((N / 2 + 1 + T - 1) / T, N, ncomp), NT, smem, st>>>(data, stride, tb.tw_full);
+}
+
+template <class R>
+void fy_pass(int N, int sign, typename CT<R>::C *data, int64_t stride, int ncomp, const FftTables<R> &tb,
+             cudaStream_t st)
+{
+    if (sign < 0) { GEV_SWITCH_N(N, (fy_n<R, NN, -1>(data, stride, ncomp, tb, st))) }
+    else { GEV_SWITCH_N(N, (fy_n<R, NN, 1>(data, stride, ncomp, tb, st))) }
+}
+
+template <class R, int N>
+void fxi_n(const typename CT<R>::C *in, int64_t in_stride, R *out, int64_t out_stride, int ncomp, const FftTables<R> &tb,
+           cudaStream_t st)
+{
+    using C = typename CT<R>::C;
+    constexpr int T = PassCfg<R>::TX, NT = 256;
+    size_t smem = (size_t)(N / 2) * (T + 1) * sizeof(C);
+    auto k = k_fx_inv<R, N, T, NT>;
+    set_smem(k, smem);
+    k<<<dim3(N / T, N, ncomp), NT, smem, st>>>(in, in_stride, out, out_stride, tb.tw_half, tb.tw_full);
+}
+
+template <class R>
+void fx_inverse(int N, const typename CT<R>::C *in, int64_t in_stride, R *out, int64_t out_stride, int ncomp,
+                const FftTables<R> &tb, cudaStream_t st)
+{
+    GEV_SWITCH_N(N, (fxi_n<R, NN>(in, in_stride, out, out_stride, ncomp, tb, st)))
+}
+
+template <class R, int N, int OP, int EXTRA>
+void fz_n(const FzArgs<R> &a, const FftTables<R> &tb, cudaStream_t st)
+{
+    using C = typename CT<R>::C;
+    constexpr int T = (OP == OP_POISSON || OP == OP_BIN) ? PassCfg<R>::TZ1 : (OP == OP_VECTOR ? PassCfg<R>::TZ3 : PassCfg<R>::TZ6);
+    constexpr int NT = (N >= 256) ? 512 : 256;
+    constexpr int CIN = OpShape<OP, EXTRA>::CIN;
+    size_t smem = (size_t)N * (CIN * T + 1) * sizeof(C);
+    auto k = k_fz<R, N, T, NT, OP, EXTRA>;
+    set_smem(k, smem);
+    k<<<dim3((N / 2 + 1 + T - 1) / T, N), NT, smem, st>>>(a, tb.tw_full);
+}
+
+template <class R, int N>
+void fz_dispatch(const FzParams &fp, const FzArgs<R> &a, const FftTables<R> &tb, cudaStream_t st)
+{
+    if (fp.op == OP_POISSON) fz_n<R, N, OP_POISSON, 0>(a, tb, st);
+    else if (fp.op == OP_BIN) fz_n<R, N, OP_BIN, 0>(a, tb, st);
+    else if (fp.op == OP_VECTOR) fz_n<R, N, OP_VECTOR, 0>(a, tb, st);
+    else {
+        switch (fp.extra) {
+        case 0: fz_n<R, N, OP_SCALAR, 0>(a, tb, st); break;
+        case EXTRA_TENSOR_PROJECT: fz_n<R, N, OP_SCALAR, EXTRA_TENSOR_PROJECT>(a, tb, st); break;
+        case EXTRA_TENSOR_EVOLVE: fz_n<R, N, OP_SCALAR, EXTRA_TENSOR_EVOLVE>(a, tb, st); break;
+        case EXTRA_VECTOR_EVOLVE: fz_n<R, N, OP_SCALAR, EXTRA_VECTOR_EVOLVE>(a, tb, st); break;
+        case EXTRA_TENSOR_PROJECT | EXTRA_VECTOR_EVOLVE: fz_n<R, N, OP_SCALAR, EXTRA_TENSOR_PROJECT | EXTRA_VECTOR_EVOLVE>(a, tb, st); break;
+        case EXTRA_TENSOR_EVOLVE | EXTRA_VECTOR_EVOLVE: fz_n<R, N, OP_SCALAR, EXTRA_TENSOR_EVOLVE | EXTRA_VECTOR_EVOLVE>(a, tb, st); break;
+        default: throw std::runtime_error("unsupported solver combination");
+        }
+    }
+}
+
+template <class R>
+void fz_pass(int N, const FzParams &fp, typename CT<R>::C *data, int64_t stride, typename CT<R>::C *hij,
+             typename CT<R>::C *hijp, typename CT<R>::C *bstate, const FftTables<R> &tb, cudaStream_t st)
+{
+    FzArgs<R> a;
+    a.data = data; a.stride = stride;
+    a.k2 = tb.k2; a.ks = tb.ks;
+    a.p0 = fp.p0; a.p1 = fp.p1; a.p2 = fp.p2; a.p3 = fp.p3;
+    a.extra = fp.extra;
+    a.hij = hij; a.hijp = hijp; a.bstate = bstate;
+    a.phi_hom = fp.phi_hom;
+    a.bins = fp.bins;
+    a.occ = fp.occ;
+    GEV_SWITCH_N(N, (fz_dispatch<R, NN>(fp, a, tb, st)))
+}
+
+#define GEV_SOLVE_INST(R)                                                                                            \
+    template void fx_forward<R>(int, int, const R *, int64_t, int, int, const R *, const R *, double, double, double, \
+                                double, CT<R>::C *, int64_t, double *, const FftTables<R> &, cudaStream_t);          \
+    template void fy_pass<R>(int, int, CT<R>::C *, int64_t, int, const FftTables<R> &, cudaStream_t);                \
+    template void fx_inverse<R>(int, const CT<R>::C *, int64_t, R *, int64_t, int, const FftTables<R> &,             \
+                                cudaStream_t);                                                                       \
+    template void fz_pass<R>(int, const FzParams &, CT<R>::C *, int64_t, CT<R>::C *, CT<R>::C *, CT<R>::C *,          \
+                             const FftTables<R> &, cudaStream_t);
+
+}  // namespace gev

@@ -1,0 +1,214 @@
+/*
+ * gev.h -- C ABI of the B200 (sm_100a) implementation of gevolution-2.0's
+ * per-step particle-mesh cycle on one GPU.
+ *
+ * Plain C types only.  Every function returns a status (GEV_OK = 0); on failure
+ * gev_last_error() returns a message.  Host pointers are borrowed for the
+ * duration of the call.  A context owns all device memory, is used from one host
+ * thread at a time, and orders its work on its own CUDA stream; calls that
+ * return scalars synchronise that stream.
+ *
+ * Layout conventions (the reference's LATfield2 conventions on one rank):
+ *   real fields      N^3 values, index x + N*(y + N*z), periodic;
+ *   symmetric tensor 6 planes in the order 00,01,02,11,12,22;
+ *   vector           3 planes;
+ *   Fourier fields   (N/2+1)*N*N complex values, index kx + (N/2+1)*(ky + N*kz),
+ *                    forward transform exp(-2 pi i k.x/N), unnormalised;
+ *   particles        pos[3n] in box units [0,1), q[3n] momentum per unit mass
+ *                    (LATfield2 part_simple pos/vel), id[n].
+ *
+ * Each entry point names the reference interface it replaces (file:line inside
+ * the gevolution-2.0 tree).
+ */
+#ifndef GEV_B200_H
+#define GEV_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gev_ctx gev_ctx;
+
+/* status codes */
+#define GEV_OK          0
+#define GEV_ERR_ARG     1   /* invalid argument (size, pointer, mode) */
+#define GEV_ERR_CUDA    2   /* CUDA runtime error */
+#define GEV_ERR_STATE   3   /* call out of order (e.g. no particles loaded) */
+#define GEV_ERR_DEVICE  4   /* a kernel raised its device error word */
+#define GEV_ERR_NOMEM   5   /* device allocation failed */
+#define GEV_ERR_CAPACITY 6  /* output buffer too small */
+
+/* precision modes: FP64 everywhere, or FP32 fields/FFTs with particle
+ * positions kept as cell index + FP64 offset and FP64 reductions */
+#define GEV_FP64   0
+#define GEV_MIXED  1
+
+/* vector methods (metadata.hpp:84-85) */
+#define GEV_VECTOR_PARABOLIC 0
+#define GEV_VECTOR_ELLIPTIC  1
+
+/* field identifiers for gev_field_get / gev_field_set */
+#define GEV_FIELD_PHI     0   /* 1 plane  */
+#define GEV_FIELD_CHI     1   /* 1 plane  */
+#define GEV_FIELD_SOURCE  2   /* 1 plane: T00 (main.cu "source") */
+#define GEV_FIELD_SIJ     3   /* 6 planes: Tij, then Sij */
+#define GEV_FIELD_BI      4   /* 3 planes: T0i, then B_i */
+#define GEV_FIELD_HIJ_FT  5   /* 6 complex planes: h_ij in Fourier space */
+#define GEV_FIELD_HIJP_FT 6   /* 6 complex planes: h_ij' in Fourier space */
+#define GEV_FIELD_BI_FT   7   /* 3 complex planes: B_i in Fourier space (parabolic state) */
+
+/* projection selectors for gev_project */
+#define GEV_PROJ_T00 1u
+#define GEV_PROJ_TIJ 2u
+#define GEV_PROJ_T0I 4u
+#define GEV_PROJ_CIC 8u
+
+typedef struct {
+    int32_t N;              /* grid points per side: multiple of 8, N/8 a power of two or 3x one, 16..1024 */
+    int32_t precision;      /* GEV_FP64 or GEV_MIXED */
+    int64_t capacity;       /* maximum number of particles */
+    double boxsize;         /* Mpc/h; used for lightcone output units */
+    int32_t vector_method;  /* GEV_VECTOR_ELLIPTIC or GEV_VECTOR_PARABOLIC */
+    int32_t tensor;         /* nonzero: keep h_ij / h_ij' state (projectFTtensor / evolveFTtensor) */
+    int32_t device;         /* CUDA device ordinal */
+    int32_t reserved;
+} gev_config;
+
+/* Context life cycle.  Replaces LATfield2's Lattice/Field/PlanFFT set-up in
+ * main.cu:298-385 (fields, Fourier fields and FFT plans) and the particle
+ * container initialisation of ic_basic.hpp:2206. */
+int gev_ctx_create(const gev_config *cfg, gev_ctx **out);
+int gev_ctx_destroy(gev_ctx *ctx);
+const char *gev_last_error(const gev_ctx *ctx);
+const char *gev_version(void);
+
+/* Particles.  set: perfParticles::initialize + addParticle_global +
+ * updateRowBuffers (ic_basic.hpp:2206-2211); mass is part_simple_info.mass
+ * (ic_basic.hpp:2198-2201).  get: perfParticles::sampleParticles
+ * (unit_tests.cu:537).  Positions are wrapped into [0,1). */
+int gev_particles_set(gev_ctx *ctx, const double *pos, const double *q, const int64_t *id,
+                      int64_t n, double mass);
+int gev_particles_get(gev_ctx *ctx, double *pos, double *q, int64_t *id, int64_t capacity,
+                      int64_t *n_out);
+int gev_particles_count(const gev_ctx *ctx, int64_t *n_out);
+
+/* Field transfer in double precision (converted to/from the context precision). */
+int gev_field_get(gev_ctx *ctx, int32_t field, double *host);
+int gev_field_set(gev_ctx *ctx, int32_t field, const double *host);
+int gev_field_components(int32_t field);
+
+/* Particle-mesh projections.  which is a mask of GEV_PROJ_*:
+ *   T00: projection_T00_project (gevolution.hpp:1887) + projection_T00_comm
+ *        (:1726) into GEV_FIELD_SOURCE, params {a, coeff};
+ *   TIJ: projection_Tij_project / _Async (:2999, :3030) + projection_Tij_comm
+ *        (:2573-2578) into GEV_FIELD_SIJ, params {a, coeff};
+ *   T0I: projection_T0i_project / _Async (:2232, :2242) + projection_T0i_comm
+ *        (:2028) into GEV_FIELD_BI, params {coeff};
+ *   CIC: scalarProjectionCIC_project (:1902) + comm into GEV_FIELD_SOURCE.
+ * use_phi != 0 applies the Bardeen-potential corrections with GEV_FIELD_PHI
+ * (the reference's phi != nullptr).  accumulate == 0 overwrites the targets
+ * (the reference zeroes them first, main.cu:616, :681, :840); accumulate != 0
+ * adds to them. */
+int gev_project(gev_ctx *ctx, uint32_t which, double a, double coeff, int32_t use_phi,
+                int32_t accumulate);
+
+/* Phi update: prepareFTsource (gevolution.hpp:183) fused into the forward FFT
+ * (main.cu:725, :742), solveModifiedPoissonFT (:806; main.cu:769) in Fourier
+ * space, backward FFT into GEV_FIELD_PHI (main.cu:794).  Reads SOURCE, PHI, CHI.
+ * T00sum receives the sum of the source field (the return value of
+ * prepareFTsource), phi_hom the k=0 mode after the solve (main.cu:808-809).
+ * prepare == 0 skips prepareFTsource (Newtonian / first cycle). */
+int gev_solve_phi(gev_ctx *ctx, int32_t prepare, double bgmodel, double coeff, double coeff2,
+                  double coeff3, double poisson_coeff, double modif, double *T00sum,
+                  double *phi_hom);
+
+/* Chi update: prepareFTsource(phi, Sij, Sij, coeff) (gevolution.hpp:119;
+ * main.cu:822) fused into the 6 forward FFTs (main.cu:829), projectFTscalar
+ * (:251; main.cu:873) and the backward FFT into GEV_FIELD_CHI (main.cu:895).
+ * With the tensor state enabled, projectFTtensor (:693) (first cycle, cycle0 != 0)
+ * or evolveFTtensor (:537) (main.cu:961-965) runs on the same Fourier pencils.
+ * With the parabolic vector method, evolveFTvector (:359; main.cu:933) updates
+ * the B_i Fourier state with a2dtau and GEV_FIELD_BI receives B_i. */
+int gev_solve_chi(gev_ctx *ctx, double coeff, int32_t cycle0, double hubble, double dtau,
+                  double dtau_old, double a2dtau);
+
+/* Elliptic B_i: forward FFT of T0i (main.cu:918), projectFTvector (:449;
+ * main.cu:925), backward FFT into GEV_FIELD_BI (main.cu:948). */
+int gev_solve_B(gev_ctx *ctx, double coeff, double modif);
+
+/* Geodesic kick and drift.  kick: perfParticles::updateVel(update_q_functor,
+ * dtau, {phi,chi,Bi}, nfield, {a, a^2 N}) (main.cu:1230-1235, gevolution.hpp:888);
+ * maxvel receives sqrt(max q^2/a^2), the value updateVel returns.  drift:
+ * perfParticles::moveParticles(update_pos_functor, dtau, fields, nfield,
+ * {a, a^2 N}) (main.cu:1252-1268, gevolution.hpp:1162), including the re-binning
+ * of particles into cells.  gev_kick_drift runs both in one pass (the kick's
+ * fields are the drift's fields, as in the reference's sequence). */
+int gev_kick(gev_ctx *ctx, double dtau, double a, double bcoeff, int32_t nfield, double *maxvel);
+int gev_drift(gev_ctx *ctx, double dtau, double a, double bcoeff, int32_t nfield);
+int gev_kick_drift(gev_ctx *ctx, double dtau_kick, double a_kick, double bcoeff_kick,
+                   int32_t nfield_kick, double dtau_drift, double a_drift, double bcoeff_drift,
+                   int32_t nfield_drift, double *maxvel);
+
+/* Validation spectrum: scalarProjectionCIC_project (gevolution.hpp:1902),
+ * forward FFT, extractPowerSpectrum (tools.hpp:339 -> :65-314) with CIC
+ * deconvolution and linear k bins up to sqrt(3) pi N (or kmax if > 0).
+ * The CIC density is left in GEV_FIELD_SOURCE. */
+int gev_power_spectrum(gev_ctx *ctx, int32_t numbins, double kmax, double *kbin, double *power,
+                       double *kscatter, double *pscatter, int32_t *occupation);
+
+/* Lightcone crossing: the particle branch of writeLightcones
+ * (output.hpp:2093-2160): findIntersectingLightcones (tools.hpp:637) and the
+ * selection, ID-backlog de-duplication and interpolation of
+ * perfParticles_gevolution::saveGadget2 (Particles_gevolution.hpp:1567,
+ * :1271-1466, :500-593).  Outputs Gadget-2 lightcone blocks in float:
+ * pos (Mpc/h), vel (Gadget units), ids.  Each shell keeps its own ID backlog
+ * (lightcone_id_backlog.hpp) inside the context. */
+typedef struct {
+    double vertex[3];     /* box units */
+    double direction[3];
+    double opening;       /* cos of the half opening angle; -1 for the full sky */
+    double distance[2];   /* [outer, inner] limits in box units (metadata.hpp lightcone_geometry) */
+    double d;             /* particleHorizon at the lightcone redshift (output.hpp:1213) */
+    int32_t tracer_factor;
+    int32_t shell;        /* backlog slot, 0..7 */
+} gev_lightcone_args;
+
+int gev_lightcone(gev_ctx *ctx, const gev_lightcone_args *lc, double tau, double dtau,
+                  double dtau_old, double a, double dadtau, int64_t capacity, float *pos,
+                  float *vel, int64_t *ids, int64_t *n_out);
+
+/* One full cycle of main.cu:608-1317 for CDM in the weak-field GR gauge:
+ * T00 and Tij projections, Phi, chi (and h_ij), T0i projection and B_i,
+ * lightcone shells, kick, background half steps, drift, step control.  The
+ * caller's state struct is advanced in place. */
+typedef struct {
+    double Omega_m, Omega_Lambda, Omega_rad;
+    double fourpiG;        /* 1.5 L^2 / c^2 (main.cu:418) */
+    double Cf, steplimit;  /* step control (main.cu:1307-1310) */
+    double z_relax;        /* B enters the geodesic for z < z_relax (main.cu:1232) */
+    double boxsize;
+} gev_cosmo;
+
+typedef struct {
+    double a, tau, dtau, dtau_old;
+    int64_t cycle;
+    double T00hom, phi_hom, maxvel;
+} gev_state;
+
+int gev_step(gev_ctx *ctx, const gev_cosmo *cosmo, gev_state *st);
+
+/* Background (background.hpp:200-207, :235-244, :268-291). */
+double gev_hconf(double a, double fourpiG, const gev_cosmo *cosmo);
+void gev_rungekutta4bg(double *a, double fourpiG, const gev_cosmo *cosmo, double dtau);
+double gev_particle_horizon(double a, double fourpiG, const gev_cosmo *cosmo);
+
+/* Stream and synchronisation helpers for callers that time or overlap work. */
+int gev_synchronize(gev_ctx *ctx);
+void *gev_stream(gev_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

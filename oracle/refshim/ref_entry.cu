@@ -1,0 +1,269 @@
+// ref_entry.cu -- compiles gevolution-2.0's own hot-path sources (gevolution.hpp,
+// background.hpp, tools.hpp, metadata.hpp, taken from the reference tree where
+// they lie) against the single-rank LATfield2 stand-in in this directory, and
+// exposes their host-side arithmetic through plain C entry points.
+//
+// TEST INFRASTRUCTURE ONLY: the result (oracle/_ref/libgevref.so) pins the oracle
+// restatement (oracle/oracle.c) to the reference's own code, and serves as the
+// reference CPU arm of bench.py.  Nothing here is part of the product path.
+//
+// Every entry point takes the same arguments as its orc_* twin in oracle.h.
+#include <cstdint>
+#include <omp.h>
+#include <nvtx3/nvToolsExt.h>
+#include "LATfield2.hpp"
+#include "cuda_staging.hpp"
+#include "metadata.hpp"
+#include "tools.hpp"
+#include "background.hpp"
+#include "gevolution.hpp"
+
+#include <cstdint>
+#include <functional>
+#include <vector>
+
+using namespace LATfield2;
+
+namespace
+{
+
+struct ParticleSet
+{
+	Lattice lat;
+	std::vector<part_simple> parts;
+	perfParticles<part_simple, part_simple_info> pcls;
+
+	ParticleSet(int N, int64_t np, const double * pos, const double * q, double mass) : lat(N, false), parts(np)
+	{
+		for (int64_t p = 0; p < np; p++)
+		{
+			for (int i = 0; i < 3; i++)
+			{
+				parts[p].pos[i] = pos[3 * p + i];
+				parts[p].vel[i] = q ? q[3 * p + i] : 0.;
+			}
+			parts[p].ID = p;
+		}
+		part_simple_info info{};
+		info.mass = mass;
+		pcls.attach(&lat, parts.data(), np, info);
+	}
+};
+
+void site_loop(int N, const std::function<void(int, int, int)> & body)
+{
+#pragma omp parallel for collapse(2) schedule(static)
+	for (int z = 0; z < N; z++)
+		for (int y = 0; y < N; y++)
+			for (int x = 0; x < N; x++) body(x, y, z);
+}
+
+cosmology make_cosmo(double Om, double OL, double Orad)
+{
+	cosmology c;
+	std::memset(&c, 0, sizeof(c));
+	c.Omega_cdm = Om;
+	c.Omega_b = 0.;
+	c.Omega_m = Om;
+	c.Omega_Lambda = OL;
+	c.Omega_rad = Orad;
+	c.num_ncdm = 0;
+	return c;
+}
+
+} // namespace
+
+extern "C" {
+
+// projection_T00_project (gevolution.hpp:1887) through particle_T00_project's host branch
+void ref_project_T00(int N, int64_t np, const double * pos, const double * q, double mass, const double * phi, double a, double coeff, double * T00)
+{
+	ParticleSet ps(N, np, pos, q, mass);
+	Field<Real> fT00(ps.lat, T00, 1), fphi(ps.lat, const_cast<double *>(phi), 1);
+	Field<Real> * fields[2] = {&fT00, phi ? &fphi : nullptr};
+	double params[2] = {a, coeff};
+	ps.pcls.projectParticles(particle_T00_project_functor(), fields, phi ? 2 : 1, params);
+}
+
+// projection_Tij_project (gevolution.hpp:2999) through particle_Tij_project's host branch
+void ref_project_Tij(int N, int64_t np, const double * pos, const double * q, double mass, const double * phi, double a, double coeff, double * Tij)
+{
+	ParticleSet ps(N, np, pos, q, mass);
+	Field<Real> fT(ps.lat, Tij, 6, symmetric), fphi(ps.lat, const_cast<double *>(phi), 1);
+	Field<Real> * fields[2] = {&fT, phi ? &fphi : nullptr};
+	double params[7] = {a, coeff, 0, 0, 0, 0, 0};
+	ps.pcls.projectParticles(particle_Tij_project_functor(), fields, phi ? 2 : 1, params);
+}
+
+// projection_T0i_project (gevolution.hpp:2232) through particle_T0i_project's host branch
+void ref_project_T0i(int N, int64_t np, const double * pos, const double * q, double mass, const double * phi, double coeff, double * T0i)
+{
+	ParticleSet ps(N, np, pos, q, mass);
+	Field<Real> fT(ps.lat, T0i, 3), fphi(ps.lat, const_cast<double *>(phi), 1);
+	Field<Real> * fields[2] = {&fT, phi ? &fphi : nullptr};
+	ps.pcls.projectParticles(particle_T0i_project_functor(), fields, phi ? 2 : 1, &coeff);
+}
+
+// scalarProjectionCIC_project (gevolution.hpp:1902)
+void ref_project_cic(int N, int64_t np, const double * pos, double mass, double * rho)
+{
+	ParticleSet ps(N, np, pos, nullptr, mass);
+	Field<Real> f(ps.lat, rho, 1);
+	scalarProjectionCIC_project(&ps.pcls, &f);
+}
+
+// prepareFTsource_T00 (gevolution.hpp:160-171), applied site by site; returns the sum of source
+double ref_prepare_T00(int N, const double * phi, const double * chi, const double * source, double bgmodel, double coeff, double coeff2, double coeff3, double * result)
+{
+	Lattice lat(N, false);
+	std::vector<double> src(source, source + (size_t) N * N * N);
+	Field<Real> fres(lat, result, 1), fsrc(lat, src.data(), 1), fphi(lat, const_cast<double *>(phi), 1), fchi(lat, const_cast<double *>(chi), 1);
+	Field<Real> * fields[4] = {&fres, &fsrc, &fphi, &fchi};
+	double params[4] = {bgmodel, coeff, coeff2, coeff3};
+	double sum = 0.;
+#pragma omp parallel for collapse(2) reduction(+ : sum) schedule(static)
+	for (int z = 0; z < N; z++)
+		for (int y = 0; y < N; y++)
+			for (int x = 0; x < N; x++)
+			{
+				Site s(lat, x, y, z);
+				Site sites[4] = {s, s, s, s};
+				double out[1];
+				prepareFTsource_T00(fields, sites, 4, params, out);
+				sum += out[0];
+			}
+	return sum;
+}
+
+// prepareFTsource_Tij (gevolution.hpp:64-107), applied site by site
+void ref_prepare_Tij(int N, const double * phi, const double * Tij, double coeff, double * Sij)
+{
+	Lattice lat(N, false);
+	std::vector<double> tij(Tij, Tij + 6 * (size_t) N * N * N);
+	Field<Real> fS(lat, Sij, 6, symmetric), fT(lat, tij.data(), 6, symmetric), fphi(lat, const_cast<double *>(phi), 1);
+	Field<Real> * fields[3] = {&fS, &fT, &fphi};
+	double params = coeff;
+	site_loop(N, [&](int x, int y, int z) {
+		Site s(lat, x, y, z);
+		Site sites[3] = {s, s, s};
+		prepareFTsource_Tij(fields, sites, 3, &params, nullptr);
+	});
+}
+
+// Fourier-space solvers, called unchanged (gevolution.hpp:251-852)
+void ref_solve_poisson(int N, const double * srcFT, double * potFT, double coeff, double modif)
+{
+	Lattice lat(N, true);
+	size_t m = (size_t) (N / 2 + 1) * N * N;
+	std::vector<Imag> src((const Imag *) srcFT, (const Imag *) srcFT + m);
+	Field<Imag> fs(lat, src.data(), 1), fp(lat, (Imag *) potFT, 1);
+	solveModifiedPoissonFT(fs, fp, coeff, modif);
+}
+
+void ref_project_scalar(int N, const double * SijFT, double * chiFT, int add)
+{
+	Lattice lat(N, true);
+	Field<Imag> fS(lat, (Imag *) SijFT, 6, symmetric), fc(lat, (Imag *) chiFT, 1);
+	projectFTscalar(fS, fc, add);
+}
+
+void ref_project_vector(int N, const double * SiFT, double * BiFT, double coeff, double modif)
+{
+	Lattice lat(N, true);
+	size_t m = (size_t) (N / 2 + 1) * N * N;
+	std::vector<Imag> s((const Imag *) SiFT, (const Imag *) SiFT + 3 * m);
+	Field<Imag> fS(lat, s.data(), 3), fB(lat, (Imag *) BiFT, 3);
+	projectFTvector(fS, fB, coeff, modif);
+}
+
+void ref_evolve_vector(int N, const double * SijFT, double * BiFT, double a2dtau)
+{
+	Lattice lat(N, true);
+	Field<Imag> fS(lat, (Imag *) SijFT, 6, symmetric), fB(lat, (Imag *) BiFT, 3);
+	evolveFTvector(fS, fB, a2dtau);
+}
+
+void ref_project_tensor(int N, const double * SijFT, double * hijFT)
+{
+	Lattice lat(N, true);
+	Field<Imag> fS(lat, (Imag *) SijFT, 6, symmetric), fh(lat, (Imag *) hijFT, 6, symmetric);
+	projectFTtensor(fS, fh);
+}
+
+void ref_evolve_tensor(int N, double * SijFT, double * hijFT, double * hijprimeFT, double hubble, double dtau, double dtau_old)
+{
+	Lattice lat(N, true);
+	Field<Imag> fS(lat, (Imag *) SijFT, 6, symmetric), fh(lat, (Imag *) hijFT, 6, symmetric), fhp(lat, (Imag *) hijprimeFT, 6, symmetric);
+	evolveFTtensor(fS, fh, fhp, hubble, dtau, dtau_old);
+}
+
+// update_q (gevolution.hpp:888-1011) through perfParticles::updateVel; returns sqrt(max q^2/a^2)
+double ref_update_q(int N, int64_t np, const double * pos, double * q, const double * phi, const double * chi, const double * Bi, int nfield, double dtau, double a, double bcoeff)
+{
+	ParticleSet ps(N, np, pos, q, 0.);
+	Field<Real> fphi(ps.lat, const_cast<double *>(phi), 1), fchi(ps.lat, const_cast<double *>(chi), 1), fB(ps.lat, const_cast<double *>(Bi), 3);
+	Field<Real> * fields[3] = {&fphi, chi ? &fchi : nullptr, Bi ? &fB : nullptr};
+	double params[7] = {a, bcoeff, 0, 0, 0, 0, 0};
+	double vmax = ps.pcls.updateVel(update_q_functor(), dtau, fields, nfield, params);
+	for (int64_t p = 0; p < np; p++)
+		for (int i = 0; i < 3; i++) q[3 * p + i] = ps.parts[p].vel[i];
+	return vmax;
+}
+
+// update_pos (gevolution.hpp:1162-1232) through perfParticles::moveParticles
+void ref_update_pos(int N, int64_t np, double * pos, const double * q, const double * phi, const double * chi, const double * Bi, int nfield, double dtau, double a, double bcoeff)
+{
+	ParticleSet ps(N, np, pos, q, 0.);
+	Field<Real> fphi(ps.lat, const_cast<double *>(phi), 1), fchi(ps.lat, const_cast<double *>(chi), 1), fB(ps.lat, const_cast<double *>(Bi), 3);
+	Field<Real> * fields[3] = {&fphi, &fchi, &fB};
+	double params[7] = {a, bcoeff, 0, 0, 0, 0, 0};
+	ps.pcls.moveParticles(update_pos_functor(), dtau, fields, nfield, params);
+	for (int64_t p = 0; p < np; p++)
+		for (int i = 0; i < 3; i++) pos[3 * p + i] = ps.parts[p].pos[i];
+}
+
+// background.hpp:200-291
+double ref_hconf(double a, double fourpiG, double Om, double OL, double Orad)
+{
+	return Hconf(a, fourpiG, make_cosmo(Om, OL, Orad));
+}
+
+double ref_rk4bg(double a, double fourpiG, double Om, double OL, double Orad, double dtau)
+{
+	rungekutta4bg(a, fourpiG, make_cosmo(Om, OL, Orad), dtau);
+	return a;
+}
+
+double ref_particle_horizon(double a, double fourpiG, double Om, double OL, double Orad)
+{
+	cosmology c = make_cosmo(Om, OL, Orad);
+	return particleHorizon(a, fourpiG, c);
+}
+
+// extractPowerSpectrum (tools.hpp:339 -> :65-314), deconvolved, linear k
+void ref_power_spectrum(int N, const double * fieldFT, int numbins, double * kbin, double * power, double * kscatter, double * pscatter, int * occupation)
+{
+	Lattice lat(N, true);
+	Field<Imag> f(lat, (Imag *) const_cast<double *>(fieldFT), 1);
+	extractPowerSpectrum(f, kbin, power, kscatter, pscatter, occupation, numbins, true, KTYPE_LINEAR);
+}
+
+// findIntersectingLightcones (tools.hpp:637-886); vertex_out holds MAX_INTERSECTS*3 doubles
+int ref_find_intersecting(const double * lc_vertex, const double * lc_direction, double opening, double outer, double inner, const double * domain, double * vertex_out)
+{
+	lightcone_geometry lc;
+	std::memset(&lc, 0, sizeof(lc));
+	for (int i = 0; i < 3; i++) { lc.vertex[i] = lc_vertex[i]; lc.direction[i] = lc_direction[i]; }
+	lc.opening = opening;
+	double dom[6];
+	for (int i = 0; i < 6; i++) dom[i] = domain[i];
+	double vtx[MAX_INTERSECTS][3];
+	int n = findIntersectingLightcones(lc, outer, inner, dom, vtx);
+	for (int v = 0; v < n && v < MAX_INTERSECTS; v++)
+		for (int i = 0; i < 3; i++) vertex_out[3 * v + i] = vtx[v][i];
+	return n;
+}
+
+int ref_max_intersects(void) { return MAX_INTERSECTS; }
+
+} // extern "C"

@@ -1,0 +1,358 @@
+"""GPU parity: every stage of the cycle through the C ABI against the FP64
+oracle (itself pinned to the reference's own code in test_oracle_pin.py).
+
+Tolerances: FP64 mode 1e-10 relative to the largest magnitude of the compared
+array (the oracle sums in a different order and uses its own FFT); mixed mode
+(FP32 fields and FFTs) 2e-5 for deposits and particle updates and 1e-4 for the
+FFT-based solves."""
+import numpy as np
+import pytest
+
+from _fixtures import particles, rel_err, smooth_field, trough_phi
+from _libs import kshape, oracle, ptr
+
+gev = pytest.importorskip("gevb200")
+
+pytestmark = pytest.mark.gpu
+
+TOL = {gev.FP64: 1e-10, gev.MIXED: 2e-5}
+TOL_FFT = {gev.FP64: 1e-10, gev.MIXED: 1e-4}
+PRECS = [gev.FP64, gev.MIXED]
+MASS = 0.32 / 32768
+
+
+def make_ctx(N, prec, n, **kw):
+    return gev.Context(N, precision=prec, capacity=n, **kw)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("use_phi", [True, False])
+def test_project_T00_Tij(prec, use_phi):
+    N = 32
+    pos, q, ids = particles(N, n=40000, seed=3)
+    phi = trough_phi(N)
+    o = oracle()
+    T00 = np.zeros(N ** 3); Tij = np.zeros(6 * N ** 3)
+    a = 0.37
+    o.project_T00(N, len(pos), ptr(pos), ptr(q), MASS, ptr(phi) if use_phi else None, a, 1.0, ptr(T00))
+    o.project_Tij(N, len(pos), ptr(pos), ptr(q), MASS, ptr(phi) if use_phi else None, a, 1.0, ptr(Tij))
+    with make_ctx(N, prec, len(pos)) as c:
+        c.set_particles(pos, q, ids, MASS)
+        c.set_field(gev.FIELD_PHI, phi)
+        c.project(gev.PROJ_T00 | gev.PROJ_TIJ, a, 1.0, use_phi)
+        g00 = c.get_field(gev.FIELD_SOURCE)
+        gij = c.get_field(gev.FIELD_SIJ)
+        assert rel_err(g00, T00) < TOL[prec]
+        for k in range(6):
+            assert rel_err(gij[k], Tij[k * N ** 3:(k + 1) * N ** 3]) < TOL[prec], k
+        # the separate Tij projection agrees with the fused one (the two kernels may
+        # contract multiply-adds differently, so equality is to rounding, not bits)
+        c.project(gev.PROJ_TIJ, a, 1.0, use_phi)
+        assert rel_err(c.get_field(gev.FIELD_SIJ), gij) < (1e-14 if prec == gev.FP64 else 1e-6)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("use_phi", [True, False])
+def test_project_T0i(prec, use_phi):
+    N = 32
+    pos, q, ids = particles(N, n=40000, seed=4)
+    phi = trough_phi(N)
+    o = oracle()
+    T0i = np.zeros(3 * N ** 3)
+    o.project_T0i(N, len(pos), ptr(pos), ptr(q), MASS, ptr(phi) if use_phi else None, 1.0, ptr(T0i))
+    with make_ctx(N, prec, len(pos)) as c:
+        c.set_particles(pos, q, ids, MASS)
+        c.set_field(gev.FIELD_PHI, phi)
+        c.project(gev.PROJ_T0I, 1.0, 1.0, use_phi)
+        g = c.get_field(gev.FIELD_BI)
+        for k in range(3):
+            assert rel_err(g[k], T0i[k * N ** 3:(k + 1) * N ** 3]) < TOL[prec], k
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_project_cic_mass_and_accumulate(prec):
+    N = 16
+    pos, q, ids = particles(N, n=5000, seed=5)
+    o = oracle()
+    rho = np.zeros(N ** 3)
+    o.project_cic(N, len(pos), ptr(pos), MASS, ptr(rho))
+    with make_ctx(N, prec, len(pos)) as c:
+        c.set_particles(pos, q, ids, MASS)
+        c.project(gev.PROJ_CIC)
+        g = c.get_field(gev.FIELD_SOURCE)
+        assert rel_err(g, rho) < TOL[prec]
+        assert abs(g.sum() / (MASS * len(pos) * N ** 3) - 1) < 1e-6
+        c.project(gev.PROJ_CIC, accumulate=True)
+        assert rel_err(c.get_field(gev.FIELD_SOURCE), 2 * rho) < TOL[prec]
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_deposit_is_order_independent_and_bitwise_reproducible(prec):
+    """The fixed-point tile reduction gives identical bits for any particle order."""
+    N = 32
+    pos, q, ids = particles(N, n=60000, seed=6)
+    phi = trough_phi(N)
+    perm = np.random.default_rng(0).permutation(len(pos))
+    outs = []
+    for p_, q_, i_ in ((pos, q, ids), (pos, q, ids), (pos[perm].copy(), q[perm].copy(), ids[perm].copy())):
+        with make_ctx(N, prec, len(pos)) as c:
+            c.set_particles(p_, q_, i_, MASS)
+            c.set_field(gev.FIELD_PHI, phi)
+            c.project(gev.PROJ_T00 | gev.PROJ_TIJ | gev.PROJ_T0I, 0.5, 1.0, True)
+            outs.append((c.get_field(gev.FIELD_SOURCE), c.get_field(gev.FIELD_SIJ), c.get_field(gev.FIELD_BI)))
+    for other in outs[1:]:
+        for x, y in zip(outs[0], other):
+            assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("N", [16, 32, 64])
+def test_solve_phi(prec, N):
+    o = oracle()
+    dx = 1.0 / N
+    source = 0.32 * (1 + 50 * smooth_field(N, 1))
+    phi = smooth_field(N, 2, 1e-5)
+    chi = smooth_field(N, 3, 1e-6)
+    H, dtau_old, a, fourpiG = 0.8, 0.01, 0.3, 1.5 * 320 ** 2 / 2997.92458 ** 2
+    args = (0.32, 3 * H * dx * dx / dtau_old, fourpiG * dx * dx / a, 3 * H * H * dx * dx)
+    res = np.zeros(N ** 3)
+    s_ref = o.prepare_T00(N, ptr(phi), ptr(chi), ptr(source), *args, ptr(res))
+    FT = np.zeros(kshape(N), dtype=np.complex128)
+    o.r2c(N, ptr(res), ptr(FT))
+    o.solve_poisson(N, ptr(FT), ptr(FT), 1 / (dx * dx), 3 * H / dtau_old)
+    ph_ref = np.zeros(N ** 3)
+    o.c2r(N, ptr(FT), ptr(ph_ref))
+    with make_ctx(N, prec, 8) as c:
+        c.set_particles(np.zeros((1, 3)), np.zeros((1, 3)))
+        c.set_field(gev.FIELD_SOURCE, source)
+        c.set_field(gev.FIELD_PHI, phi)
+        c.set_field(gev.FIELD_CHI, chi)
+        s, phom = c.solve_phi(True, *args, 1 / (dx * dx), 3 * H / dtau_old)
+        assert abs(s / s_ref - 1) < (1e-12 if prec == gev.FP64 else 1e-6)
+        assert abs(phom - FT[0, 0, 0].real) <= TOL_FFT[prec] * abs(FT).max()
+        assert rel_err(c.get_field(gev.FIELD_PHI), ph_ref) < TOL_FFT[prec]
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_fft_round_trip_full_size(prec):
+    """A Poisson solve with modif >> k^2 is the identity up to k^2/modif: the
+    forward + inverse passes reproduce the input at a production grid size."""
+    N = 256
+    f = smooth_field(N, 9, 1.0, kmax=20)
+    with make_ctx(N, prec, 8) as c:
+        c.set_particles(np.zeros((1, 3)), np.zeros((1, 3)))
+        c.set_field(gev.FIELD_SOURCE, f)
+        big = 1e30
+        c.solve_phi(False, 0, 0, 0, 0, -big, big)
+        g = c.get_field(gev.FIELD_PHI)
+        assert rel_err(g, f) < (1e-12 if prec == gev.FP64 else 3e-6)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("N", [16, 32])
+def test_solve_chi(prec, N):
+    o = oracle()
+    dx = 1.0 / N
+    Tij = np.concatenate([smooth_field(N, 10 + k, 1e-3) for k in range(6)])
+    phi = smooth_field(N, 20, 1e-5)
+    coeff = 2 * 0.017 * dx * dx / 0.4
+    S = np.zeros(6 * N ** 3)
+    o.prepare_Tij(N, ptr(phi), ptr(Tij), coeff, ptr(S))
+    SFT = np.zeros((6,) + kshape(N), dtype=np.complex128)
+    for k in range(6):
+        o.r2c(N, ptr(S[k * N ** 3:(k + 1) * N ** 3].copy()), ptr(SFT[k]))
+    chiFT = np.zeros(kshape(N), dtype=np.complex128)
+    o.project_scalar(N, ptr(SFT), ptr(chiFT), 0)
+    chi_ref = np.zeros(N ** 3)
+    o.c2r(N, ptr(chiFT), ptr(chi_ref))
+    with make_ctx(N, prec, 8, tensor=True) as c:
+        c.set_particles(np.zeros((1, 3)), np.zeros((1, 3)))
+        c.set_field(gev.FIELD_SIJ, Tij)
+        c.set_field(gev.FIELD_PHI, phi)
+        c.solve_chi(coeff, cycle0=True)
+        assert rel_err(c.get_field(gev.FIELD_CHI), chi_ref) < TOL_FFT[prec]
+        hFT = np.zeros((6,) + kshape(N), dtype=np.complex128)
+        o.project_tensor(N, ptr(SFT), ptr(hFT))
+        assert rel_err(c.get_field(gev.FIELD_HIJ_FT), hFT) < TOL_FFT[prec]
+        # one evolveFTtensor step on the same source
+        hp = np.zeros_like(hFT)
+        S2 = SFT.copy()
+        o.evolve_tensor(N, ptr(S2), ptr(hFT), ptr(hp), 0.9, 0.01, 0.012)
+        c.solve_chi(coeff, cycle0=False, hubble=0.9, dtau=0.01, dtau_old=0.012)
+        assert rel_err(c.get_field(gev.FIELD_HIJ_FT), hFT) < TOL_FFT[prec]
+        assert rel_err(c.get_field(gev.FIELD_HIJP_FT), hp) < TOL_FFT[prec]
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_solve_chi_parabolic_B(prec):
+    N = 16
+    o = oracle()
+    dx = 1.0 / N
+    Tij = np.concatenate([smooth_field(N, 30 + k, 1e-3) for k in range(6)])
+    phi = smooth_field(N, 40, 1e-5)
+    coeff = 2 * 0.017 * dx * dx / 0.4
+    S = np.zeros(6 * N ** 3)
+    o.prepare_Tij(N, ptr(phi), ptr(Tij), coeff, ptr(S))
+    SFT = np.zeros((6,) + kshape(N), dtype=np.complex128)
+    for k in range(6):
+        o.r2c(N, ptr(S[k * N ** 3:(k + 1) * N ** 3].copy()), ptr(SFT[k]))
+    BFT = np.zeros((3,) + kshape(N), dtype=np.complex128)
+    a2dtau = 0.3 ** 2 * 0.01
+    o.evolve_vector(N, ptr(SFT), ptr(BFT), a2dtau)
+    B_ref = np.zeros(3 * N ** 3)
+    for k in range(3):
+        o.c2r(N, ptr(BFT[k].copy()), ptr(B_ref[k * N ** 3:(k + 1) * N ** 3]))
+    with make_ctx(N, prec, 8, vector_method=gev.VECTOR_PARABOLIC) as c:
+        c.set_particles(np.zeros((1, 3)), np.zeros((1, 3)))
+        c.set_field(gev.FIELD_SIJ, Tij)
+        c.set_field(gev.FIELD_PHI, phi)
+        c.solve_chi(coeff, a2dtau=a2dtau)
+        assert rel_err(c.get_field(gev.FIELD_BI_FT), BFT) < TOL_FFT[prec]
+        assert rel_err(c.get_field(gev.FIELD_BI), B_ref) < TOL_FFT[prec]
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_solve_B(prec):
+    N = 32
+    o = oracle()
+    dx = 1.0 / N
+    T0i = np.concatenate([smooth_field(N, 50 + k, 1e-4) for k in range(3)])
+    FT = np.zeros((3,) + kshape(N), dtype=np.complex128)
+    for k in range(3):
+        o.r2c(N, ptr(T0i[k * N ** 3:(k + 1) * N ** 3].copy()), ptr(FT[k]))
+    coeff = 0.017 * dx * dx
+    o.project_vector(N, ptr(FT), ptr(FT), coeff, 0.0)
+    B_ref = np.zeros(3 * N ** 3)
+    for k in range(3):
+        o.c2r(N, ptr(FT[k].copy()), ptr(B_ref[k * N ** 3:(k + 1) * N ** 3]))
+    with make_ctx(N, prec, 8) as c:
+        c.set_particles(np.zeros((1, 3)), np.zeros((1, 3)))
+        c.set_field(gev.FIELD_BI, T0i)
+        c.solve_B(coeff)
+        assert rel_err(c.get_field(gev.FIELD_BI), B_ref) < TOL_FFT[prec]
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("nfield", [2, 3])
+def test_kick(prec, nfield):
+    N = 32
+    pos, q, ids = particles(N, n=30000, seed=7)
+    phi, chi = trough_phi(N), smooth_field(N, 60, 1e-6)
+    Bi = np.concatenate([smooth_field(N, 61 + k, 1e-7) for k in range(3)])
+    a, dtau = 0.4, 0.02
+    q_ref = q.copy()
+    o = oracle()
+    vmax = o.update_q(N, len(pos), ptr(pos), ptr(q_ref), ptr(phi), ptr(chi), ptr(Bi), nfield, dtau, a, a * a * N)
+    with make_ctx(N, prec, len(pos)) as c:
+        c.set_particles(pos, q, ids, MASS)
+        c.set_field(gev.FIELD_PHI, phi); c.set_field(gev.FIELD_CHI, chi); c.set_field(gev.FIELD_BI, Bi)
+        v = c.kick(dtau, a, a * a * N, nfield)
+        p2, q2, i2 = c.get_particles()
+        order = np.argsort(i2)
+        assert np.array_equal(i2[order], ids)
+        assert rel_err(q2[order], q_ref) < TOL[prec]
+        assert abs(v / vmax - 1) < TOL[prec]
+        assert np.abs(p2[order] - pos).max() < 1e-12
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("nfield", [0, 3])
+def test_drift_and_rebin(prec, nfield):
+    N = 32
+    pos, q, ids = particles(N, n=30000, seed=8, qscale=0.05)
+    phi, chi = trough_phi(N), smooth_field(N, 70, 1e-6)
+    Bi = np.concatenate([smooth_field(N, 71 + k, 1e-7) for k in range(3)])
+    a, dtau = 0.4, 0.1   # moves particles across cells and tiles
+    pos_ref = pos.copy()
+    o = oracle()
+    o.update_pos(N, len(pos), ptr(pos_ref), ptr(q), ptr(phi), ptr(chi), ptr(Bi), nfield, dtau, a, a * a * N)
+    with make_ctx(N, prec, len(pos)) as c:
+        c.set_particles(pos, q, ids, MASS)
+        c.set_field(gev.FIELD_PHI, phi); c.set_field(gev.FIELD_CHI, chi); c.set_field(gev.FIELD_BI, Bi)
+        c.drift(dtau, a, a * a * N, nfield)
+        p2, q2, i2 = c.get_particles()
+        order = np.argsort(i2)
+        d = p2[order] - pos_ref
+        d -= np.round(d)
+        tol = 1e-12 if prec == gev.FP64 else 1e-7
+        assert np.abs(d).max() < tol
+        # after re-binning the deposit still sees every particle exactly once
+        c.project(gev.PROJ_CIC)
+        rho = c.get_field(gev.FIELD_SOURCE)
+        assert abs(rho.sum() / (MASS * len(pos) * N ** 3) - 1) < 1e-6
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_power_spectrum(prec):
+    N = 32
+    pos, q, ids = particles(N, seed=11, lattice=True, disp=0.4)
+    o = oracle()
+    rho = np.zeros(N ** 3)
+    o.project_cic(N, len(pos), ptr(pos), MASS, ptr(rho))
+    FT = np.zeros(kshape(N), dtype=np.complex128)
+    o.r2c(N, ptr(rho), ptr(FT))
+    nb = 64
+    ref = [np.zeros(nb) for _ in range(4)]
+    occ = np.zeros(nb, dtype=np.int32)
+    o.lib.orc_power_spectrum(N, ptr(FT), nb, ptr(ref[0]), ptr(ref[1]), ptr(ref[2]), ptr(ref[3]), ptr(occ), 0.0)
+    with make_ctx(N, prec, len(pos)) as c:
+        c.set_particles(pos, q, ids, MASS)
+        kb, pw, ks, ps, oc = c.power_spectrum(nb)
+        assert np.array_equal(oc, occ)
+        assert rel_err(kb, ref[0]) < 1e-12
+        tol = 1e-9 if prec == gev.FP64 else 1e-4
+        assert rel_err(pw, ref[1]) < tol
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_step_matches_oracle(prec):
+    """Three full cycles of main.cu's loop against the oracle's orc_step."""
+    import ctypes
+    from _libs import _d, _i, _l  # noqa: F401
+    N = 32
+    pos, q, ids = particles(N, seed=12, lattice=True, disp=0.2, qscale=2e-4)
+    mass = 0.32 / len(pos)
+    fourpiG = 1.5 * 320.0 ** 2 / 2997.92458 ** 2
+    phi = trough_phi(N, 1e-6)
+    chi = np.zeros(N ** 3)
+    Bi = np.zeros(3 * N ** 3)
+    o = oracle()
+
+    class OSim(ctypes.Structure):
+        _fields_ = [("N", ctypes.c_int), ("boxsize", ctypes.c_double), ("fourpiG", ctypes.c_double),
+                    ("mass", ctypes.c_double), ("Om", ctypes.c_double), ("OL", ctypes.c_double),
+                    ("Orad", ctypes.c_double), ("z_relax", ctypes.c_double), ("Cf", ctypes.c_double),
+                    ("steplimit", ctypes.c_double), ("with_B", ctypes.c_int)]
+
+    class OState(ctypes.Structure):
+        _fields_ = [("a", ctypes.c_double), ("tau", ctypes.c_double), ("dtau", ctypes.c_double),
+                    ("dtau_old", ctypes.c_double), ("cycle", ctypes.c_int), ("T00hom", ctypes.c_double),
+                    ("phi_hom", ctypes.c_double), ("maxvel", ctypes.c_double)]
+
+    o.lib.orc_step.argtypes = [ctypes.POINTER(OSim), ctypes.POINTER(OState), ctypes.c_int64] + [ctypes.c_void_p] * 5
+    o.lib.orc_step.restype = None
+    sim = OSim(N, 320.0, fourpiG, mass, 0.32, 0.68, 0.0, 30.0, 48.0, 0.04, 1)
+    a0 = 1.0 / 51
+    cosmo = gev.Cosmo(0.32, 0.68, 0.0, fourpiG, 48.0, 0.04, 30.0, 320.0)
+    H = gev.hconf(a0, fourpiG, ctypes.byref(cosmo))
+    dtau0 = min(48.0 / N, 0.04 / H)
+    ost = OState(a0, 0.1, dtau0, 0.0, 0, 0, 0, 0)
+    gst = gev.State(a0, 0.1, dtau0, 0.0, 0, 0, 0, 0)
+    p_ref, q_ref = pos.copy(), q.copy()
+    with make_ctx(N, prec, len(pos)) as c:
+        c.set_particles(pos, q, ids, mass)
+        c.set_field(gev.FIELD_PHI, phi)
+        for _ in range(3):
+            o.lib.orc_step(ctypes.byref(sim), ctypes.byref(ost), len(pos), ptr(p_ref), ptr(q_ref), ptr(phi), ptr(chi), ptr(Bi))
+            c.step(cosmo, gst)
+        assert abs(gst.a / ost.a - 1) < 1e-14
+        assert abs(gst.maxvel / ost.maxvel - 1) < (1e-8 if prec == gev.FP64 else 1e-4)
+        assert abs(gst.T00hom / ost.T00hom - 1) < (1e-10 if prec == gev.FP64 else 1e-6)
+        assert rel_err(c.get_field(gev.FIELD_PHI), phi) < (1e-8 if prec == gev.FP64 else 1e-3)
+        assert rel_err(c.get_field(gev.FIELD_CHI), chi) < (1e-6 if prec == gev.FP64 else 2e-2)
+        p2, q2, i2 = c.get_particles()
+        order = np.argsort(i2)
+        d = p2[order] - p_ref
+        d -= np.round(d)
+        assert np.abs(d).max() * N < (1e-8 if prec == gev.FP64 else 1e-4)
+        assert rel_err(q2[order], q_ref) < (1e-7 if prec == gev.FP64 else 1e-3)

@@ -1,0 +1,215 @@
+"""Pin the oracle: every orc_* restatement against the reference's own source
+code compiled on the CPU (oracle/_ref/libgevref.so, built from the reference
+tree by oracle/Makefile with the single-rank LATfield2 stand-in), and the
+oracle FFT against numpy.  CPU only."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from _fixtures import particles, rel_err, smooth_field, trough_phi
+from _libs import OrcCosmo, kshape, oracle, ptr, ref
+
+MASS = 1e-3
+
+
+@pytest.fixture(scope="module")
+def libs():
+    r = ref()
+    if r is None:
+        pytest.skip("reference CPU build (oracle/_ref) not built here")
+    return oracle(), r
+
+
+@pytest.mark.parametrize("N", [8, 16, 24])
+def test_fft_matches_numpy(N):
+    o = oracle()
+    f = np.random.default_rng(N).normal(size=N ** 3)
+    FT = np.zeros(kshape(N), dtype=np.complex128)
+    o.r2c(N, ptr(f), ptr(FT))
+    ref_ft = np.fft.rfftn(f.reshape(N, N, N))
+    assert np.abs(FT - ref_ft).max() < 1e-10 * np.abs(ref_ft).max()
+    back = np.zeros(N ** 3)
+    o.c2r(N, ptr(FT), ptr(back))
+    assert rel_err(back, f * N ** 3) < 1e-12
+
+
+@pytest.mark.parametrize("N", [8, 12])
+def test_c2r_of_non_hermitian_input(N):
+    """C2R convention for spectra that are not exactly Hermitian: inverse along
+    z and y, then the x transform keeps only the real parts of the kx = 0 and
+    kx = N/2 entries -- numpy's irfftn does the same."""
+    o = oracle()
+    rng = np.random.default_rng(N)
+    FT = np.ascontiguousarray(rng.normal(size=kshape(N)) + 1j * rng.normal(size=kshape(N)))
+    a = np.zeros(N ** 3)
+    o.c2r(N, ptr(FT), ptr(a))
+    b = np.fft.irfftn(FT, s=(N, N, N), axes=(0, 1, 2)) * N ** 3
+    assert rel_err(a, b) < 1e-12
+
+
+@pytest.mark.parametrize("use_phi", [True, False])
+def test_projections_match_reference(libs, use_phi):
+    o, r = libs
+    N = 16
+    pos, q, _ = particles(N, n=3000, seed=1)
+    phi = trough_phi(N) if use_phi else None
+    for name, nc, args in (("T00", 1, (0.3, 1.0)), ("Tij", 6, (0.3, 1.0)), ("T0i", 3, (1.0,))):
+        A = np.zeros(nc * N ** 3); B = np.zeros(nc * N ** 3)
+        getattr(o, "project_" + name)(N, len(pos), ptr(pos), ptr(q), MASS, ptr(phi), *args, ptr(A))
+        getattr(r, "project_" + name)(N, len(pos), ptr(pos), ptr(q), MASS, ptr(phi), *args, ptr(B))
+        assert rel_err(A, B) < 1e-14, name
+    A = np.zeros(N ** 3); B = np.zeros(N ** 3)
+    o.project_cic(N, len(pos), ptr(pos), MASS, ptr(A))
+    r.project_cic(N, len(pos), ptr(pos), MASS, ptr(B))
+    assert rel_err(A, B) < 1e-14
+
+
+def test_particles_on_cell_edges(libs):
+    """Positions exactly on lattice points and at 1 - eps (edge cases of the cell assignment)."""
+    o, r = libs
+    N = 16
+    pos = np.array([[0, 0, 0], [0.5, 0.25, 0.75], [1 - 1e-16, 0.9999999, 1e-17], [3 / 16, 5 / 16, 15 / 16]], dtype=float)
+    q = np.full_like(pos, 0.01)
+    phi = trough_phi(N)
+    for name, nc in (("T00", 1), ("Tij", 6)):
+        A = np.zeros(nc * N ** 3); B = np.zeros(nc * N ** 3)
+        getattr(o, "project_" + name)(N, len(pos), ptr(pos), ptr(q), MASS, ptr(phi), 0.3, 1.0, ptr(A))
+        getattr(r, "project_" + name)(N, len(pos), ptr(pos), ptr(q), MASS, ptr(phi), 0.3, 1.0, ptr(B))
+        assert rel_err(A, B) < 1e-14
+
+
+def test_prepare_sources_match_reference(libs):
+    o, r = libs
+    N = 16
+    phi, chi = smooth_field(N, 1, 1e-4), smooth_field(N, 2, 1e-5)
+    src = 0.3 + smooth_field(N, 3, 1e-2)
+    A = np.zeros(N ** 3); B = np.zeros(N ** 3)
+    sa = o.prepare_T00(N, ptr(phi), ptr(chi), ptr(src), 0.3, 0.1, 0.2, 0.3, ptr(A))
+    sb = r.prepare_T00(N, ptr(phi), ptr(chi), ptr(src), 0.3, 0.1, 0.2, 0.3, ptr(B))
+    assert abs(sa / sb - 1) < 1e-14 and rel_err(A, B) < 1e-14
+    Tij = np.concatenate([smooth_field(N, 10 + k, 1e-3) for k in range(6)])
+    A = np.zeros(6 * N ** 3); B = np.zeros(6 * N ** 3)
+    o.prepare_Tij(N, ptr(phi), ptr(Tij), 0.7, ptr(A))
+    r.prepare_Tij(N, ptr(phi), ptr(Tij), 0.7, ptr(B))
+    assert rel_err(A, B) < 1e-14
+
+
+def _spectrum(N, ncomp, seed):
+    rng = np.random.default_rng(seed)
+    return np.ascontiguousarray(rng.normal(size=(ncomp,) + kshape(N)) + 1j * rng.normal(size=(ncomp,) + kshape(N)))
+
+
+@pytest.mark.parametrize("N", [8, 16])
+def test_fourier_solvers_match_reference(libs, N):
+    o, r = libs
+    S6 = _spectrum(N, 6, 1)
+    S3 = _spectrum(N, 3, 2)
+    for modif in (0.0, 3.0):
+        A = np.zeros(kshape(N), dtype=complex); B = np.zeros(kshape(N), dtype=complex)
+        o.solve_poisson(N, ptr(S6[0]), ptr(A), 2.5, modif)
+        r.solve_poisson(N, ptr(S6[0]), ptr(B), 2.5, modif)
+        assert rel_err(A.view(float), B.view(float)) < 1e-13
+    for add in (0, 1):
+        A = _spectrum(N, 1, 9)[0]; B = A.copy()
+        o.project_scalar(N, ptr(S6), ptr(A), add)
+        r.project_scalar(N, ptr(S6), ptr(B), add)
+        assert rel_err(A.view(float), B.view(float)) < 1e-13
+    A = np.zeros((3,) + kshape(N), dtype=complex); B = A.copy()
+    o.project_vector(N, ptr(S3), ptr(A), 1.7, 0.0)
+    r.project_vector(N, ptr(S3), ptr(B), 1.7, 0.0)
+    assert rel_err(A.view(float), B.view(float)) < 1e-13
+    A = _spectrum(N, 3, 4); B = A.copy()
+    o.evolve_vector(N, ptr(S6), ptr(A), 0.03)
+    r.evolve_vector(N, ptr(S6), ptr(B), 0.03)
+    assert rel_err(A.view(float), B.view(float)) < 1e-13
+    A = np.zeros((6,) + kshape(N), dtype=complex); B = A.copy()
+    o.project_tensor(N, ptr(S6), ptr(A))
+    r.project_tensor(N, ptr(S6), ptr(B))
+    assert rel_err(A.view(float), B.view(float)) < 1e-13
+    for dtau in (0.01, 3.0):   # both branches of k^2 dtau^2 < 1
+        h1, hp1 = _spectrum(N, 6, 5), _spectrum(N, 6, 6)
+        h2, hp2 = h1.copy(), hp1.copy()
+        s1, s2 = S6.copy(), S6.copy()
+        o.evolve_tensor(N, ptr(s1), ptr(h1), ptr(hp1), 0.8, dtau, 0.9 * dtau)
+        r.evolve_tensor(N, ptr(s2), ptr(h2), ptr(hp2), 0.8, dtau, 0.9 * dtau)
+        for x, y in ((h1, h2), (hp1, hp2), (s1, s2)):
+            assert rel_err(x.view(float), y.view(float)) < 1e-13
+
+
+@pytest.mark.parametrize("nfield", [1, 2, 3])
+def test_kick_drift_match_reference(libs, nfield):
+    o, r = libs
+    N = 16
+    pos, q, _ = particles(N, n=2000, seed=3)
+    phi, chi = trough_phi(N), smooth_field(N, 4, 1e-5)
+    Bi = np.concatenate([smooth_field(N, 5 + k, 1e-6) for k in range(3)])
+    qa, qb = q.copy(), q.copy()
+    va = o.update_q(N, len(pos), ptr(pos), ptr(qa), ptr(phi), ptr(chi), ptr(Bi), max(nfield, 1), 0.05, 0.3, 0.09 * N)
+    vb = r.update_q(N, len(pos), ptr(pos), ptr(qb), ptr(phi), ptr(chi), ptr(Bi), max(nfield, 1), 0.05, 0.3, 0.09 * N)
+    assert abs(va / vb - 1) < 1e-14 and rel_err(qa, qb) < 1e-14
+    for nf in (0, nfield):
+        pa, pb = pos.copy(), pos.copy()
+        o.update_pos(N, len(pos), ptr(pa), ptr(q), ptr(phi), ptr(chi), ptr(Bi), nf, 0.3, 0.3, 0.09 * N)
+        r.update_pos(N, len(pos), ptr(pb), ptr(q), ptr(phi), ptr(chi), ptr(Bi), nf, 0.3, 0.3, 0.09 * N)
+        d = pa - pb
+        d -= np.round(d)
+        assert np.abs(d).max() < 1e-15
+
+
+def test_background_matches_reference(libs):
+    o, r = libs
+    c = OrcCosmo(0.32, 0.68, 8.5e-5)
+    o.lib.orc_rk4bg.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.c_void_p, ctypes.c_double]
+    for a in (0.01, 0.3, 1.0):
+        fourpiG = 1.5 * 1280.0 ** 2 / 2997.92458 ** 2
+        h1 = o.hconf(a, fourpiG, ctypes.byref(c))
+        h2 = r.hconf(a, fourpiG, 0.32, 0.68, 8.5e-5)
+        assert abs(h1 / h2 - 1) < 1e-15
+        x = ctypes.c_double(a)
+        o.lib.orc_rk4bg(ctypes.byref(x), fourpiG, ctypes.byref(c), 0.01)
+        assert abs(x.value / r.rk4bg(a, fourpiG, 0.32, 0.68, 8.5e-5, 0.01) - 1) < 1e-15
+        t1 = o.particle_horizon(a, fourpiG, ctypes.byref(c))
+        t2 = r.particle_horizon(a, fourpiG, 0.32, 0.68, 8.5e-5)
+        assert abs(t1 / t2 - 1) < 1e-10
+
+
+def test_power_spectrum_matches_reference(libs):
+    o, r = libs
+    N = 16
+    pos, _, _ = particles(N, seed=7, lattice=True, disp=0.4)
+    rho = np.zeros(N ** 3)
+    o.project_cic(N, len(pos), ptr(pos), MASS, ptr(rho))
+    FT = np.zeros(kshape(N), dtype=complex)
+    o.r2c(N, ptr(rho), ptr(FT))
+    nb = 40
+    a = [np.zeros(nb) for _ in range(4)]; oa = np.zeros(nb, dtype=np.int32)
+    b = [np.zeros(nb) for _ in range(4)]; ob = np.zeros(nb, dtype=np.int32)
+    o.lib.orc_power_spectrum(N, ptr(FT), nb, *[ptr(x) for x in a], ptr(oa), 0.0)
+    r.power_spectrum(N, ptr(FT), nb, *[ptr(x) for x in b], ptr(ob))
+    assert np.array_equal(oa, ob)
+    assert rel_err(a[0], b[0]) < 1e-12 and rel_err(a[1], b[1]) < 1e-12
+    # the scatters are sqrt(<x^2> - <x>^2): cancellation leaves roundoff-level noise
+    # in bins where every mode has the same |k|
+    assert rel_err(a[2], b[2]) < 1e-6 and rel_err(a[3], b[3]) < 1e-6
+
+
+@pytest.mark.parametrize("opening", [-1.0, 0.7])
+def test_find_intersecting_matches_reference(libs, opening):
+    o, r = libs
+    N = 32
+    domain = np.array([-0.5 / N] * 3 + [(N + 0.5) / N] * 3)
+    d = np.array([0.6, 0.8, 0.0])
+    for vtx, outer, inner in (([0, 0, 0], 0.75, 0.7), ([0.3, 0.2, 0.9], 1.4, 1.3), ([0.5, 0.5, 0.5], 0.3, 0.25)):
+        vtx = np.asarray(vtx, dtype=float)
+        va = np.zeros(3 * 64); vb = np.zeros(3 * 64)
+        o.lib.orc_find_intersecting.argtypes = [ctypes.c_void_p] * 2 + [ctypes.c_double] * 3 + [ctypes.c_void_p] * 2
+        na = o.lib.orc_find_intersecting(ptr(vtx), ptr(d), opening, outer, inner, ptr(domain), ptr(va))
+        nb = r.find_intersecting(ptr(vtx), ptr(d), opening, outer, inner, ptr(domain), ptr(vb))
+        if nb >= r.max_intersects():
+            # the reference truncates at MAX_INTERSECTS in thread order; the oracle keeps more
+            assert na >= nb
+            continue
+        assert na == nb
+        sa = sorted(map(tuple, va[:3 * na].reshape(-1, 3))); sb = sorted(map(tuple, vb[:3 * nb].reshape(-1, 3)))
+        assert sa == sb
