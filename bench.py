@@ -1,0 +1,443 @@
+#!/usr/bin/env python
+"""bench.py -- throughput of gevolution-2.0's per-step particle-mesh cycle on B200.
+
+Workload (default): box 2560 Mpc/h, grid 512^3, 512^3 particles, mixed
+precision (FP32 fields and FFTs; particle positions as cell index + FP64
+offset; FP64 background and reductions), GR weak-field gauge, elliptic B, one
+full-sky lightcone shell (vertex at the box corner, 0.5-1.0 box lengths) that is
+active in every timed cycle.  Seeded Zel'dovich initial conditions at z = 100
+(Eisenstein-Hu no-wiggle P(k), A_s = 2.1e-9, n_s = 0.965, h = 0.67,
+Omega_m = 0.32).  One "step" is one cycle of main.cu's loop: T00/Tij projection,
+Phi, chi, T0i projection, B, lightcone, kick, drift, background, step control.
+
+Metric: Mpart-steps/s = particles x cycles / second (whole job: all ranks).
+Multi-GPU (torchrun): every rank evolves its own independent box (replicas;
+the single-box cycle has no data-parallel split in this build) -> weak scaling.
+
+--impl reference times the CPU restatement of the reference cycle (the oracle,
+OpenMP over all host cores) on a bounded sample of the same physics.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gevolution-2.0_b200", "python"))
+
+OMEGA_M, OMEGA_L, H_LITTLE = 0.32, 0.68, 0.67
+C_LIGHT = 2997.92458
+T_START = time.time()
+
+
+def log(msg):
+    print("[bench %7.1fs] %s" % (time.time() - T_START, msg), file=sys.stderr, flush=True)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--N", type=int, default=512)
+    p.add_argument("--boxsize", type=float, default=None, help="Mpc/h (default: 5 Mpc/h per cell)")
+    p.add_argument("--z-in", type=float, default=100.0)
+    p.add_argument("--seed", type=int, default=42)
+    p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--cpu-sample-N", type=int, default=128)
+    p.add_argument("--cpu-sample-steps", type=int, default=2)
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region (nvidia-smi, 200 ms)
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def lightcone_args(gev, d):
+    """Full-sky shell, vertex at the box corner, comoving radius 0.5-1.0 box lengths."""
+    return gev.LightconeArgs((0.0, 0.0, 0.0), (1.0 / math.sqrt(3),) * 3, -1.0, (1.0, 0.5), d, 1, 0)
+
+
+def run_gpu(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    import gevb200 as gev
+    from gevb200 import roofline
+    from gevb200.ics import zeldovich
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    N = args.N
+    box = args.boxsize or 5.0 * N
+    np_ = N ** 3
+    log("initial conditions %d^3" % N)
+    pos_t, q_t, ids_t, phi_t, mass, a0, fourpiG = zeldovich(N, box, args.z_in, args.seed + 1000 * rank, device=dev)
+    log("initial conditions done")
+    # host copies in pinned memory: the C ABI takes host buffers
+    pos_h = pos_t.cpu().pin_memory().numpy()
+    q_h = q_t.cpu().pin_memory().numpy()
+    ids_h = ids_t.cpu().pin_memory().numpy()
+    phi_h = phi_t.cpu().numpy()
+    del pos_t, q_t, ids_t, phi_t
+    torch.cuda.empty_cache()
+
+    z_relax = args.z_in
+    cosmo = gev.Cosmo(OMEGA_M, OMEGA_L, 0.0, fourpiG, 48.0, 0.04, z_relax, box)
+    H = gev.hconf(a0, fourpiG, ctypes.byref(cosmo))
+    dtau0 = min(48.0 / N, 0.04 / H)
+    tau0 = gev.particle_horizon(a0, fourpiG, ctypes.byref(cosmo))
+    d_lc = tau0 + 0.75   # the shell's crossing surface sits at 0.75 box lengths during the timed cycles
+    lc = lightcone_args(gev, d_lc)
+    lc_cap = int(0.2 * np_)
+
+    def make(precision):
+        c = gev.Context(N, precision=precision, capacity=np_, boxsize=box, vector_method=gev.VECTOR_ELLIPTIC, device=local_rank)
+        c.set_particles(pos_h, q_h, ids_h, mass)
+        c.set_field(gev.FIELD_PHI, phi_h)
+        return c
+
+    def cycle(c, st):
+        """One cycle of main.cu's loop with the lightcone between the solves and the kick."""
+        a = st.a
+        Hc = gev.hconf(a, fourpiG, ctypes.byref(cosmo))
+        c.lightcone(lc, st.tau, st.dtau, st.dtau_old, a, a * Hc, lc_cap, fetch=False)
+        c.step(cosmo, st)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def timed_run(precision, steps, warmup):
+        log("context (%s)" % ("fp64" if precision == gev.FP64 else "mixed"))
+        c = make(precision)
+        st = gev.State(a0, tau0, dtau0, 0.0, 0, 0.0, 0.0, 0.0)
+        stream = torch.cuda.ExternalStream(c.stream())
+        log("warm-up")
+        for _ in range(warmup):
+            cycle(c, st)
+        c.synchronize()
+        log("timed cycles")
+        clocks = Clocks(local_rank)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        clocks.start()
+        l0 = c.kernel_launches()
+        e0.record(stream)
+        for _ in range(steps):
+            cycle(c, st)
+        e1.record(stream)
+        e1.synchronize()
+        launches = c.kernel_launches() - l0
+        clk = clocks.stop()
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        return c, st, ms, launches, clk, stream
+
+    # ---- mixed precision: the headline ----
+    c, st, ms, launches, clk, stream = timed_run(gev.MIXED, args.steps, args.warmup)
+    t = torch.tensor([ms], device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * np_ * args.steps / (ms_max * 1e-3) / 1e6
+
+    # ---- per-stage breakdown on the final state (CUDA events on the context stream) ----
+    log("mixed: %.3f ms/cycle; stage breakdown" % (ms_max / args.steps))
+    stages = {}
+
+    def stage(name, fn, reps=5):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fn()
+        c.synchronize()
+        ev0.record(stream)
+        for _ in range(reps):
+            fn()
+        ev1.record(stream)
+        ev1.synchronize()
+        stages[name] = ev0.elapsed_time(ev1) / reps
+
+    a = st.a
+    dx = 1.0 / N
+    Hc = gev.hconf(a, fourpiG, ctypes.byref(cosmo))
+    stage("deposit_T00_Tij", lambda: c.project(gev.PROJ_T00 | gev.PROJ_TIJ, a, 1.0, True))
+    stage("solve_phi", lambda: c.solve_phi(True, OMEGA_M, 3 * Hc * dx * dx / st.dtau_old, fourpiG * dx * dx / a,
+                                           3 * Hc * Hc * dx * dx, 1 / (dx * dx), 3 * Hc / st.dtau_old))
+    stage("solve_chi", lambda: c.solve_chi(2 * fourpiG * dx * dx / a))
+    stage("deposit_T0i", lambda: c.project(gev.PROJ_T0I, a, 1.0, True))
+    stage("solve_B", lambda: c.solve_B(fourpiG * dx * dx))
+    stage("kick_drift", lambda: c.kick_drift(0.0, a, a * a * N, 3, 0.0, a, a * a * N, 3))
+    stage("lightcone", lambda: c.lightcone(lc, st.tau, st.dtau, st.dtau_old, a, a * Hc, lc_cap, fetch=False))
+
+    peak, peak_kind = measured_peaks()
+    dom = max((s for s in stages if s != "lightcone"), key=lambda s: stages[s])
+    dom_bytes = roofline.stage_bytes(dom, N, "mixed")
+    achieved = dom_bytes / (stages[dom] * 1e-3) / 1e9
+    step_alg = roofline.step_bytes(N, "mixed")
+    step_gbs = step_alg / (ms_max / args.steps * 1e-3) / 1e9
+
+    # ---- validation: P(k) of the mixed run vs an FP64 run from the same ICs ----
+    log("stages %s" % json.dumps(stages))
+    pk_mixed = c.power_spectrum(1024)
+    c.close()
+    del c
+    fp64 = None
+    if not args.no_fp64:
+        c64, st64, ms64, _, _, _ = timed_run(gev.FP64, args.steps, args.warmup)
+        pk64 = c64.power_spectrum(1024)
+        occ = pk64[4] > 0
+        kb = pk64[0][occ]
+        kny = math.pi * N
+        sel = kb < 0.5 * kny
+        rel = np.abs(pk_mixed[1][occ][sel] / pk64[1][occ][sel] - 1)
+        fp64 = {"value": np_ * args.steps / (ms64 * 1e-3) / 1e6, "ms_per_step": ms64 / args.steps,
+                "mixed_speedup": (np_ * args.steps / (ms_max * 1e-3)) / (np_ * args.steps / (ms64 * 1e-3)),
+                "pk_max_rel_err_vs_fp64": float(rel.max()), "pk_k_range_h_per_mpc": [float(kb[sel].min() / box), float(kb[sel].max() / box)],
+                "cycles_compared": args.warmup + args.steps}
+        c64.close()
+        del c64
+
+    # ---- e2e: the same cycles through the C ABI with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        log("e2e")
+        c = make(gev.MIXED)
+        st = gev.State(a0, tau0, dtau0, 0.0, 0, 0.0, 0.0, 0.0)
+        cycle(c, st)                          # warm-up
+        pos_o = torch.empty(pos_h.shape, dtype=torch.float64).pin_memory().numpy()
+        q_o = torch.empty(q_h.shape, dtype=torch.float64).pin_memory().numpy()
+        ids_o = torch.empty(ids_h.shape, dtype=torch.int64).pin_memory().numpy()
+        pos_i, q_i, ids_i = pos_h, q_h, ids_h
+        pin = torch.empty((lc_cap, 3), dtype=torch.float32).pin_memory().numpy()
+        pinv = torch.empty((lc_cap, 3), dtype=torch.float32).pin_memory().numpy()
+        pini = torch.empty(lc_cap, dtype=torch.int64).pin_memory().numpy()
+        lib = gev._lib
+        stream = torch.cuda.ExternalStream(c.stream())
+        barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        n = ctypes.c_int64()
+        lc_bytes = 0
+        for _ in range(args.e2e_steps):
+            c.set_particles(pos_i, q_i, ids_i, mass)           # H2D of the cycle's particle state
+            cycle(c, st)
+            lib.gev_lightcone_fetch(c.handle, lc_cap, pin.ctypes.data_as(ctypes.c_void_p), pinv.ctypes.data_as(ctypes.c_void_p),
+                                    pini.ctypes.data_as(ctypes.c_void_p), ctypes.byref(n))
+            lc_bytes += n.value * 32
+            lib.gev_particles_get(c.handle, pos_o.ctypes.data_as(ctypes.c_void_p), q_o.ctypes.data_as(ctypes.c_void_p),
+                                  ids_o.ctypes.data_as(ctypes.c_void_p), np_, ctypes.byref(n))
+            # the state read back is the next cycle's input (the first input was the initial conditions)
+            pos_i, pos_o, q_i, q_o, ids_i, ids_o = pos_o, pos_i, q_o, q_i, ids_o, ids_i
+        ev1.record(stream)
+        ev1.synchronize()
+        ms_e2e = ev0.elapsed_time(ev1)
+        t = torch.tensor([ms_e2e], device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+        e2e = {"value": world * np_ * args.e2e_steps / (ms_e2e * 1e-3) / 1e6, "unit": "Mpart-steps/s",
+               "h2d_bytes_per_step": int(np_ * 56), "d2h_bytes_per_step": int(np_ * 56 + lc_bytes // max(args.e2e_steps, 1)),
+               "steps": args.e2e_steps}
+        c.close()
+
+    # ---- CPU baseline: the oracle on a bounded sample, rank 0 only ----
+    cpu = None
+    if rank == 0 and world == 1:
+        log("cpu baseline")
+        cpu = cpu_sample(args)
+
+    if rank == 0:
+        line = {
+            "metric": "Mpart-steps/s at 512^3 (mixed vs FP64 GPU, P(k) err<1e-4); grad/fwd ratio",
+            "value": value, "unit": "Mpart-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 fields/FFT + f64 particle offsets, background and reductions",
+            "data": "synthetic: seeded Zel'dovich ICs (EH no-wiggle P(k)) at z=%g" % args.z_in,
+            "config": {"workload": "PM cycle, box %g Mpc/h, grid %d^3, %d^3 particles, mixed precision, GR, elliptic B, "
+                                   "full-sky lightcone shell 0.5-1.0 box lengths" % (box, N, N),
+                       "N": N, "particles": np_, "boxsize_mpc_h": box, "parallelism": "replicas" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (particles %.1f GB, fields %.1f GB)" % (np_ * 48 / 1e9, N ** 3 * 12 * 4 / 1e9)},
+            "gpu_launches": launches,
+            "stage_ms": stages,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "algorithmic_bytes_per_launch": dom_bytes,
+                         "step_algorithmic_bytes": step_alg, "step_achieved_gbs": step_gbs, "step_frac": step_gbs / peak},
+            "clocks": clk,
+            "fp64": fp64,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# CPU: the oracle cycle (OpenMP, all host cores) on a bounded sample
+# ---------------------------------------------------------------------------
+def oracle_cycle_rate(Ns, steps, seed):
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from _libs import oracle, ptr
+    from _fixtures import particles, trough_phi
+
+    o = oracle()
+
+    class OSim(ctypes.Structure):
+        _fields_ = [("N", ctypes.c_int), ("boxsize", ctypes.c_double), ("fourpiG", ctypes.c_double),
+                    ("mass", ctypes.c_double), ("Om", ctypes.c_double), ("OL", ctypes.c_double),
+                    ("Orad", ctypes.c_double), ("z_relax", ctypes.c_double), ("Cf", ctypes.c_double),
+                    ("steplimit", ctypes.c_double), ("with_B", ctypes.c_int)]
+
+    class OState(ctypes.Structure):
+        _fields_ = [("a", ctypes.c_double), ("tau", ctypes.c_double), ("dtau", ctypes.c_double),
+                    ("dtau_old", ctypes.c_double), ("cycle", ctypes.c_int), ("T00hom", ctypes.c_double),
+                    ("phi_hom", ctypes.c_double), ("maxvel", ctypes.c_double)]
+
+    o.lib.orc_step.argtypes = [ctypes.POINTER(OSim), ctypes.POINTER(OState), ctypes.c_int64] + [ctypes.c_void_p] * 5
+    o.lib.orc_step.restype = None
+    box = 5.0 * Ns
+    fourpiG = 1.5 * box * box / C_LIGHT ** 2
+    pos, q, ids = particles(Ns, seed=seed, lattice=True, disp=0.2, qscale=2e-4)
+    phi = trough_phi(Ns, 1e-6)
+    chi = np.zeros(Ns ** 3)
+    Bi = np.zeros(3 * Ns ** 3)
+    sim = OSim(Ns, box, fourpiG, OMEGA_M / Ns ** 3, OMEGA_M, OMEGA_L, 0.0, 100.0, 48.0, 0.04, 1)
+    a0 = 1.0 / 101
+    H = math.sqrt((2 * fourpiG / 3) * (OMEGA_M / a0 + OMEGA_L * a0 * a0))
+    st = OState(a0, 0.1, min(48.0 / Ns, 0.04 / H), 0.0, 0, 0, 0, 0)
+    o.lib.orc_step(ctypes.byref(sim), ctypes.byref(st), len(pos), ptr(pos), ptr(q), ptr(phi), ptr(chi), ptr(Bi))   # warm-up
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.lib.orc_step(ctypes.byref(sim), ctypes.byref(st), len(pos), ptr(pos), ptr(q), ptr(phi), ptr(chi), ptr(Bi))
+    dt = time.perf_counter() - t0
+    return Ns ** 3 * steps / dt / 1e6, dt
+
+
+def cpu_sample(args):
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    rate, dt = oracle_cycle_rate(args.cpu_sample_N, args.cpu_sample_steps, args.seed)
+    return {"value": rate, "unit": "Mpart-steps/s", "cores": int(os.environ.get("OMP_NUM_THREADS", cores)),
+            "kind": "port",
+            "sample": "%d cycles of the FP64 oracle cycle (orc_step) on a %d^3 box with %d^3 particles, %.1f s"
+                      % (args.cpu_sample_steps, args.cpu_sample_N, args.cpu_sample_N, dt)}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    Ns = args.cpu_sample_N
+    rate, dt = oracle_cycle_rate(Ns, max(1, min(args.steps, 3)), args.seed)
+    line = {"impl": "reference", "metric": "Mpart-steps/s at 512^3 (mixed vs FP64 GPU, P(k) err<1e-4); grad/fwd ratio",
+            "value": rate, "unit": "Mpart-steps/s", "n_gpus": args.gpus, "steps": max(1, min(args.steps, 3)),
+            "warmup": 1, "ms_per_step": dt / max(1, min(args.steps, 3)) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded perturbed lattice",
+            "config": {"workload": "PM cycle sample: box %g Mpc/h, grid %d^3, %d^3 particles (same physics and cell size as "
+                                   "the 512^3 workload)" % (5.0 * Ns, Ns, Ns), "N": Ns},
+            "cpu_baseline": {"value": rate, "unit": "Mpart-steps/s", "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
+                             "sample": "FP64 oracle cycle, %d^3, %.1f s" % (Ns, dt)},
+            "e2e": {"value": rate, "unit": "Mpart-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                             device_id=torch.device("cuda", local_rank))
+    try:
+        run_gpu(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

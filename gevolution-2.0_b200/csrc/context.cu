@@ -174,8 +174,10 @@ struct CtxBase {
     virtual void power_spectrum(int nb, double kmax, double *kb, double *pw, double *ks, double *ps, int32_t *occ) = 0;
     virtual void lightcone(const gev_lightcone_args &lc, double tau, double dtau, double dtau_old, double a, double dadtau,
                            int64_t cap, float *pos, float *vel, int64_t *ids, int64_t *n_out) = 0;
+    virtual void fetch_lightcone(int64_t cap, float *pos, float *vel, int64_t *ids, int64_t *n_out) = 0;
     virtual void sync() = 0;
     virtual cudaStream_t stream() = 0;
+    virtual int64_t kernel_launches() const = 0;
 };
 
 template <class R> struct Ctx final : CtxBase {
@@ -199,10 +201,14 @@ template <class R> struct Ctx final : CtxBase {
     DBuf<double> stage;                  // particle / field transfer staging
     DBuf<int64_t> stage_id;
     DBuf<float> lc_pos, lc_vel;
-    DBuf<int64_t> lc_id, prelog;
-    DBuf<int64_t> backlog[8];
-    int64_t backlog_n[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    DBuf<int64_t> lc_id;
+    DBuf<unsigned long long> idset[8][2];   // per shell: ID logs of the previous and current cycle
+    int idset_cur[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    bool backlog_valid[8] = {false, false, false, false, false, false, false, false};
+    int64_t idset_cap = 0;
+    int64_t lc_last = 0;
     bool cur_is_A = true;
+    int64_t launch_count = 0;
     int64_t np = 0;
     double mass = 0.0;
     bool have_particles = false;
@@ -308,7 +314,13 @@ template <class R> struct Ctx final : CtxBase {
     }
     PView<R> cur() const { return view(cur_is_A); }
 
-    void launched(const char *what) { ck(cudaGetLastError(), what); }
+    // every kernel launch of the library goes through here (count = kernels launched)
+    void launched(const char *what, int kernels = 1)
+    {
+        ck(cudaGetLastError(), what);
+        launch_count += kernels;
+    }
+    int64_t kernel_launches() const override { return launch_count; }
 
     void check_device_error()
     {
@@ -350,7 +362,7 @@ template <class R> struct Ctx final : CtxBase {
     {
         const int64_t nb = g.ntiles * 8;
         launch_scan(counts.p, bstart.p, nb, bsums.p, st);
-        launched("scan");
+        launched("scan", 3);
         launch_scatter<R>(cur(), view(!cur_is_A), bstart.p, bucket.p, rank.p, st);
         launched("scatter");
         cur_is_A = !cur_is_A;
@@ -667,7 +679,8 @@ template <class R> struct Ctx final : CtxBase {
         *n_out = 0;
         // output condition, output.hpp:2093
         if (!(lc.distance[0] > dist + 0.5 * dtau_old && lc.distance[1] <= dist + 0.5 * dtau_old && dist + 0.5 * dtau_old > 0.)) {
-            backlog_n[s] = 0;   // the reference clears the backlog every cycle (output.hpp:2172)
+            backlog_valid[s] = false;   // the reference clears the backlog every cycle (output.hpp:2172)
+            lc_last = 0;
             return;
         }
         LcKernelArgs la{};
@@ -682,40 +695,50 @@ template <class R> struct Ctx final : CtxBase {
         la.opening = lc.opening;
         la.dtau = dtau; la.dtau_old = dtau_old; la.a = a; la.dadtau = dadtau; la.boxsize = cfg.boxsize;
         la.tracer_factor = lc.tracer_factor > 0 ? lc.tracer_factor : 1;
-        la.backlog = backlog[s].p;
-        la.backlog_n = backlog_n[s];
+        // ID sets: capacity a power of two >= np/4 (the log holds particles within
+        // 0.1 dtau of the inner edge, a small fraction of the box)
+        if (idset_cap == 0) {
+            int64_t c = 1 << 16;
+            while (c < np / 4) c <<= 1;
+            idset_cap = c;
+        }
+        for (int b = 0; b < 2; b++)
+            if (!idset[s][b].p) {
+                idset[s][b].alloc(idset_cap, "lightcone ID log");
+                ck(cudaMemsetAsync(idset[s][b].p, 0xff, idset_cap * sizeof(unsigned long long), st), "memset");
+            }
+        unsigned long long *older = idset[s][idset_cur[s]].p, *newer = idset[s][1 - idset_cur[s]].p;
+        la.backlog = older;
+        la.backlog_cap = backlog_valid[s] ? idset_cap : 0;
+        ck(cudaMemsetAsync(newer, 0xff, idset_cap * sizeof(unsigned long long), st), "memset");
         const int64_t lcap = std::max<int64_t>(cap, 1);
         la.capacity = lcap;
         if ((int64_t)lc_id.n < lcap) { lc_pos.alloc(3 * lcap, "lightcone"); lc_vel.alloc(3 * lcap, "lightcone"); lc_id.alloc(lcap, "lightcone"); }
-        const int64_t pcap = std::max<int64_t>(np / 8, 1024);
-        if ((int64_t)prelog.n < pcap) prelog.alloc(pcap, "lightcone log");
-        ck(cudaMemsetAsync(u64.p + 1, 0, 2 * sizeof(unsigned long long), st), "memset");
-        launch_lightcone<R>(cur(), N, phi.p, la, lc_pos.p, lc_vel.p, lc_id.p, u64.p + 1, prelog.p, u64.p + 2, (int64_t)prelog.n,
-                            derr.p, st);
+        ck(cudaMemsetAsync(u64.p + 1, 0, sizeof(unsigned long long), st), "memset");
+        launch_lightcone<R>(cur(), N, phi.p, la, lc_pos.p, lc_vel.p, lc_id.p, u64.p + 1, newer, idset_cap, derr.p, st);
         launched("lightcone");
-        unsigned long long cnt[2];
-        ck(cudaMemcpyAsync(cnt, u64.p + 1, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st), "D2H");
-        ck(cudaStreamSynchronize(st), "synchronize");
-        *n_out = (int64_t)cnt[0];
-        if ((int64_t)cnt[0] > cap || (int64_t)cnt[1] > (int64_t)prelog.n) {
-            ck(cudaMemsetAsync(derr.p, 0, sizeof(int), st), "memset");
-            throw CapacityError("lightcone output exceeds the buffer capacity (n_out holds the required size)");
-        }
-        const int64_t n = (int64_t)cnt[0];
-        if (n > 0) {
-            ck(cudaMemcpyAsync(pos, lc_pos.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, st), "D2H");
-            ck(cudaMemcpyAsync(vel, lc_vel.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, st), "D2H");
-            ck(cudaMemcpyAsync(ids, lc_id.p, n * sizeof(int64_t), cudaMemcpyDeviceToHost, st), "D2H");
-        }
-        // the IDs logged near the inner edge become the next cycle's backlog (sorted, unique)
-        std::vector<int64_t> lg((size_t)cnt[1]);
-        if (cnt[1]) ck(cudaMemcpyAsync(lg.data(), prelog.p, cnt[1] * sizeof(int64_t), cudaMemcpyDeviceToHost, st), "D2H");
+        // the IDs logged near the inner edge become the next cycle's backlog
+        idset_cur[s] = 1 - idset_cur[s];
+        backlog_valid[s] = true;
+        unsigned long long cnt = 0;
+        ck(cudaMemcpyAsync(&cnt, u64.p + 1, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st), "D2H");
         sync();
-        std::sort(lg.begin(), lg.end());
-        lg.erase(std::unique(lg.begin(), lg.end()), lg.end());
-        if ((int64_t)backlog[s].n < (int64_t)lg.size()) backlog[s].alloc(std::max<size_t>(lg.size(), 1024), "backlog");
-        if (!lg.empty()) ck(cudaMemcpyAsync(backlog[s].p, lg.data(), lg.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st), "H2D");
-        backlog_n[s] = (int64_t)lg.size();
+        *n_out = (int64_t)cnt;
+        lc_last = (int64_t)cnt;
+        if ((int64_t)cnt > lcap) throw CapacityError("lightcone output exceeds the buffer capacity (n_out holds the required size)");
+        if (pos || vel || ids) fetch_lightcone(cap, pos, vel, ids, n_out);
+    }
+
+    void fetch_lightcone(int64_t cap, float *pos, float *vel, int64_t *ids, int64_t *n_out) override
+    {
+        *n_out = lc_last;
+        if (lc_last > cap) throw CapacityError("host arrays smaller than the lightcone output");
+        const int64_t n = lc_last;
+        if (n > 0) {
+            if (pos) ck(cudaMemcpyAsync(pos, lc_pos.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, st), "D2H");
+            if (vel) ck(cudaMemcpyAsync(vel, lc_vel.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, st), "D2H");
+            if (ids) ck(cudaMemcpyAsync(ids, lc_id.p, n * sizeof(int64_t), cudaMemcpyDeviceToHost, st), "D2H");
+        }
         ck(cudaStreamSynchronize(st), "synchronize");
     }
 };
@@ -908,8 +931,14 @@ int gev_power_spectrum(gev_ctx *ctx, int32_t numbins, double kmax, double *kbin,
 int gev_lightcone(gev_ctx *ctx, const gev_lightcone_args *lc, double tau, double dtau, double dtau_old, double a,
                   double dadtau, int64_t capacity, float *pos, float *vel, int64_t *ids, int64_t *n_out)
 {
-    if (!lc || !n_out || (capacity > 0 && (!pos || !vel || !ids))) return fail(ctx, GEV_ERR_ARG, "null argument");
+    if (!lc || !n_out || capacity < 0) return fail(ctx, GEV_ERR_ARG, "null argument");
     return guarded(ctx, [&](gev::CtxBase &c) { c.lightcone(*lc, tau, dtau, dtau_old, a, dadtau, capacity, pos, vel, ids, n_out); });
+}
+
+int gev_lightcone_fetch(gev_ctx *ctx, int64_t capacity, float *pos, float *vel, int64_t *ids, int64_t *n_out)
+{
+    if (!n_out) return fail(ctx, GEV_ERR_ARG, "null argument");
+    return guarded(ctx, [&](gev::CtxBase &c) { c.fetch_lightcone(capacity, pos, vel, ids, n_out); });
 }
 
 double gev_hconf(double a, double fourpiG, const gev_cosmo *cosmo) { return gev::hconf(a, fourpiG, *cosmo); }
@@ -977,5 +1006,7 @@ int gev_synchronize(gev_ctx *ctx)
 }
 
 void *gev_stream(gev_ctx *ctx) { return (ctx && ctx->impl) ? (void *)ctx->impl->stream() : nullptr; }
+
+int64_t gev_kernel_launches(const gev_ctx *ctx) { return (ctx && ctx->impl) ? ctx->impl->kernel_launches() : -1; }
 
 }  // extern "C"

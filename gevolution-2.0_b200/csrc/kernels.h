@@ -88,13 +88,15 @@ struct LcKernelArgs {
     double inner, outer, dist;
     double dtau, dtau_old, a, dadtau, boxsize;
     int tracer_factor;
-    const int64_t *backlog;
-    int64_t backlog_n;
-    int64_t capacity;
+    const unsigned long long *backlog;   // ID set of the previous cycle (hash table)
+    int64_t backlog_cap;                 // power of two (0: empty)
+    int64_t capacity;                    // output slots
 };
+constexpr unsigned long long LC_EMPTY = ~0ull;   // free slot of an ID set (tables are filled with 0xff bytes)
+constexpr int64_t LC_MAX_PROBES = 4096;          // bound on linear probing (load factor stays below 1/4)
 template <class R>
 void launch_lightcone(const PView<R> &p, int N, const R *phi, const LcKernelArgs &la, float *pos, float *vel,
-                      int64_t *ids, unsigned long long *count, int64_t *prelog, unsigned long long *prelog_count,
-                      int64_t prelog_cap, int *err, cudaStream_t st);
+                      int64_t *ids, unsigned long long *count, unsigned long long *newlog, int64_t newlog_cap, int *err,
+                      cudaStream_t st);
 
 }  // namespace gev

@@ -6,9 +6,15 @@
 // of the vertex, the ID-backlog de-duplication of the check zone
 // (count_lightcone_duplicate_ids / mark_lightcone_kept_particles, :1468-1510),
 // the interpolation to the crossing time (bufferTracerParticle with
-// EXACT_OUTPUT_REDSHIFTS, :500-560) and the logging of IDs near the inner
-// edge for the next cycle's backlog.  Slots come from one atomic counter; the
-// output order is not significant (the reference's is not either).
+// EXACT_OUTPUT_REDSHIFTS, :500-560) and the logging of IDs near the inner edge
+// for the next cycle.
+//
+// The ID logs are open-addressing hash sets in device memory (keys are particle
+// IDs, EMPTY marks a free slot): membership is a set property, so the result
+// does not depend on insertion order, and no host sort of the log is needed
+// (the reference sorts its backlog, lightcone_id_backlog.hpp:58-70, for binary
+// search).  Output slots come from one atomic counter; the output order is not
+// significant (the reference's is not either).
 #include "common.cuh"
 #include "kernels.h"
 #include "particles.cuh"
@@ -18,15 +24,40 @@ namespace gev {
 constexpr double LC_IDCHECK_ZONE = 0.05;            // metadata.hpp:38-40
 constexpr double LC_GADGET_VEL = 3.335640952e-6;    // GADGET_VELOCITY_CONVERSION, metadata.hpp
 
-__device__ __forceinline__ bool backlog_contains(const int64_t *b, int64_t n, int64_t id)
+__device__ __forceinline__ uint64_t mix64(uint64_t x)
 {
-    int64_t lo = 0, hi = n;
-    while (lo < hi) {
-        int64_t mid = lo + (hi - lo) / 2;
-        if (b[mid] < id) lo = mid + 1;
-        else hi = mid;
+    // splitmix64 finaliser
+    x ^= x >> 30; x *= 0xbf58476d1ce4e5b9ull;
+    x ^= x >> 27; x *= 0x94d049bb133111ebull;
+    x ^= x >> 31;
+    return x;
+}
+
+__device__ __forceinline__ bool idset_contains(const unsigned long long *tab, int64_t cap, int64_t id)
+{
+    if (cap <= 0) return false;
+    uint64_t h = mix64((uint64_t)id) & (uint64_t)(cap - 1);
+    const int64_t maxp = cap < LC_MAX_PROBES ? cap : LC_MAX_PROBES;
+    for (int64_t probe = 0; probe < maxp; probe++) {
+        unsigned long long k = tab[h];
+        if (k == (unsigned long long)id) return true;
+        if (k == LC_EMPTY) return false;
+        h = (h + 1) & (uint64_t)(cap - 1);
     }
-    return lo < n && b[lo] == id;
+    return false;
+}
+
+// returns false when the table is full
+__device__ __forceinline__ bool idset_insert(unsigned long long *tab, int64_t cap, int64_t id)
+{
+    uint64_t h = mix64((uint64_t)id) & (uint64_t)(cap - 1);
+    const int64_t maxp = cap < LC_MAX_PROBES ? cap : LC_MAX_PROBES;
+    for (int64_t probe = 0; probe < maxp; probe++) {
+        unsigned long long prev = atomicCAS(&tab[h], LC_EMPTY, (unsigned long long)id);
+        if (prev == LC_EMPTY || prev == (unsigned long long)id) return true;
+        h = (h + 1) & (uint64_t)(cap - 1);
+    }
+    return false;
 }
 
 template <class R>
@@ -37,8 +68,8 @@ __device__ __forceinline__ double gphi(const R *phi, int N, int x, int y, int z)
 
 template <class R>
 __global__ void k_lightcone(PView<R> p, int N, const R *__restrict__ phi, LcKernelArgs la, float *opos, float *ovel,
-                            int64_t *oid, unsigned long long *count, int64_t *prelog,
-                            unsigned long long *prelog_count, int64_t prelog_cap, int *err)
+                            int64_t *oid, unsigned long long *count, unsigned long long *newlog, int64_t newlog_cap,
+                            int *err)
 {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= p.n) return;
@@ -59,7 +90,7 @@ __global__ void k_lightcone(PView<R> p, int N, const R *__restrict__ phi, LcKern
         if (!(la.opening == -1. || (r[0] * la.direction[0] + r[1] * la.direction[1] + r[2] * la.direction[2]) / d > la.opening)) continue;
 
         // check zone near the outer edge: drop IDs written in the previous cycle
-        if (la.outer - d <= 2. * LC_IDCHECK_ZONE * la.dtau_old && backlog_contains(la.backlog, la.backlog_n, id)) return;
+        if (la.outer - d <= 2. * LC_IDCHECK_ZONE * la.dtau_old && idset_contains(la.backlog, la.backlog_cap, id)) return;
 
         double vlos = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + la.a * (la.a + la.dtau_old * la.dadtau));
         vlos = (q[0] * r[0] + q[1] * r[1] + q[2] * r[2]) / d / vlos;
@@ -70,16 +101,13 @@ __global__ void k_lightcone(PView<R> p, int N, const R *__restrict__ phi, LcKern
         // bufferTracerParticle (EXACT_OUTPUT_REDSHIFTS)
         double phip = 0., g[3] = {0., 0., 0.};
         if (phi) {
-            double w[8];
+            double w[8], P[8];
 #pragma unroll
-            for (int k = 0; k < 8; k++)
+            for (int k = 0; k < 8; k++) {
                 w[k] = (((k >> 2) & 1) ? fr[0] : 1. - fr[0]) * (((k >> 1) & 1) ? fr[1] : 1. - fr[1]) * ((k & 1) ? fr[2] : 1. - fr[2]);
-            double P[8];
-#pragma unroll
-            for (int k = 0; k < 8; k++) P[k] = gphi(phi, N, c[0] + ((k >> 2) & 1), c[1] + ((k >> 1) & 1), c[2] + (k & 1));
-#pragma unroll
-            for (int k = 0; k < 8; k++) phip += w[k] * P[k];
-            // P[4bx+2by+bz]
+                P[k] = gphi(phi, N, c[0] + ((k >> 2) & 1), c[1] + ((k >> 1) & 1), c[2] + (k & 1));   // P[4bx+2by+bz]
+                phip += w[k] * P[k];
+            }
             g[0] = (1 - fr[1]) * (1 - fr[2]) * (P[4] - P[0]) + fr[1] * (1 - fr[2]) * (P[6] - P[2]) + (1 - fr[1]) * fr[2] * (P[5] - P[1]) + fr[1] * fr[2] * (P[7] - P[3]);
             g[1] = (1 - fr[0]) * (1 - fr[2]) * (P[2] - P[0]) + fr[0] * (1 - fr[2]) * (P[6] - P[4]) + (1 - fr[0]) * fr[2] * (P[3] - P[1]) + fr[0] * fr[2] * (P[7] - P[5]);
             g[2] = (1 - fr[0]) * (1 - fr[1]) * (P[1] - P[0]) + fr[0] * (1 - fr[1]) * (P[5] - P[4]) + (1 - fr[0]) * fr[1] * (P[3] - P[2]) + fr[0] * fr[1] * (P[7] - P[6]);
@@ -98,13 +126,9 @@ __global__ void k_lightcone(PView<R> p, int N, const R *__restrict__ phi, LcKern
                 ovel[3 * slot + k] = (float)((q[k] - dtau_vel * f0 * g[k] * (double)N / f2) * rescale_vel) / (float)at;
             }
             oid[slot] = id;
-        } else {
-            atomicOr(err, ERR_LC_OVERFLOW);
         }
         if (d - la.inner < 2. * LC_IDCHECK_ZONE * la.dtau) {
-            unsigned long long ls = atomicAdd(prelog_count, 1ull);
-            if (ls < (unsigned long long)prelog_cap) prelog[ls] = id;
-            else atomicOr(err, ERR_LC_OVERFLOW);
+            if (!idset_insert(newlog, newlog_cap, id)) atomicOr(err, ERR_LC_OVERFLOW);
         }
         return;
     }
@@ -112,19 +136,17 @@ __global__ void k_lightcone(PView<R> p, int N, const R *__restrict__ phi, LcKern
 
 template <class R>
 void launch_lightcone(const PView<R> &p, int N, const R *phi, const LcKernelArgs &la, float *pos, float *vel,
-                      int64_t *ids, unsigned long long *count, int64_t *prelog, unsigned long long *prelog_count,
-                      int64_t prelog_cap, int *err, cudaStream_t st)
+                      int64_t *ids, unsigned long long *count, unsigned long long *newlog, int64_t newlog_cap, int *err,
+                      cudaStream_t st)
 {
     if (p.n > 0)
-        k_lightcone<R><<<cdiv(p.n, 256), 256, 0, st>>>(p, N, phi, la, pos, vel, ids, count, prelog, prelog_count,
-                                                      prelog_cap, err);
+        k_lightcone<R><<<cdiv(p.n, 256), 256, 0, st>>>(p, N, phi, la, pos, vel, ids, count, newlog, newlog_cap, err);
 }
 
 template void launch_lightcone<float>(const PView<float> &, int, const float *, const LcKernelArgs &, float *, float *,
-                                      int64_t *, unsigned long long *, int64_t *, unsigned long long *, int64_t, int *,
-                                      cudaStream_t);
+                                      int64_t *, unsigned long long *, unsigned long long *, int64_t, int *, cudaStream_t);
 template void launch_lightcone<double>(const PView<double> &, int, const double *, const LcKernelArgs &, float *,
-                                       float *, int64_t *, unsigned long long *, int64_t *, unsigned long long *,
-                                       int64_t, int *, cudaStream_t);
+                                       float *, int64_t *, unsigned long long *, unsigned long long *, int64_t, int *,
+                                       cudaStream_t);
 
 }  // namespace gev

@@ -85,9 +85,11 @@ _drift = _sig("gev_drift", [_p, _d, _d, _d, _i])
 _kick_drift = _sig("gev_kick_drift", [_p, _d, _d, _d, _i, _d, _d, _d, _i, ctypes.POINTER(_d)])
 _pk = _sig("gev_power_spectrum", [_p, _i, _d, _p, _p, _p, _p, _p])
 _lc = _sig("gev_lightcone", [_p, ctypes.POINTER(LightconeArgs), _d, _d, _d, _d, _d, _l, _p, _p, _p, ctypes.POINTER(_l)])
+_lcf = _sig("gev_lightcone_fetch", [_p, _l, _p, _p, _p, ctypes.POINTER(_l)])
 _step = _sig("gev_step", [_p, ctypes.POINTER(Cosmo), ctypes.POINTER(State)])
 _sync = _sig("gev_synchronize", [_p])
 _stream = _sig("gev_stream", [_p], _p)
+_launches = _sig("gev_kernel_launches", [_p], _l)
 hconf = _sig("gev_hconf", [_d, _d, ctypes.POINTER(Cosmo)], _d)
 particle_horizon = _sig("gev_particle_horizon", [_d, _d, ctypes.POINTER(Cosmo)], _d)
 _rk4 = _sig("gev_rungekutta4bg", [ctypes.POINTER(_d), _d, ctypes.POINTER(Cosmo), _d], None)
@@ -160,6 +162,10 @@ class Context:
     def synchronize(self):
         self._ck(_sync(self._h))
 
+    def kernel_launches(self):
+        """Number of kernels this context has launched (the library's own kernels)."""
+        return int(_launches(self._h))
+
     # ---- particles ----
     def set_particles(self, pos, q, ids=None, mass=1.0):
         pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
@@ -229,13 +235,27 @@ class Context:
         self._ck(_pk(self._h, int(numbins), float(kmax), _ptr(kb), _ptr(pw), _ptr(ks), _ptr(ps), _ptr(oc)))
         return kb, pw, ks, ps, oc
 
-    def lightcone(self, args, tau, dtau, dtau_old, a, dadtau, capacity):
+    def lightcone(self, args, tau, dtau, dtau_old, a, dadtau, capacity, fetch=True):
+        """Selects the shell's crossing particles; returns (pos, vel, ids) host
+        arrays, or the count alone when fetch is False (data stays on the device)."""
+        n = _l()
+        if not fetch:
+            self._ck(_lc(self._h, ctypes.byref(args), tau, dtau, dtau_old, a, dadtau, int(capacity), None, None, None,
+                         ctypes.byref(n)))
+            return n.value
+        pos = np.empty((max(capacity, 1), 3), dtype=np.float32)
+        vel = np.empty((max(capacity, 1), 3), dtype=np.float32)
+        ids = np.empty(max(capacity, 1), dtype=np.int64)
+        self._ck(_lc(self._h, ctypes.byref(args), tau, dtau, dtau_old, a, dadtau, int(capacity), _ptr(pos), _ptr(vel),
+                     _ptr(ids), ctypes.byref(n)))
+        return pos[:n.value], vel[:n.value], ids[:n.value]
+
+    def lightcone_fetch(self, capacity):
         pos = np.empty((max(capacity, 1), 3), dtype=np.float32)
         vel = np.empty((max(capacity, 1), 3), dtype=np.float32)
         ids = np.empty(max(capacity, 1), dtype=np.int64)
         n = _l()
-        self._ck(_lc(self._h, ctypes.byref(args), tau, dtau, dtau_old, a, dadtau, int(capacity), _ptr(pos), _ptr(vel),
-                     _ptr(ids), ctypes.byref(n)))
+        self._ck(_lcf(self._h, int(capacity), _ptr(pos), _ptr(vel), _ptr(ids), ctypes.byref(n)))
         return pos[:n.value], vel[:n.value], ids[:n.value]
 
     def step(self, cosmo, state):

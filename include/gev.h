@@ -164,7 +164,11 @@ int gev_power_spectrum(gev_ctx *ctx, int32_t numbins, double kmax, double *kbin,
  * perfParticles_gevolution::saveGadget2 (Particles_gevolution.hpp:1567,
  * :1271-1466, :500-593).  Outputs Gadget-2 lightcone blocks in float:
  * pos (Mpc/h), vel (Gadget units), ids.  Each shell keeps its own ID backlog
- * (lightcone_id_backlog.hpp) inside the context. */
+ * (lightcone_id_backlog.hpp) inside the context, as a device hash set; particle
+ * ID -1 is reserved.  The selected particles stay in a device buffer of
+ * `capacity` slots; pos/vel/ids may be NULL to leave them there (copy them
+ * later with gev_lightcone_fetch).  n_out receives the number selected; more
+ * than `capacity` fails with GEV_ERR_CAPACITY and n_out the size needed. */
 typedef struct {
     double vertex[3];     /* box units */
     double direction[3];
@@ -178,6 +182,10 @@ typedef struct {
 int gev_lightcone(gev_ctx *ctx, const gev_lightcone_args *lc, double tau, double dtau,
                   double dtau_old, double a, double dadtau, int64_t capacity, float *pos,
                   float *vel, int64_t *ids, int64_t *n_out);
+/* Copy the last gev_lightcone result to host arrays of `capacity` particles
+ * (the host side of saveGadget2's write, Particles_gevolution.hpp:1567). */
+int gev_lightcone_fetch(gev_ctx *ctx, int64_t capacity, float *pos, float *vel, int64_t *ids,
+                        int64_t *n_out);
 
 /* One full cycle of main.cu:608-1317 for CDM in the weak-field GR gauge:
  * T00 and Tij projections, Phi, chi (and h_ij), T0i projection and B_i,
@@ -204,9 +212,11 @@ double gev_hconf(double a, double fourpiG, const gev_cosmo *cosmo);
 void gev_rungekutta4bg(double *a, double fourpiG, const gev_cosmo *cosmo, double dtau);
 double gev_particle_horizon(double a, double fourpiG, const gev_cosmo *cosmo);
 
-/* Stream and synchronisation helpers for callers that time or overlap work. */
+/* Stream and synchronisation helpers for callers that time or overlap work.
+ * gev_kernel_launches counts the kernels this context has launched so far. */
 int gev_synchronize(gev_ctx *ctx);
 void *gev_stream(gev_ctx *ctx);
+int64_t gev_kernel_launches(const gev_ctx *ctx);
 
 #ifdef __cplusplus
 }

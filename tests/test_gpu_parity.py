@@ -305,6 +305,65 @@ def test_power_spectrum(prec):
 
 
 @pytest.mark.parametrize("prec", PRECS)
+def test_lightcone_selection_and_backlog(prec):
+    """Two consecutive cycles of one full-sky shell: selection and interpolated
+    output against the oracle, and the ID-backlog de-duplication of the check
+    zone in the second cycle (particles logged near the inner edge in cycle 1
+    are not written again near the outer edge in cycle 2)."""
+    import ctypes
+    from _libs import _d, _l, _p  # noqa: F401
+    N = 32
+    pos, q, ids = particles(N, seed=21, lattice=True, disp=0.45, qscale=1e-3)
+    phi = trough_phi(N, 1e-5)
+    o = oracle()
+    o.lib.orc_lightcone_select.argtypes = [ctypes.c_int, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_double] * 5 + \
+                                          [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]
+    o.lib.orc_lightcone_select.restype = ctypes.c_int64
+
+    class OLc(ctypes.Structure):
+        _fields_ = [("vertex", ctypes.c_double * 3), ("direction", ctypes.c_double * 3), ("opening", ctypes.c_double),
+                    ("dist_lo", ctypes.c_double), ("dist_hi", ctypes.c_double)]
+
+    vtx = np.array([0.5, 0.5, 0.5])
+    d_h, a, dadtau, box = 1.3, 0.5, 0.4, 320.0
+    dtau = dtau_old = 0.02
+    cap = 20000
+    lc = gev.LightconeArgs((0.5, 0.5, 0.5), (1.0, 0.0, 0.0), -1.0, (0.45, 0.1), d_h, 1, 0)
+    results = []
+    with make_ctx(N, prec, len(pos), boxsize=box) as c:
+        c.set_particles(pos, q, ids, MASS)
+        c.set_field(gev.FIELD_PHI, phi)
+        for tau in (1.0, 1.0 + dtau):
+            results.append(c.lightcone(lc, tau, dtau, dtau_old, a, dadtau, cap))
+    log1 = set()
+    r = np.sqrt(((pos - vtx) ** 2).sum(axis=1))
+    for cyc, tau in enumerate((1.0, 1.0 + dtau)):
+        dist = d_h - tau
+        ol = OLc((0.5, 0.5, 0.5), (1.0, 0.0, 0.0), -1.0, 0.0, dist)
+        op = np.zeros((cap, 3), dtype=np.float32); ov = np.zeros((cap, 3), dtype=np.float32); oi = np.zeros(cap, dtype=np.int64)
+        n = o.lib.orc_lightcone_select(N, len(pos), ptr(pos), ptr(q), ptr(ids), ptr(phi), ctypes.byref(ol), tau, dtau,
+                                       dtau_old, a, dadtau, cap, ptr(op), ptr(ov), ptr(oi), box)
+        inner, outer = dist - 0.5 * dtau, dist + 0.55 * dtau_old
+        sel = (r >= inner) & (r < outer)
+        assert n == sel.sum() and n > 100
+        keep = np.ones(n, dtype=bool)
+        if cyc == 1:
+            rid = dict(zip(ids, r))
+            check = np.array([outer - rid[i] <= 0.1 * dtau_old for i in oi[:n]])
+            dup = np.array([i in log1 for i in oi[:n]])
+            keep = ~(check & dup)
+            assert (check & dup).sum() > 0
+        log1 = set(ids[sel & (r - inner < 0.1 * dtau)])
+        gp, gv, gi = results[cyc]
+        order_g, order_o = np.argsort(gi), np.argsort(oi[:n][keep])
+        assert np.array_equal(gi[order_g], oi[:n][keep][order_o])
+        tol = 1e-6 if prec == gev.FP64 else 1e-4
+        assert rel_err(gp[order_g], op[:n][keep][order_o]) < tol
+        assert rel_err(gv[order_g], ov[:n][keep][order_o]) < tol
+
+
+@pytest.mark.parametrize("prec", PRECS)
 def test_step_matches_oracle(prec):
     """Three full cycles of main.cu's loop against the oracle's orc_step."""
     import ctypes
