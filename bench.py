@@ -52,6 +52,7 @@ def parse():
     p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--cpu-sample-N", type=int, default=128)
     p.add_argument("--cpu-sample-steps", type=int, default=2)
     return p.parse_args()
@@ -314,7 +315,7 @@ def run_gpu(args, rank, world, local_rank):
 
     # ---- CPU baseline: the oracle on a bounded sample, rank 0 only ----
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_cpu:
         log("cpu baseline")
         cpu = cpu_sample(args)
 

@@ -1,16 +1,25 @@
 // deposit.cu -- deterministic tile deposits of T00, Tij and T0i.
 //
-// One CTA owns the 8^3 vertices of a tile and gathers every particle whose CIC
-// stencil touches them: its own 8 class buckets plus the face-class buckets of
-// the 7 lower neighbour tiles (tile_segments).  Contributions are accumulated
-// in shared memory as 64-bit fixed point with a per-CTA, per-component scale
-// chosen from the exact maximum contribution (first pass) and the particle
-// count, so the sum is exact integer arithmetic: the result does not depend on
-// particle order or thread scheduling (bitwise reproducible), and each output
-// vertex is written exactly once with plain stores -- no global atomics and no
-// halo fold (projection_comm1, gevolution.hpp:1543, is not needed on one GPU).
+// One CTA owns the 8^3 vertices of a tile, one thread per vertex, and gathers
+// every particle whose CIC stencil touches them: its own 8 class buckets plus
+// the face-class buckets of the 7 lower neighbour tiles (tile_segments_block).
 //
-// Arithmetic follows the reference functors term by term, in FP64:
+// Per chunk of particles the CTA
+//   1. turns each particle into a short record of per-particle factors (FP64
+//      arithmetic, stored in the field precision R) and counts it into one of
+//      the 9^3 cells of the tile's reach (relative cell -1..7 per axis);
+//   2. scans the cell counts and sorts record indexes by cell (counting sort);
+//   3. lets every vertex thread walk the 8 cells whose stencil covers it and
+//      add the contributions into 64-bit fixed-point accumulators held in
+//      registers -- no shared-memory atomics on the accumulation path.
+// The fixed-point scale of each component comes from an upper bound of the
+// per-particle contribution and the particle count, so the sum is exact
+// integer arithmetic and the result does not depend on particle order or
+// thread scheduling (bitwise reproducible).  Each output vertex is written
+// exactly once with plain stores -- no global atomics and no halo fold
+// (projection_comm1, gevolution.hpp:1543, is not needed on one GPU).
+//
+// Arithmetic follows the reference functors term by term:
 //   particle_T00_project  gevolution.hpp:1729-1854
 //   particle_Tij_project  gevolution.hpp:2582-2965 (non-CIC_PROJECT_TIJ)
 //   particle_T0i_project  gevolution.hpp:2031-2201
@@ -20,214 +29,396 @@
 
 namespace gev {
 
-constexpr int DEP_NT = 256;
+constexpr int DEP_NT = 512;   // one thread per tile vertex
 
-// φ staged over the vertex region [-1, 8] of the tile (10^3)
-template <class R>
-__device__ __forceinline__ double phs(const R *s, int vx, int vy, int vz)
-{
-    return (double)s[(vx + 1) + 10 * ((vy + 1) + 10 * (vz + 1))];
-}
+template <class R> struct DepCh;
+template <> struct DepCh<float> { static constexpr int v = 1024; static constexpr int EMAX = 120; };
+template <> struct DepCh<double> { static constexpr int v = 768; static constexpr int EMAX = 1000; };
 
-// Visit every contribution of one particle: f(component, vx, vy, vz, value),
-// vertex coordinates relative to the tile origin.
-template <class R, int KIND, bool USE_PHI, class F>
-__device__ __forceinline__ void particle_contribs(const PView<R> &p, uint32_t i, int N, int x0, int y0, int z0,
-                                                  const R *phis, double a, double m00, double mij, F &&f)
+// record layout: [d0 d1 d2 | T00: E F G | Tij: W00 W11 W22 W01 W02 W12 | T0i: Q0 Q1 Q2]
+template <int KIND> struct DepShape {
+    static constexpr bool HAS00 = (KIND == DEP_T00 || KIND == DEP_T00_TIJ);
+    static constexpr bool HASIJ = (KIND == DEP_TIJ || KIND == DEP_T00_TIJ);
+    static constexpr bool HAS0I = (KIND == DEP_T0I);
+    static constexpr int NC = (HAS00 ? 1 : 0) + (HASIJ ? 6 : 0) + (HAS0I ? 3 : 0);
+    static constexpr int F00 = 3;
+    static constexpr int FIJ = 3 + (HAS00 ? 3 : 0);
+    static constexpr int F0I = 3;
+    static constexpr int NF = 3 + (HAS00 ? 3 : 0) + (HASIJ ? 6 : 0) + (HAS0I ? 3 : 0);
+    static constexpr int NFP = (NF + 3) & ~3;   // padded for 16-byte record loads
+    static constexpr int CIJ = HAS00 ? 1 : 0;   // first Tij output component
+};
+
+constexpr int DEP_NCELL = 729;                  // 9^3 cells of a tile's reach
+constexpr uint16_t DEP_SKIP = 0xFFFFu;
+
+template <class R> __device__ __forceinline__ long long to_fixed(R v);
+template <> __device__ __forceinline__ long long to_fixed<float>(float v) { return __float2ll_rn(v); }
+template <> __device__ __forceinline__ long long to_fixed<double>(double v) { return __double2ll_rn(v); }
+
+__device__ __forceinline__ int phi_slot(int vx, int vy, int vz) { return (vx + 1) + 10 * ((vy + 1) + 10 * (vz + 1)); }
+
+// Per-particle factors of one particle (FP64).  Returns false when the
+// particle lies outside the tile's reach (stale bucket order).  bnd[] receives
+// an upper bound of |contribution| per output component.
+template <class R, int KIND, bool USE_PHI>
+__device__ __forceinline__ bool make_record(const PView<R> &p, uint32_t i, int N, int x0, int y0, int z0,
+                                            const R *phis, double a, double m00, double mij,
+                                            double (&v)[DepShape<KIND>::NF], int &lc,
+                                            double (&bnd)[DepShape<KIND>::NC])
 {
+    using S = DepShape<KIND>;
     uint32_t cell = p.cell[i];
     int cx = (int)(cell % (uint32_t)N), cy = (int)((cell / (uint32_t)N) % (uint32_t)N), cz = (int)(cell / ((uint32_t)N * (uint32_t)N));
     int rx = rel_coord(cx, x0, N), ry = rel_coord(cy, y0, N), rz = rel_coord(cz, z0, N);
-    // a particle outside the tile's reach means the bucket order is stale: skip it
-    // (the staged phi region covers vertices -1..8 only)
-    if (rx < -1 || rx > 7 || ry < -1 || ry > 7 || rz < -1 || rz > 7) return;
-    double d[3] = {p.off[i], p.off[p.cap + i], p.off[2 * p.cap + i]};
-    double q[3] = {(double)p.q[i], (double)p.q[p.cap + i], (double)p.q[2 * p.cap + i]};
-    double ph[8];
+    if (rx < -1 || rx > 7 || ry < -1 || ry > 7 || rz < -1 || rz > 7) return false;
+    lc = (rx + 1) + 9 * ((ry + 1) + 9 * (rz + 1));
+    const double d[3] = {p.off[i], p.off[p.cap + i], p.off[2 * p.cap + i]};
+    const double q[3] = {(double)p.q[i], (double)p.q[p.cap + i], (double)p.q[2 * p.cap + i]};
+    v[0] = d[0]; v[1] = d[1]; v[2] = d[2];
+    double pm = 0.0, pint = 0.0;
     if (USE_PHI) {
 #pragma unroll
-        for (int k = 0; k < 8; k++) ph[k] = phs(phis, rx + ((k >> 2) & 1), ry + ((k >> 1) & 1), rz + (k & 1));
+        for (int k = 0; k < 8; k++) {
+            const int bx = (k >> 2) & 1, by = (k >> 1) & 1, bz = k & 1;
+            double ph = (double)phis[phi_slot(rx + bx, ry + by, rz + bz)];
+            double w = (bx ? d[0] : 1.0 - d[0]) * (by ? d[1] : 1.0 - d[1]) * (bz ? d[2] : 1.0 - d[2]);
+            pint += w * ph;
+            pm = fmax(pm, fabs(ph));
+        }
     }
-    double w8[8];
-#pragma unroll
-    for (int k = 0; k < 8; k++)
-        w8[k] = (((k >> 2) & 1) ? d[0] : 1.0 - d[0]) * (((k >> 1) & 1) ? d[1] : 1.0 - d[1]) * ((k & 1) ? d[2] : 1.0 - d[2]);
-
-    if constexpr (KIND == DEP_T00 || KIND == DEP_T00_TIJ) {
-        // T00 -> component 0
+    if constexpr (S::HAS00) {
         if (USE_PHI) {
             double f2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
             double e = sqrt(f2 + a * a);
             double fc = 3.0 * e + f2 / e;
-            f2 = (0.5 * fc * fc + f2 / (1.0 + f2 / a / a)) / e;
-#pragma unroll
-            for (int k = 0; k < 8; k++)
-                f(0, rx + ((k >> 2) & 1), ry + ((k >> 1) & 1), rz + (k & 1), w8[k] * (e + fc * ph[k] + f2 * ph[k] * ph[k]) * m00);
+            double g = (0.5 * fc * fc + f2 / (1.0 + f2 / a / a)) / e;
+            v[S::F00 + 0] = e * m00;
+            v[S::F00 + 1] = fc * m00;
+            v[S::F00 + 2] = g * m00;
+            bnd[0] = fabs(e * m00) + fabs(fc * m00) * pm + fabs(g * m00) * pm * pm;
         } else {
-#pragma unroll
-            for (int k = 0; k < 8; k++) f(0, rx + ((k >> 2) & 1), ry + ((k >> 1) & 1), rz + (k & 1), w8[k] * m00);
+            v[S::F00 + 0] = m00;
+            v[S::F00 + 1] = 0.0;
+            v[S::F00 + 2] = 0.0;
+            bnd[0] = fabs(m00);
         }
     }
-    if constexpr (KIND == DEP_TIJ || KIND == DEP_T00_TIJ) {
-        constexpr int C0 = (KIND == DEP_T00_TIJ) ? 1 : 0;   // first Tij component slot
+    if constexpr (S::HASIJ) {
         double qq = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
         double e = sqrt(qq + a * a);
-        double fac = 1.0;
-        if (USE_PHI) {
-            double pint = 0.0;
+        double fac = USE_PHI ? 1.0 + (4.0 + a * a / (qq + a * a)) * pint : 1.0;
+        const double W[6] = {fac * mij * q[0] * q[0] / e, fac * mij * q[1] * q[1] / e, fac * mij * q[2] * q[2] / e,
+                             fac * mij * q[0] * q[1] / e, fac * mij * q[0] * q[2] / e, fac * mij * q[1] * q[2] / e};
+        // output order 00,01,02,11,12,22
+        const int comp[6] = {0, 3, 5, 1, 2, 4};
 #pragma unroll
-            for (int k = 0; k < 8; k++) pint += w8[k] * ph[k];
-            fac = 1.0 + (4.0 + a * a / (qq + a * a)) * pint;
+        for (int k = 0; k < 6; k++) {
+            v[S::FIJ + k] = W[k];
+            bnd[S::CIJ + comp[k]] = fabs(W[k]);
         }
-        const int dslot[3] = {0, 3, 5};
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            double W = fac * mij * q[c] * q[c] / e;
-#pragma unroll
-            for (int k = 0; k < 8; k++) f(C0 + dslot[c], rx + ((k >> 2) & 1), ry + ((k >> 1) & 1), rz + (k & 1), W * w8[k]);
-        }
-        double W;
-        W = fac * mij * q[0] * q[1] / e;   // (0,1): x and x+e2
-        f(C0 + 1, rx, ry, rz, W * (1.0 - d[2]));
-        f(C0 + 1, rx, ry, rz + 1, W * d[2]);
-        W = fac * mij * q[0] * q[2] / e;   // (0,2): x and x+e1
-        f(C0 + 2, rx, ry, rz, W * (1.0 - d[1]));
-        f(C0 + 2, rx, ry + 1, rz, W * d[1]);
-        W = fac * mij * q[1] * q[2] / e;   // (1,2): x and x+e0
-        f(C0 + 4, rx, ry, rz, W * (1.0 - d[0]));
-        f(C0 + 4, rx + 1, ry, rz, W * d[0]);
     }
-    if constexpr (KIND == DEP_T0I) {
-        double p_[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        if (USE_PHI) {
+    if constexpr (S::HAS0I) {
 #pragma unroll
-            for (int k = 0; k < 8; k++) p_[k] = ph[k];
+        for (int k = 0; k < 3; k++) {
+            v[S::F0I + k] = m00 * q[k];
+            bnd[k] = fabs(m00 * q[k]) * (1.0 + 2.0 * pm);
         }
-        const double m = m00;
-        f(0, rx, ry, rz, (1 - d[1]) * (1 - d[2]) * (1 + p_[0] + p_[4]) * m * q[0]);
-        f(1, rx, ry, rz, (1 - d[0]) * (1 - d[2]) * (1 + p_[0] + p_[2]) * m * q[1]);
-        f(2, rx, ry, rz, (1 - d[0]) * (1 - d[1]) * (1 + p_[0] + p_[1]) * m * q[2]);
-        f(1, rx + 1, ry, rz, d[0] * (1 - d[2]) * (1 + p_[4] + p_[6]) * m * q[1]);
-        f(2, rx + 1, ry, rz, d[0] * (1 - d[1]) * (1 + p_[4] + p_[5]) * m * q[2]);
-        f(0, rx, ry + 1, rz, d[1] * (1 - d[2]) * (1 + p_[2] + p_[6]) * m * q[0]);
-        f(2, rx, ry + 1, rz, d[1] * (1 - d[0]) * (1 + p_[2] + p_[3]) * m * q[2]);
-        f(0, rx, ry, rz + 1, d[2] * (1 - d[1]) * (1 + p_[1] + p_[5]) * m * q[0]);
-        f(1, rx, ry, rz + 1, d[2] * (1 - d[0]) * (1 + p_[1] + p_[3]) * m * q[1]);
-        f(0, rx, ry + 1, rz + 1, d[1] * d[2] * (1 + p_[3] + p_[7]) * m * q[0]);
-        f(1, rx + 1, ry, rz + 1, d[0] * d[2] * (1 + p_[5] + p_[7]) * m * q[1]);
-        f(2, rx + 1, ry + 1, rz, d[0] * d[1] * (1 + p_[6] + p_[7]) * m * q[2]);
+    }
+    return true;
+}
+
+// add the contributions of one record to the vertex at offset b from its cell
+template <class R, int KIND, bool USE_PHI>
+__device__ __forceinline__ void gather_one(const R *r, int bx, int by, int bz, R phv, R phx, R phy, R phz,
+                                           const R *scl, long long (&acc)[DepShape<KIND>::NC])
+{
+    using S = DepShape<KIND>;
+    const R wx = bx ? r[0] : (R)1 - r[0];
+    const R wy = by ? r[1] : (R)1 - r[1];
+    const R wz = bz ? r[2] : (R)1 - r[2];
+    const R w = wx * wy * wz;
+    if constexpr (S::HAS00) {
+        R val = USE_PHI ? w * (r[S::F00] + (r[S::F00 + 1] + r[S::F00 + 2] * phv) * phv) : w * r[S::F00];
+        acc[0] += to_fixed<R>(val * scl[0]);
+    }
+    if constexpr (S::HASIJ) {
+        constexpr int C = S::CIJ;
+        acc[C + 0] += to_fixed<R>(w * r[S::FIJ + 0] * scl[C + 0]);
+        acc[C + 3] += to_fixed<R>(w * r[S::FIJ + 1] * scl[C + 3]);
+        acc[C + 5] += to_fixed<R>(w * r[S::FIJ + 2] * scl[C + 5]);
+        if (!bx && !by) acc[C + 1] += to_fixed<R>(wz * r[S::FIJ + 3] * scl[C + 1]);   // (0,1): x and x+e2
+        if (!bx && !bz) acc[C + 2] += to_fixed<R>(wy * r[S::FIJ + 4] * scl[C + 2]);   // (0,2): x and x+e1
+        if (!by && !bz) acc[C + 4] += to_fixed<R>(wx * r[S::FIJ + 5] * scl[C + 4]);   // (1,2): x and x+e0
+    }
+    if constexpr (S::HAS0I) {
+        // component i lands on the vertices with b_i = 0, weighted by the other two
+        // axes and by 1 + phi(vertex) + phi(vertex + e_i)
+        if (!bx) acc[0] += to_fixed<R>(wy * wz * r[S::F0I + 0] * ((R)1 + phv + phx) * scl[0]);
+        if (!by) acc[1] += to_fixed<R>(wx * wz * r[S::F0I + 1] * ((R)1 + phv + phy) * scl[1]);
+        if (!bz) acc[2] += to_fixed<R>(wx * wy * r[S::F0I + 2] * ((R)1 + phv + phz) * scl[2]);
     }
 }
 
-template <int KIND> struct DepShape {
-    static constexpr int NC = (KIND == DEP_T00) ? 1 : (KIND == DEP_TIJ ? 6 : (KIND == DEP_T00_TIJ ? 7 : 3));
-};
+template <class R, int NFP> __device__ __forceinline__ void load_record(const R *src, R (&dst)[NFP])
+{
+    if constexpr (sizeof(R) == 4) {
+#pragma unroll
+        for (int k = 0; k < NFP; k += 4) {
+            float4 t = *reinterpret_cast<const float4 *>(src + k);
+            dst[k] = t.x; dst[k + 1] = t.y; dst[k + 2] = t.z; dst[k + 3] = t.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < NFP; k += 2) {
+            double2 t = *reinterpret_cast<const double2 *>(src + k);
+            dst[k] = t.x; dst[k + 1] = t.y;
+        }
+    }
+}
+
+template <class R, int KIND>
+__host__ __device__ constexpr size_t dep_smem_bytes()
+{
+    return (size_t)DepShape<KIND>::NFP * DepCh<R>::v * sizeof(R) + (size_t)(2 * 730) * sizeof(int) +
+           (size_t)3 * DepCh<R>::v * sizeof(uint16_t);
+}
 
 // outputs: component c is written to out[c] (N^3 plane each)
 template <class R, int KIND, bool USE_PHI>
-__global__ void __launch_bounds__(DEP_NT) k_deposit(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt,
-                                                    const R *__restrict__ phi, DepOut<R> out, double a, double m00,
-                                                    double mij, int accumulate)
+__global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt,
+                                                       const R *__restrict__ phi, DepOut<R> out, double a, double m00,
+                                                       double mij, int accumulate)
 {
-    constexpr int NC = DepShape<KIND>::NC;
-    __shared__ unsigned long long acc[NC][512];
+    using S = DepShape<KIND>;
+    constexpr int NC = S::NC, NF = S::NF, NFP = S::NFP;
+    constexpr int CH = DepCh<R>::v;
+    extern __shared__ __align__(16) unsigned char dsm[];
+    R *rec = reinterpret_cast<R *>(dsm);                      // [CH][NFP]
+    int *cstart = reinterpret_cast<int *>(rec + CH * NFP);    // 730
+    int *ccount = cstart + 730;                               // 729 (+1 pad)
+    uint16_t *order = reinterpret_cast<uint16_t *>(ccount + 730);
+    uint16_t *rcell = order + CH;
+    uint16_t *rslot = rcell + CH;
+
     __shared__ R phis[USE_PHI ? 1000 : 1];
-    __shared__ uint32_t seg_lo[20], seg_hi[20], seg_pre[21];
+    __shared__ uint32_t cand_lo[64], cand_hi[64], seg_lo[64], seg_hi[64], seg_pre[65];
     __shared__ int nseg;
     __shared__ unsigned long long vmax[NC];
-    __shared__ double scl[NC], iscl[NC];
+    __shared__ R scl_s[NC];
+    __shared__ double iscl_s[NC];
+    __shared__ int wsum[DEP_NT / 32];
 
+    const int t = threadIdx.x;
     const int tile = blockIdx.x;
     const int tx = tile % nt, ty = (tile / nt) % nt, tz = tile / (nt * nt);
     const int x0 = tx * 8, y0 = ty * 8, z0 = tz * 8;
 
-    if (threadIdx.x == 0) {
-        int ns = tile_segments(bstart, nt, tx, ty, tz, seg_lo, seg_hi);
-        seg_pre[0] = 0;
-        for (int s = 0; s < ns; s++) seg_pre[s + 1] = seg_pre[s] + (seg_hi[s] - seg_lo[s]);
-        nseg = ns;
-    }
-    for (int i = threadIdx.x; i < NC * 512; i += DEP_NT) (&acc[0][0])[i] = 0ull;
-    if (threadIdx.x < NC) vmax[threadIdx.x] = 0ull;
+    tile_segments_block(bstart, nt, tx, ty, tz, cand_lo, cand_hi, seg_lo, seg_hi, seg_pre, &nseg);
+    if (t < NC) vmax[t] = 0ull;
+    for (int c = t; c < 730; c += DEP_NT) ccount[c] = 0;
     if (USE_PHI) {
-        for (int i = threadIdx.x; i < 1000; i += DEP_NT) {
-            int vx = i % 10 - 1, vy = (i / 10) % 10 - 1, vz = i / 100 - 1;
-            phis[i] = phi[sidx(N, wrapi(x0 + vx, N), wrapi(y0 + vy, N), wrapi(z0 + vz, N))];
+        constexpr int PER = (1000 + DEP_NT - 1) / DEP_NT;
+        R pv[PER];
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            int s = t + k * DEP_NT;
+            if (s < 1000) {
+                int vx = s % 10 - 1, vy = (s / 10) % 10 - 1, vz = s / 100 - 1;
+                pv[k] = __ldg(phi + sidx(N, wrapi(x0 + vx, N), wrapi(y0 + vy, N), wrapi(z0 + vz, N)));
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            int s = t + k * DEP_NT;
+            if (s < 1000) phis[s] = pv[k];
         }
     }
     __syncthreads();
     const int ns = nseg;
     const uint32_t total = seg_pre[ns];
-
-    // pass 1: exact maximum |contribution| per component
-    {
-        double lm[NC];
+    if (total == 0) {
+        // nothing reaches this tile: the deposit is zero
+        const int gx = x0 + (t & 7), gy = y0 + ((t >> 3) & 7), gz = z0 + (t >> 6);
+        const int64_t gi = sidx(N, gx, gy, gz);
+        if (!accumulate) {
 #pragma unroll
-        for (int c = 0; c < NC; c++) lm[c] = 0.0;
-        for (uint32_t j = threadIdx.x; j < total; j += DEP_NT) {
-            uint32_t i = seg_map(ns, seg_lo, seg_pre, j);
-            particle_contribs<R, KIND, USE_PHI>(p, i, N, x0, y0, z0, phis, a, m00, mij,
-                                                [&](int c, int vx, int vy, int vz, double v) {
-                                                    if ((unsigned)vx < 8u && (unsigned)vy < 8u && (unsigned)vz < 8u) lm[c] = fmax(lm[c], fabs(v));
-                                                });
+            for (int c = 0; c < NC; c++) out.p[c][gi] = (R)0;
         }
+        return;
+    }
+    const bool multi = total > (uint32_t)CH;
+
+    auto reduce_bounds = [&](double (&lb)[NC]) {
 #pragma unroll
         for (int c = 0; c < NC; c++) {
-            double m = lm[c];
+            double m = lb[c];
             for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-            if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(&vmax[c], (unsigned long long)__double_as_longlong(m));
+            if ((t & 31) == 0 && m > 0.0) atomicMax(&vmax[c], (unsigned long long)__double_as_longlong(m));
         }
-    }
-    __syncthreads();
-    if (threadIdx.x < NC) {
-        double m = __longlong_as_double((long long)vmax[threadIdx.x]);
-        int e = 0;
-        if (m > 0.0 && total > 0) {
-            int ex;
-            frexp(m * (double)total, &ex);
-            e = 61 - ex;
-            e = e > 1000 ? 1000 : (e < -1000 ? -1000 : e);
+    };
+    auto set_scales = [&]() {
+        if (t < NC) {
+            double m = __longlong_as_double((long long)vmax[t]);
+            int e = 0;
+            if (m > 0.0) {
+                int ex;
+                frexp(m * (double)total, &ex);
+                e = 61 - ex;
+                e = e > DepCh<R>::EMAX ? DepCh<R>::EMAX : (e < -DepCh<R>::EMAX ? -DepCh<R>::EMAX : e);
+            }
+            scl_s[t] = (R)ldexp(1.0, e);
+            iscl_s[t] = ldexp(1.0, -e);
         }
-        scl[threadIdx.x] = ldexp(1.0, e);
-        iscl[threadIdx.x] = ldexp(1.0, -e);
-    }
-    __syncthreads();
+    };
 
-    // pass 2: fixed-point accumulation
-    for (uint32_t j = threadIdx.x; j < total; j += DEP_NT) {
-        uint32_t i = seg_map(ns, seg_lo, seg_pre, j);
-        particle_contribs<R, KIND, USE_PHI>(p, i, N, x0, y0, z0, phis, a, m00, mij,
-                                            [&](int c, int vx, int vy, int vz, double v) {
-                                                if ((unsigned)vx < 8u && (unsigned)vy < 8u && (unsigned)vz < 8u) {
-                                                    long long fx = __double2ll_rn(v * scl[c]);
-                                                    atomicAdd(&acc[c][vx + 8 * (vy + 8 * vz)], (unsigned long long)fx);
-                                                }
-                                            });
+    if (multi) {
+        // bounds over every particle first: the scale must be fixed before the first chunk
+        double lb[NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++) lb[c] = 0.0;
+        for (uint32_t j = t; j < total; j += DEP_NT) {
+            uint32_t i = seg_map(ns, seg_lo, seg_pre, j);
+            double v[NF], b[NC];
+            int lc;
+            if (make_record<R, KIND, USE_PHI>(p, i, N, x0, y0, z0, phis, a, m00, mij, v, lc, b)) {
+#pragma unroll
+                for (int c = 0; c < NC; c++) lb[c] = fmax(lb[c], b[c]);
+            }
+        }
+        reduce_bounds(lb);
+        __syncthreads();
+        set_scales();
     }
-    __syncthreads();
 
-    for (int i = threadIdx.x; i < NC * 512; i += DEP_NT) {
-        int c = i >> 9, v = i & 511;
-        int vx = v & 7, vy = (v >> 3) & 7, vz = v >> 6;
-        double val = (double)(long long)acc[c][v] * iscl[c];
-        int64_t gi = sidx(N, x0 + vx, y0 + vy, z0 + vz);
+    // this thread's vertex and the phi values its contributions need
+    const int vx = t & 7, vy = (t >> 3) & 7, vz = t >> 6;
+    R phv = 0, phx = 0, phy = 0, phz = 0;
+    if (USE_PHI) {
+        phv = phis[phi_slot(vx, vy, vz)];
+        phx = phis[phi_slot(vx + 1, vy, vz)];
+        phy = phis[phi_slot(vx, vy + 1, vz)];
+        phz = phis[phi_slot(vx, vy, vz + 1)];
+    }
+    long long acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) acc[c] = 0;
+
+    for (uint32_t base = 0; base < total; base += CH) {
+        const int n = (int)min((uint32_t)CH, total - base);
+        // 1. records and cell counts
+        {
+            double lb[NC];
+#pragma unroll
+            for (int c = 0; c < NC; c++) lb[c] = 0.0;
+            for (int j = t; j < n; j += DEP_NT) {
+                uint32_t i = seg_map(ns, seg_lo, seg_pre, base + (uint32_t)j);
+                double v[NF], b[NC];
+                int lc;
+                if (make_record<R, KIND, USE_PHI>(p, i, N, x0, y0, z0, phis, a, m00, mij, v, lc, b)) {
+                    R *dst = rec + (size_t)j * NFP;
+#pragma unroll
+                    for (int k = 0; k < NF; k++) dst[k] = (R)v[k];
+#pragma unroll
+                    for (int c = 0; c < NC; c++) lb[c] = fmax(lb[c], b[c]);
+                    rcell[j] = (uint16_t)lc;
+                    rslot[j] = (uint16_t)atomicAdd(&ccount[lc], 1);
+                } else {
+                    rcell[j] = DEP_SKIP;
+                }
+            }
+            if (!multi) reduce_bounds(lb);
+        }
+        __syncthreads();
+        if (!multi) set_scales();
+        // 2. exclusive scan of the 729 cell counts (two cells per thread)
+        {
+            const int c0 = 2 * t, c1 = 2 * t + 1;
+            const int n0 = c0 < DEP_NCELL ? ccount[c0] : 0;
+            const int n1 = c1 < DEP_NCELL ? ccount[c1] : 0;
+            int s = n0 + n1, incl = s;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int u = __shfl_up_sync(0xffffffffu, incl, o);
+                if ((t & 31) >= o) incl += u;
+            }
+            if ((t & 31) == 31) wsum[t >> 5] = incl;
+            __syncthreads();
+            if (t < 32) {
+                int w = t < DEP_NT / 32 ? wsum[t] : 0, wi = w;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    int u = __shfl_up_sync(0xffffffffu, wi, o);
+                    if (t >= o) wi += u;
+                }
+                if (t < DEP_NT / 32) wsum[t] = wi - w;   // exclusive warp offsets
+            }
+            __syncthreads();
+            const int excl = incl - s + wsum[t >> 5];
+            if (c0 < DEP_NCELL) cstart[c0] = excl;
+            if (c1 < DEP_NCELL) cstart[c1] = excl + n0;
+        }
+        __syncthreads();
+        // 3. counting sort of record indexes by cell
+        for (int j = t; j < n; j += DEP_NT) {
+            const uint16_t lc = rcell[j];
+            if (lc != DEP_SKIP) order[cstart[lc] + rslot[j]] = (uint16_t)j;
+        }
+        __syncthreads();
+        // 4. gather: the vertex receives from the cells v - b, b in {0,1}^3
+        R scl[NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++) scl[c] = scl_s[c];
+#pragma unroll 1
+        for (int b = 0; b < 8; b++) {
+            const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
+            const int lc = (vx - bx + 1) + 9 * ((vy - by + 1) + 9 * (vz - bz + 1));
+            const int k0 = cstart[lc], k1 = k0 + ccount[lc];
+            for (int k = k0; k < k1; k++) {
+                R r[NFP];
+                load_record<R, NFP>(rec + (size_t)order[k] * NFP, r);
+                gather_one<R, KIND, USE_PHI>(r, bx, by, bz, phv, phx, phy, phz, scl, acc);
+            }
+        }
+        __syncthreads();
+        for (int c = t; c < DEP_NCELL; c += DEP_NT) ccount[c] = 0;
+        __syncthreads();
+    }
+
+    const int64_t gi = sidx(N, x0 + vx, y0 + vy, z0 + vz);
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+        double val = (double)acc[c] * iscl_s[c];
         R *o = out.p[c];
         if (accumulate) o[gi] = (R)((double)o[gi] + val);
         else o[gi] = (R)val;
     }
 }
 
+template <class R, int KIND, bool USE_PHI>
+static void launch_k(const PView<R> &p, const uint32_t *bstart, int N, const R *phi, const DepOut<R> &out, double a,
+                     double m00, double mij, int accumulate, cudaStream_t st)
+{
+    constexpr size_t smem = dep_smem_bytes<R, KIND>();
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_deposit<R, KIND, USE_PHI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_set = true;
+    }
+    const int nt = N / 8;
+    const unsigned grid = (unsigned)nt * nt * nt;
+    k_deposit<R, KIND, USE_PHI><<<grid, DEP_NT, smem, st>>>(p, bstart, N, nt, phi, out, a, m00, mij, accumulate);
+}
+
 template <class R>
 void launch_deposit(int kind, bool use_phi, const PView<R> &p, const uint32_t *bstart, int N, const R *phi,
                     const DepOut<R> &out, double a, double m00, double mij, int accumulate, cudaStream_t st)
 {
-    int nt = N / 8;
-    unsigned grid = (unsigned)nt * nt * nt;
-#define GEV_DEP(K)                                                                                               \
-    if (kind == K) {                                                                                             \
-        if (use_phi) k_deposit<R, K, true><<<grid, DEP_NT, 0, st>>>(p, bstart, N, nt, phi, out, a, m00, mij, accumulate); \
-        else k_deposit<R, K, false><<<grid, DEP_NT, 0, st>>>(p, bstart, N, nt, phi, out, a, m00, mij, accumulate); \
-        return;                                                                                                  \
+#define GEV_DEP(K)                                                                          \
+    if (kind == K) {                                                                        \
+        if (use_phi) launch_k<R, K, true>(p, bstart, N, phi, out, a, m00, mij, accumulate, st);  \
+        else launch_k<R, K, false>(p, bstart, N, phi, out, a, m00, mij, accumulate, st);         \
+        return;                                                                             \
     }
     GEV_DEP(DEP_T00)
     GEV_DEP(DEP_TIJ)

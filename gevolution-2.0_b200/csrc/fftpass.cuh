@@ -15,7 +15,7 @@
 namespace gev {
 
 // ---------------------------------------------------------------------------
-// fused source preparation (PHINONLINEAR), evaluated in FP64
+// fused source preparation (PHINONLINEAR): T00 in FP64, Tij in the field precision
 // ---------------------------------------------------------------------------
 // FX_COPY, FX_PREP_T00, FX_PREP_TIJ: common.cuh
 
@@ -33,6 +33,35 @@ template <class R>
 __device__ __forceinline__ double ld(const R *f, int N, int x, int y, int z)
 {
     return (double)f[sidx(N, wrapi(x, N), wrapi(y, N), wrapi(z, N))];
+}
+
+template <class R>
+__device__ __forceinline__ R ldr(const R *f, int N, int x, int y, int z)
+{
+    return __ldg(f + sidx(N, wrapi(x, N), wrapi(y, N), wrapi(z, N)));
+}
+
+// Strided fill of TOT elements (element idx = threadIdx.x + k*NT): each thread
+// issues B loads before the matching B stores, so B global loads per thread are
+// in flight instead of one (the passes are bound by load latency otherwise).
+template <int TOT, int NT, int B, class V, class LOAD, class STORE>
+__device__ __forceinline__ void staged_fill(LOAD &&load, STORE &&store)
+{
+    constexpr int PER = (TOT + NT - 1) / NT;
+#pragma unroll
+    for (int k0 = 0; k0 < PER; k0 += B) {
+        V v[B];
+#pragma unroll
+        for (int k = 0; k < B; k++) {
+            const int idx = threadIdx.x + (k0 + k) * NT;
+            if (k0 + k < PER && (PER * NT == TOT || idx < TOT)) v[k] = load(idx);
+        }
+#pragma unroll
+        for (int k = 0; k < B; k++) {
+            const int idx = threadIdx.x + (k0 + k) * NT;
+            if (k0 + k < PER && (PER * NT == TOT || idx < TOT)) store(idx, v[k]);
+        }
+    }
 }
 
 // prepareFTsource_T00: gevolution.hpp:160-171
@@ -53,24 +82,32 @@ __device__ __forceinline__ double prep_t00(const FxArgs<R> &a, int N, int x, int
     return r;
 }
 
-// prepareFTsource_Tij for one symmetric component c (00,01,02,11,12,22): gevolution.hpp:64-107
+// prepareFTsource_Tij for one symmetric component c (00,01,02,11,12,22),
+// gevolution.hpp:64-107, in the field precision R.  Diagonal:
+// (phi(x+e_i) - phi(x-e_i))^2 / 2 + coeff T_ii.  Off-diagonal, the reference's
+//   pi pj - p0 pij + (p0^2 - pi^2 - pj^2 + pij^2) / 2
+// is evaluated in the algebraically identical form 2uv + w (u + v + w/2), with
+// u = pi - p0, v = pj - p0, w = pij - pi - pj + p0: the squares of the
+// potential cancel exactly in that form, so it keeps full relative accuracy in
+// FP32 where the reference's form loses (phi / grad phi)^2 to cancellation.
 template <class R>
-__device__ __forceinline__ double prep_tij(const R *T, const R *phi, double coeff, int c, int N, int x, int y, int z)
+__device__ __forceinline__ R prep_tij(const R *T, const R *phi, R coeff, int c, int N, int x, int y, int z)
 {
-    int64_t i = sidx(N, x, y, z);
-    double t = (double)T[i];
+    const int64_t i = sidx(N, x, y, z);
+    const R t = __ldg(T + i);
     const int ai = (c == 0 || c == 1 || c == 2) ? 0 : (c == 5 ? 2 : 1);
     const int aj = (c == 0) ? 0 : (c == 1 ? 1 : ((c == 2 || c == 4 || c == 5) ? 2 : 1));
-    int ei[3] = {ai == 0, ai == 1, ai == 2}, ej[3] = {aj == 0, aj == 1, aj == 2};
+    const int ei[3] = {ai == 0, ai == 1, ai == 2}, ej[3] = {aj == 0, aj == 1, aj == 2};
     if (ai == aj) {
-        double g = ld(phi, N, x + ei[0], y + ei[1], z + ei[2]) - ld(phi, N, x - ei[0], y - ei[1], z - ei[2]);
-        return 0.5 * g * g + coeff * t;
+        const R g = ldr(phi, N, x + ei[0], y + ei[1], z + ei[2]) - ldr(phi, N, x - ei[0], y - ei[1], z - ei[2]);
+        return (R)0.5 * g * g + coeff * t;
     }
-    double p0 = (double)phi[i];
-    double pi_ = ld(phi, N, x + ei[0], y + ei[1], z + ei[2]);
-    double pj = ld(phi, N, x + ej[0], y + ej[1], z + ej[2]);
-    double pij = ld(phi, N, x + ei[0] + ej[0], y + ei[1] + ej[1], z + ei[2] + ej[2]);
-    return pi_ * pj - p0 * pij + 0.5 * (p0 * p0 - pi_ * pi_ - pj * pj + pij * pij) + coeff * t;
+    const R p0 = __ldg(phi + i);
+    const R pi_ = ldr(phi, N, x + ei[0], y + ei[1], z + ei[2]);
+    const R pj = ldr(phi, N, x + ej[0], y + ej[1], z + ej[2]);
+    const R pij = ldr(phi, N, x + ei[0] + ej[0], y + ei[1] + ej[1], z + ei[2] + ej[2]);
+    const R u = pi_ - p0, v = pj - p0, w = (pij - pi_) - (pj - p0);
+    return (R)2 * u * v + w * (u + v + (R)0.5 * w) + coeff * t;
 }
 
 // ---------------------------------------------------------------------------
@@ -92,24 +129,26 @@ __global__ void __launch_bounds__(NT) k_fx_fwd(FxArgs<R> a, int64_t in_stride, i
     C *out = a.out + (int64_t)comp * out_stride;
     double lsum = 0.0;
 
-    for (int idx = threadIdx.x; idx < M * T; idx += NT) {
-        int n = idx % M, t = idx / M, y = y0 + t;
-        R v0, v1;
-        if constexpr (MODE == FX_COPY) {
-            const R *row = in + sidx(N, 0, y, z);
-            v0 = row[2 * n];
-            v1 = row[2 * n + 1];
-        } else if constexpr (MODE == FX_PREP_T00) {
-            double s0, s1;
-            v0 = (R)prep_t00(a, N, 2 * n, y, z, s0);
-            v1 = (R)prep_t00(a, N, 2 * n + 1, y, z, s1);
-            lsum += s0 + s1;
-        } else {
-            v0 = (R)prep_tij(in, a.phi, a.c, a.comp0 + comp, N, 2 * n, y, z);
-            v1 = (R)prep_tij(in, a.phi, a.c, a.comp0 + comp, N, 2 * n + 1, y, z);
-        }
-        buf[n * LD + t] = mk(v0, v1);
-    }
+    staged_fill<M * T, NT, (MODE == FX_COPY ? 8 : 4), C>(
+        [&](int idx) {
+            const int n = idx % M, t = idx / M, y = y0 + t;
+            R v0, v1;
+            if constexpr (MODE == FX_COPY) {
+                const R *row = in + sidx(N, 0, y, z);
+                v0 = __ldg(row + 2 * n);
+                v1 = __ldg(row + 2 * n + 1);
+            } else if constexpr (MODE == FX_PREP_T00) {
+                double s0, s1;
+                v0 = (R)prep_t00(a, N, 2 * n, y, z, s0);
+                v1 = (R)prep_t00(a, N, 2 * n + 1, y, z, s1);
+                lsum += s0 + s1;
+            } else {
+                v0 = prep_tij(in, a.phi, (R)a.c, a.comp0 + comp, N, 2 * n, y, z);
+                v1 = prep_tij(in, a.phi, (R)a.c, a.comp0 + comp, N, 2 * n + 1, y, z);
+            }
+            return mk(v0, v1);
+        },
+        [&](int idx, C v) { buf[(idx % M) * LD + idx / M] = v; });
     __syncthreads();
     fft_lines<M, -1, T, NT>(buf, LD, tw_half);
 
@@ -141,7 +180,7 @@ __global__ void __launch_bounds__(NT) k_fx_fwd(FxArgs<R> a, int64_t in_stride, i
 // y pass (in place), complex.  grid (ceil(P/T), N, ncomp)
 // ---------------------------------------------------------------------------
 template <class R, int N, int T, int NT, int S>
-__global__ void __launch_bounds__(NT) k_fy(typename CT<R>::C *data, int64_t stride,
+__global__ void __launch_bounds__(NT, 4) k_fy(typename CT<R>::C *data, int64_t stride,
                                            const typename CT<R>::C *__restrict__ tw)
 {
     using C = typename CT<R>::C;
@@ -150,10 +189,12 @@ __global__ void __launch_bounds__(NT) k_fy(typename CT<R>::C *data, int64_t stri
     C *buf = reinterpret_cast<C *>(smem_raw);
     const int kx0 = blockIdx.x * T, z = blockIdx.y;
     C *d = data + (int64_t)blockIdx.z * stride;
-    for (int idx = threadIdx.x; idx < N * T; idx += NT) {
-        int t = idx % T, n = idx / T, kx = kx0 + t;
-        buf[n * LD + t] = (kx < P) ? d[kx + (int64_t)P * (n + (int64_t)N * z)] : mk(R(0), R(0));
-    }
+    staged_fill<N * T, NT, 8, C>(
+        [&](int idx) {
+            const int t = idx % T, n = idx / T, kx = kx0 + t;
+            return (kx < P) ? d[kx + (int64_t)P * (n + (int64_t)N * z)] : mk(R(0), R(0));
+        },
+        [&](int idx, C v) { buf[(idx / T) * LD + idx % T] = v; });
     __syncthreads();
     fft_lines<N, S, T, NT>(buf, LD, tw);
     for (int idx = threadIdx.x; idx < N * T; idx += NT) {
@@ -179,18 +220,20 @@ __global__ void __launch_bounds__(NT) k_fx_inv(const typename CT<R>::C *in, int6
     const int y0 = blockIdx.x * T, z = blockIdx.y;
     const C *src = in + (int64_t)blockIdx.z * in_stride;
     R *dst = out + (int64_t)blockIdx.z * out_stride;
-    for (int idx = threadIdx.x; idx < M * T; idx += NT) {
-        int k = idx % M, t = idx / M, y = y0 + t;
-        const C *row = src + (int64_t)P * (y + (int64_t)N * z);
-        C A = row[k], B = row[M - k];
-        if (k == 0) { A.y = R(0); B.y = R(0); }
-        B.y = -B.y;
-        C w = __ldg(tw_full + k);
-        w.y = -w.y;                                    // exp(+2 pi i k / N)
-        C dd = cmul(csub(A, B), w);
-        C s = cadd(A, B);
-        buf[k * LD + t] = mk(s.x - dd.y, s.y + dd.x);  // (A+B) + i (A-B) w
-    }
+    staged_fill<M * T, NT, 4, C>(
+        [&](int idx) {
+            const int k = idx % M, t = idx / M, y = y0 + t;
+            const C *row = src + (int64_t)P * (y + (int64_t)N * z);
+            C A = __ldg(row + k), B = __ldg(row + M - k);
+            if (k == 0) { A.y = R(0); B.y = R(0); }
+            B.y = -B.y;
+            C w = __ldg(tw_full + k);
+            w.y = -w.y;                                // exp(+2 pi i k / N)
+            C dd = cmul(csub(A, B), w);
+            C s = cadd(A, B);
+            return mk(s.x - dd.y, s.y + dd.x);         // (A+B) + i (A-B) w
+        },
+        [&](int idx, C v) { buf[(idx % M) * LD + idx / M] = v; });
     __syncthreads();
     fft_lines<M, 1, T, NT>(buf, LD, tw_half);
     for (int idx = threadIdx.x; idx < M * T; idx += NT) {
@@ -389,7 +432,7 @@ __device__ __forceinline__ void fz_apply(const FzArgs<R> &a, int N, int kx, int 
 
 // grid (ceil(P/T), N); T kx-columns at one ky, all CIN components of the solve.
 template <class R, int N, int T, int NT, int OP, int EXTRA>
-__global__ void __launch_bounds__(NT) k_fz(FzArgs<R> a, const typename CT<R>::C *__restrict__ tw)
+__global__ void __launch_bounds__(NT, 2) k_fz(FzArgs<R> a, const typename CT<R>::C *__restrict__ tw)
 {
     using C = typename CT<R>::C;
     constexpr int P = N / 2 + 1;
@@ -399,12 +442,19 @@ __global__ void __launch_bounds__(NT) k_fz(FzArgs<R> a, const typename CT<R>::C 
     C *buf = reinterpret_cast<C *>(smem_raw);
     const int kx0 = blockIdx.x * T, ky = blockIdx.y;
 
-    for (int idx = threadIdx.x; idx < N * CIN * T; idx += NT) {
-        int t = idx % T, r = idx / T, c = r % CIN, n = r / CIN, kx = kx0 + t;
-        buf[n * LD + c * T + t] = (kx < P) ? a.data[c * a.stride + kx + (int64_t)P * (ky + (int64_t)N * n)] : mk(R(0), R(0));
-    }
+    staged_fill<N * CIN * T, NT, 8, C>(
+        [&](int idx) {
+            const int t = idx % T, r = idx / T, c = r % CIN, n = r / CIN, kx = kx0 + t;
+            return (kx < P) ? a.data[c * a.stride + kx + (int64_t)P * (ky + (int64_t)N * n)] : mk(R(0), R(0));
+        },
+        [&](int idx, C v) {
+            const int t = idx % T, r = idx / T, c = r % CIN, n = r / CIN;
+            buf[n * LD + c * T + t] = v;
+        });
     __syncthreads();
-    fft_lines<N, -1, CIN * T, NT>(buf, LD, tw);
+    // one component at a time keeps the butterfly registers per thread small
+#pragma unroll 1
+    for (int c = 0; c < CIN; c++) fft_lines<N, -1, T, NT>(buf + c * T, LD, tw);
 
     for (int idx = threadIdx.x; idx < N * T; idx += NT) {
         int t = idx % T, n = idx / T, kx = kx0 + t;
@@ -419,7 +469,8 @@ __global__ void __launch_bounds__(NT) k_fz(FzArgs<R> a, const typename CT<R>::C 
     }
     if constexpr (COUT > 0) {
         __syncthreads();
-        fft_lines<N, 1, COUT * T, NT>(buf, LD, tw);
+#pragma unroll 1
+        for (int c = 0; c < COUT; c++) fft_lines<N, 1, T, NT>(buf + c * T, LD, tw);
         for (int idx = threadIdx.x; idx < N * COUT * T; idx += NT) {
             int t = idx % T, r = idx / T, c = r % COUT, n = r / COUT, kx = kx0 + t;
             if (kx < P) a.data[c * a.stride + kx + (int64_t)P * (ky + (int64_t)N * n)] = buf[n * LD + c * T + t];

@@ -57,6 +57,45 @@ __device__ __forceinline__ int tile_segments(const uint32_t *bstart, int nt, int
     return ns;
 }
 
+// Block-cooperative form of tile_segments: 64 threads read the 64 candidate
+// (neighbour, class) bucket ranges in parallel, thread 0 merges the non-empty
+// ones (in the same order) and builds the prefix sums.  Arrays hold 64 (+1)
+// entries.  Contains a __syncthreads(); every thread of the block must call it.
+__device__ __forceinline__ void tile_segments_block(const uint32_t *bstart, int nt, int tx, int ty, int tz,
+                                                    uint32_t *cand_lo, uint32_t *cand_hi, uint32_t *seg_lo,
+                                                    uint32_t *seg_hi, uint32_t *seg_pre, int *nseg)
+{
+    const int t = threadIdx.x;
+    if (t < 64) {
+        const int m = t >> 3, c = t & 7;   // neighbour offset bits, class
+        uint32_t lo = 0, hi = 0;
+        if ((c & m) == m) {
+            const int dx = m & 1, dy = (m >> 1) & 1, dz = (m >> 2) & 1;
+            const int nx = tx - dx < 0 ? nt - 1 : tx - dx;
+            const int ny = ty - dy < 0 ? nt - 1 : ty - dy;
+            const int nz = tz - dz < 0 ? nt - 1 : tz - dz;
+            const uint32_t nb = (uint32_t)nx + (uint32_t)nt * ((uint32_t)ny + (uint32_t)nt * (uint32_t)nz);
+            lo = bstart[8 * nb + c];
+            hi = bstart[8 * nb + c + 1];
+        }
+        cand_lo[t] = lo;
+        cand_hi[t] = hi;
+    }
+    __syncthreads();
+    if (t == 0) {
+        int ns = 0;
+        for (int k = 0; k < 64; k++) {
+            const uint32_t lo = cand_lo[k], hi = cand_hi[k];
+            if (hi <= lo) continue;
+            if (ns > 0 && seg_hi[ns - 1] == lo) seg_hi[ns - 1] = hi;
+            else { seg_lo[ns] = lo; seg_hi[ns] = hi; ns++; }
+        }
+        seg_pre[0] = 0;
+        for (int s = 0; s < ns; s++) seg_pre[s + 1] = seg_pre[s] + (seg_hi[s] - seg_lo[s]);
+        *nseg = ns;
+    }
+}
+
 // map a position inside the concatenated segment list to a particle index
 __device__ __forceinline__ uint32_t seg_map(int ns, const uint32_t *seg_lo, const uint32_t *seg_pre, uint32_t i)
 {

@@ -60,12 +60,39 @@ __global__ void __launch_bounds__(KD_NT) k_kick_drift(PView<R> p, const uint32_t
     const bool need_phi = kp.do_kick || (kp.do_drift && kp.nfield_d >= 1);
     const bool need_chi = (kp.do_kick && kp.nfield_k >= 2) || (kp.do_drift && kp.nfield_d >= 2);
     const bool need_B = (kp.do_kick && kp.nfield_k >= 3) || (kp.do_drift && kp.nfield_d >= 3);
-    for (int i = threadIdx.x; i < KD_W * KD_W * KD_W; i += KD_NT) {
-        int vx = i % KD_W - 1, vy = (i / KD_W) % KD_W - 1, vz = i / (KD_W * KD_W) - 1;
-        int64_t g = sidx(N, wrapi(x0 + vx, N), wrapi(y0 + vy, N), wrapi(z0 + vz, N));
-        if (need_phi) sf[0][i] = phi[g];
-        if (need_chi) sf[1][i] = chi[g];
-        if (need_B) { sf[2][i] = Bi[g]; sf[3][i] = Bi[n3 + g]; sf[4][i] = Bi[2 * n3 + g]; }
+    {
+        // all loads of this thread's share first, then the shared-memory stores,
+        // so that up to PER*5 global loads are in flight per thread
+        constexpr int NS = KD_W * KD_W * KD_W;
+        constexpr int PER = (NS + KD_NT - 1) / KD_NT;
+        int64_t gi[PER];
+        R v[PER][5];
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const int i = threadIdx.x + k * KD_NT;
+            const int ii = i < NS ? i : NS - 1;
+            const int vx = ii % KD_W - 1, vy = (ii / KD_W) % KD_W - 1, vz = ii / (KD_W * KD_W) - 1;
+            gi[k] = sidx(N, wrapi(x0 + vx, N), wrapi(y0 + vy, N), wrapi(z0 + vz, N));
+        }
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            if (need_phi) v[k][0] = __ldg(phi + gi[k]);
+            if (need_chi) v[k][1] = __ldg(chi + gi[k]);
+            if (need_B) {
+                v[k][2] = __ldg(Bi + gi[k]);
+                v[k][3] = __ldg(Bi + n3 + gi[k]);
+                v[k][4] = __ldg(Bi + 2 * n3 + gi[k]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const int i = threadIdx.x + k * KD_NT;
+            if (i < NS) {
+                if (need_phi) sf[0][i] = v[k][0];
+                if (need_chi) sf[1][i] = v[k][1];
+                if (need_B) { sf[2][i] = v[k][2]; sf[3][i] = v[k][3]; sf[4][i] = v[k][4]; }
+            }
+        }
     }
     __syncthreads();
     const R *P_ = sf[0], *X_ = sf[1], *B0 = sf[2], *B1 = sf[3], *B2 = sf[4];

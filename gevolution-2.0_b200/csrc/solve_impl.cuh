@@ -11,9 +11,9 @@ namespace gev {
 
 template <class R> struct PassCfg {
     static constexpr int TX = sizeof(R) == 4 ? 16 : 8;   // rows per x-pass CTA
-    static constexpr int TY = sizeof(R) == 4 ? 16 : 8;   // columns per y-pass CTA
-    static constexpr int TZ1 = sizeof(R) == 4 ? 16 : 8;  // Poisson
-    static constexpr int TZ3 = sizeof(R) == 4 ? 8 : 4;   // vector
+    static constexpr int TY = sizeof(R) == 4 ? 8 : 4;    // columns per y-pass CTA
+    static constexpr int TZ1 = sizeof(R) == 4 ? 8 : 4;   // Poisson
+    static constexpr int TZ3 = sizeof(R) == 4 ? 4 : 2;   // vector
     static constexpr int TZ6 = sizeof(R) == 4 ? 4 : 2;   // scalar / tensor
 };
 
@@ -64,7 +64,7 @@ template <class R, int N, int S>
 void fy_n(typename CT<R>::C *data, int64_t stride, int ncomp, const FftTables<R> &tb, cudaStream_t st)
 {
     using C = typename CT<R>::C;
-    constexpr int T = PassCfg<R>::TY, NT = (N >= 256) ? 512 : 256;
+    constexpr int T = PassCfg<R>::TY, NT = 256;
     size_t smem = (size_t)N * (T + 1) * sizeof(C);
     auto k = k_fy<R, N, T, NT, S>;
     set_smem(k, smem);
@@ -103,7 +103,7 @@ void fz_n(const FzArgs<R> &a, const FftTables<R> &tb, cudaStream_t st)
 {
     using C = typename CT<R>::C;
     constexpr int T = (OP == OP_POISSON || OP == OP_BIN) ? PassCfg<R>::TZ1 : (OP == OP_VECTOR ? PassCfg<R>::TZ3 : PassCfg<R>::TZ6);
-    constexpr int NT = (N >= 256) ? 512 : 256;
+    constexpr int NT = 256;
     constexpr int CIN = OpShape<OP, EXTRA>::CIN;
     size_t smem = (size_t)N * (CIN * T + 1) * sizeof(C);
     auto k = k_fz<R, N, T, NT, OP, EXTRA>;
