@@ -5,10 +5,11 @@
 // the face-class buckets of the 7 lower neighbour tiles (tile_segments_block).
 //
 // Per chunk of particles the CTA
-//   1. turns each particle into a short record of per-particle factors (FP64
-//      arithmetic, stored in the field precision R) and counts it into one of
-//      the 9^3 cells of the tile's reach (relative cell -1..7 per axis);
-//   2. scans the cell counts and sorts record indexes by cell (counting sort);
+//   1. turns each particle into a short record of per-particle factors (in the
+//      field precision R) and counts it into one of the 9^3 cells of the
+//      tile's reach (relative cell -1..7 per axis);
+//   2. scans the cell counts, sorts record indexes by cell (counting sort) and
+//      pre-multiplies each record by the fixed-point scales;
 //   3. lets every vertex thread walk the 8 cells whose stencil covers it and
 //      add the contributions into 64-bit fixed-point accumulators held in
 //      registers -- no shared-memory atomics on the accumulation path.
@@ -58,58 +59,60 @@ template <> __device__ __forceinline__ long long to_fixed<double>(double v) { re
 
 __device__ __forceinline__ int phi_slot(int vx, int vy, int vz) { return (vx + 1) + 10 * ((vy + 1) + 10 * (vz + 1)); }
 
-// Per-particle factors of one particle (FP64).  Returns false when the
+// Per-particle factors of one particle, in the field precision R (FP32 in
+// mixed mode: the record is stored in R anyway).  Returns false when the
 // particle lies outside the tile's reach (stale bucket order).  bnd[] receives
-// an upper bound of |contribution| per output component.
+// an upper bound of |contribution| per output component.  The reference's
+// divisions by e = sqrt(q^2 + a^2) are taken as one reciprocal, and
+// f2 / (1 + f2/a^2) as f2 a^2 / e^2 (the same quantity).
 template <class R, int KIND, bool USE_PHI>
 __device__ __forceinline__ bool make_record(const PView<R> &p, uint32_t i, int N, int x0, int y0, int z0,
-                                            const R *phis, double a, double m00, double mij,
-                                            double (&v)[DepShape<KIND>::NF], int &lc,
-                                            double (&bnd)[DepShape<KIND>::NC])
+                                            const R *phis, R a, R m00, R mij, R (&v)[DepShape<KIND>::NF], int &lc,
+                                            R (&bnd)[DepShape<KIND>::NC])
 {
     using S = DepShape<KIND>;
-    uint32_t cell = p.cell[i];
-    int cx = (int)(cell % (uint32_t)N), cy = (int)((cell / (uint32_t)N) % (uint32_t)N), cz = (int)(cell / ((uint32_t)N * (uint32_t)N));
-    int rx = rel_coord(cx, x0, N), ry = rel_coord(cy, y0, N), rz = rel_coord(cz, z0, N);
+    const uint32_t cell = p.cell[i];
+    const int cx = (int)(cell % (uint32_t)N), cy = (int)((cell / (uint32_t)N) % (uint32_t)N), cz = (int)(cell / ((uint32_t)N * (uint32_t)N));
+    const int rx = rel_coord(cx, x0, N), ry = rel_coord(cy, y0, N), rz = rel_coord(cz, z0, N);
     if (rx < -1 || rx > 7 || ry < -1 || ry > 7 || rz < -1 || rz > 7) return false;
     lc = (rx + 1) + 9 * ((ry + 1) + 9 * (rz + 1));
-    const double d[3] = {p.off[i], p.off[p.cap + i], p.off[2 * p.cap + i]};
-    const double q[3] = {(double)p.q[i], (double)p.q[p.cap + i], (double)p.q[2 * p.cap + i]};
+    const R d[3] = {(R)p.off[i], (R)p.off[p.cap + i], (R)p.off[2 * p.cap + i]};
+    const R q[3] = {p.q[i], p.q[p.cap + i], p.q[2 * p.cap + i]};
     v[0] = d[0]; v[1] = d[1]; v[2] = d[2];
-    double pm = 0.0, pint = 0.0;
+    R pm = 0, pint = 0;
     if (USE_PHI) {
 #pragma unroll
         for (int k = 0; k < 8; k++) {
             const int bx = (k >> 2) & 1, by = (k >> 1) & 1, bz = k & 1;
-            double ph = (double)phis[phi_slot(rx + bx, ry + by, rz + bz)];
-            double w = (bx ? d[0] : 1.0 - d[0]) * (by ? d[1] : 1.0 - d[1]) * (bz ? d[2] : 1.0 - d[2]);
+            const R ph = phis[phi_slot(rx + bx, ry + by, rz + bz)];
+            const R w = (bx ? d[0] : (R)1 - d[0]) * (by ? d[1] : (R)1 - d[1]) * (bz ? d[2] : (R)1 - d[2]);
             pint += w * ph;
             pm = fmax(pm, fabs(ph));
         }
     }
+    const R f2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+    const R e2 = f2 + a * a;
+    const R e = sqrt(e2);
+    const R ie = (R)1 / e;
     if constexpr (S::HAS00) {
         if (USE_PHI) {
-            double f2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
-            double e = sqrt(f2 + a * a);
-            double fc = 3.0 * e + f2 / e;
-            double g = (0.5 * fc * fc + f2 / (1.0 + f2 / a / a)) / e;
+            const R fc = (R)3 * e + f2 * ie;
+            const R g = ((R)0.5 * fc * fc + f2 * a * a * ie * ie) * ie;
             v[S::F00 + 0] = e * m00;
             v[S::F00 + 1] = fc * m00;
             v[S::F00 + 2] = g * m00;
             bnd[0] = fabs(e * m00) + fabs(fc * m00) * pm + fabs(g * m00) * pm * pm;
         } else {
             v[S::F00 + 0] = m00;
-            v[S::F00 + 1] = 0.0;
-            v[S::F00 + 2] = 0.0;
+            v[S::F00 + 1] = 0;
+            v[S::F00 + 2] = 0;
             bnd[0] = fabs(m00);
         }
     }
     if constexpr (S::HASIJ) {
-        double qq = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
-        double e = sqrt(qq + a * a);
-        double fac = USE_PHI ? 1.0 + (4.0 + a * a / (qq + a * a)) * pint : 1.0;
-        const double W[6] = {fac * mij * q[0] * q[0] / e, fac * mij * q[1] * q[1] / e, fac * mij * q[2] * q[2] / e,
-                             fac * mij * q[0] * q[1] / e, fac * mij * q[0] * q[2] / e, fac * mij * q[1] * q[2] / e};
+        const R fac = USE_PHI ? (R)1 + ((R)4 + a * a * ie * ie) * pint : (R)1;
+        const R s = fac * mij * ie;
+        const R W[6] = {s * q[0] * q[0], s * q[1] * q[1], s * q[2] * q[2], s * q[0] * q[1], s * q[0] * q[2], s * q[1] * q[2]};
         // output order 00,01,02,11,12,22
         const int comp[6] = {0, 3, 5, 1, 2, 4};
 #pragma unroll
@@ -122,16 +125,36 @@ __device__ __forceinline__ bool make_record(const PView<R> &p, uint32_t i, int N
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             v[S::F0I + k] = m00 * q[k];
-            bnd[k] = fabs(m00 * q[k]) * (1.0 + 2.0 * pm);
+            bnd[k] = fabs(m00 * q[k]) * ((R)1 + (R)2 * pm);
         }
     }
     return true;
 }
 
-// add the contributions of one record to the vertex at offset b from its cell
+// Multiply a record's value fields by the fixed-point scales of the
+// components they feed (the CIC weights stay unscaled).
+template <class R, int KIND> __device__ __forceinline__ void scale_record(R *r, const R *scl)
+{
+    using S = DepShape<KIND>;
+    if constexpr (S::HAS00) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) r[S::F00 + k] *= scl[0];
+    }
+    if constexpr (S::HASIJ) {
+        const int comp[6] = {0, 3, 5, 1, 2, 4};
+#pragma unroll
+        for (int k = 0; k < 6; k++) r[S::FIJ + k] *= scl[S::CIJ + comp[k]];
+    }
+    if constexpr (S::HAS0I) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) r[S::F0I + k] *= scl[k];
+    }
+}
+
+// add the contributions of one (scaled) record to the vertex at offset b from its cell
 template <class R, int KIND, bool USE_PHI>
 __device__ __forceinline__ void gather_one(const R *r, int bx, int by, int bz, R phv, R phx, R phy, R phz,
-                                           const R *scl, long long (&acc)[DepShape<KIND>::NC])
+                                           long long (&acc)[DepShape<KIND>::NC])
 {
     using S = DepShape<KIND>;
     const R wx = bx ? r[0] : (R)1 - r[0];
@@ -139,24 +162,24 @@ __device__ __forceinline__ void gather_one(const R *r, int bx, int by, int bz, R
     const R wz = bz ? r[2] : (R)1 - r[2];
     const R w = wx * wy * wz;
     if constexpr (S::HAS00) {
-        R val = USE_PHI ? w * (r[S::F00] + (r[S::F00 + 1] + r[S::F00 + 2] * phv) * phv) : w * r[S::F00];
-        acc[0] += to_fixed<R>(val * scl[0]);
+        const R val = USE_PHI ? w * (r[S::F00] + (r[S::F00 + 1] + r[S::F00 + 2] * phv) * phv) : w * r[S::F00];
+        acc[0] += to_fixed<R>(val);
     }
     if constexpr (S::HASIJ) {
         constexpr int C = S::CIJ;
-        acc[C + 0] += to_fixed<R>(w * r[S::FIJ + 0] * scl[C + 0]);
-        acc[C + 3] += to_fixed<R>(w * r[S::FIJ + 1] * scl[C + 3]);
-        acc[C + 5] += to_fixed<R>(w * r[S::FIJ + 2] * scl[C + 5]);
-        if (!bx && !by) acc[C + 1] += to_fixed<R>(wz * r[S::FIJ + 3] * scl[C + 1]);   // (0,1): x and x+e2
-        if (!bx && !bz) acc[C + 2] += to_fixed<R>(wy * r[S::FIJ + 4] * scl[C + 2]);   // (0,2): x and x+e1
-        if (!by && !bz) acc[C + 4] += to_fixed<R>(wx * r[S::FIJ + 5] * scl[C + 4]);   // (1,2): x and x+e0
+        acc[C + 0] += to_fixed<R>(w * r[S::FIJ + 0]);
+        acc[C + 3] += to_fixed<R>(w * r[S::FIJ + 1]);
+        acc[C + 5] += to_fixed<R>(w * r[S::FIJ + 2]);
+        if (!bx && !by) acc[C + 1] += to_fixed<R>(wz * r[S::FIJ + 3]);   // (0,1): x and x+e2
+        if (!bx && !bz) acc[C + 2] += to_fixed<R>(wy * r[S::FIJ + 4]);   // (0,2): x and x+e1
+        if (!by && !bz) acc[C + 4] += to_fixed<R>(wx * r[S::FIJ + 5]);   // (1,2): x and x+e0
     }
     if constexpr (S::HAS0I) {
         // component i lands on the vertices with b_i = 0, weighted by the other two
         // axes and by 1 + phi(vertex) + phi(vertex + e_i)
-        if (!bx) acc[0] += to_fixed<R>(wy * wz * r[S::F0I + 0] * ((R)1 + phv + phx) * scl[0]);
-        if (!by) acc[1] += to_fixed<R>(wx * wz * r[S::F0I + 1] * ((R)1 + phv + phy) * scl[1]);
-        if (!bz) acc[2] += to_fixed<R>(wx * wy * r[S::F0I + 2] * ((R)1 + phv + phz) * scl[2]);
+        if (!bx) acc[0] += to_fixed<R>(wy * wz * r[S::F0I + 0] * ((R)1 + phv + phx));
+        if (!by) acc[1] += to_fixed<R>(wx * wz * r[S::F0I + 1] * ((R)1 + phv + phy));
+        if (!bz) acc[2] += to_fixed<R>(wx * wy * r[S::F0I + 2] * ((R)1 + phv + phz));
     }
 }
 
@@ -202,8 +225,7 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
     uint16_t *rslot = rcell + CH;
 
     __shared__ R phis[USE_PHI ? 1000 : 1];
-    __shared__ uint32_t cand_lo[64], cand_hi[64], seg_lo[64], seg_hi[64], seg_pre[65];
-    __shared__ int nseg;
+    __shared__ uint32_t seg_lo[64], seg_hi[64], seg_pre[65];
     __shared__ unsigned long long vmax[NC];
     __shared__ R scl_s[NC];
     __shared__ double iscl_s[NC];
@@ -214,7 +236,8 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
     const int tx = tile % nt, ty = (tile / nt) % nt, tz = tile / (nt * nt);
     const int x0 = tx * 8, y0 = ty * 8, z0 = tz * 8;
 
-    tile_segments_block(bstart, nt, tx, ty, tz, cand_lo, cand_hi, seg_lo, seg_hi, seg_pre, &nseg);
+    const R ra = (R)a, rm00 = (R)m00, rmij = (R)mij;
+    tile_segments_block(bstart, nt, tx, ty, tz, seg_lo, seg_hi, seg_pre);
     if (t < NC) vmax[t] = 0ull;
     for (int c = t; c < 730; c += DEP_NT) ccount[c] = 0;
     if (USE_PHI) {
@@ -235,8 +258,7 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
         }
     }
     __syncthreads();
-    const int ns = nseg;
-    const uint32_t total = seg_pre[ns];
+    const uint32_t total = seg_pre[64];
     if (total == 0) {
         // nothing reaches this tile: the deposit is zero
         const int gx = x0 + (t & 7), gy = y0 + ((t >> 3) & 7), gz = z0 + (t >> 6);
@@ -249,12 +271,12 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
     }
     const bool multi = total > (uint32_t)CH;
 
-    auto reduce_bounds = [&](double (&lb)[NC]) {
+    auto reduce_bounds = [&](R (&lb)[NC]) {
 #pragma unroll
         for (int c = 0; c < NC; c++) {
-            double m = lb[c];
+            R m = lb[c];
             for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-            if ((t & 31) == 0 && m > 0.0) atomicMax(&vmax[c], (unsigned long long)__double_as_longlong(m));
+            if ((t & 31) == 0 && m > (R)0) atomicMax(&vmax[c], (unsigned long long)__double_as_longlong((double)m));
         }
     };
     auto set_scales = [&]() {
@@ -274,14 +296,14 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
 
     if (multi) {
         // bounds over every particle first: the scale must be fixed before the first chunk
-        double lb[NC];
+        R lb[NC];
 #pragma unroll
-        for (int c = 0; c < NC; c++) lb[c] = 0.0;
+        for (int c = 0; c < NC; c++) lb[c] = 0;
         for (uint32_t j = t; j < total; j += DEP_NT) {
-            uint32_t i = seg_map(ns, seg_lo, seg_pre, j);
-            double v[NF], b[NC];
+            const uint32_t i = seg_find(seg_lo, seg_pre, j);
+            R v[NF], b[NC];
             int lc;
-            if (make_record<R, KIND, USE_PHI>(p, i, N, x0, y0, z0, phis, a, m00, mij, v, lc, b)) {
+            if (make_record<R, KIND, USE_PHI>(p, i, N, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
 #pragma unroll
                 for (int c = 0; c < NC; c++) lb[c] = fmax(lb[c], b[c]);
             }
@@ -308,17 +330,17 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
         const int n = (int)min((uint32_t)CH, total - base);
         // 1. records and cell counts
         {
-            double lb[NC];
+            R lb[NC];
 #pragma unroll
-            for (int c = 0; c < NC; c++) lb[c] = 0.0;
+            for (int c = 0; c < NC; c++) lb[c] = 0;
             for (int j = t; j < n; j += DEP_NT) {
-                uint32_t i = seg_map(ns, seg_lo, seg_pre, base + (uint32_t)j);
-                double v[NF], b[NC];
+                const uint32_t i = seg_find(seg_lo, seg_pre, base + (uint32_t)j);
+                R v[NF], b[NC];
                 int lc;
-                if (make_record<R, KIND, USE_PHI>(p, i, N, x0, y0, z0, phis, a, m00, mij, v, lc, b)) {
+                if (make_record<R, KIND, USE_PHI>(p, i, N, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
                     R *dst = rec + (size_t)j * NFP;
 #pragma unroll
-                    for (int k = 0; k < NF; k++) dst[k] = (R)v[k];
+                    for (int k = 0; k < NF; k++) dst[k] = v[k];
 #pragma unroll
                     for (int c = 0; c < NC; c++) lb[c] = fmax(lb[c], b[c]);
                     rcell[j] = (uint16_t)lc;
@@ -359,16 +381,16 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
             if (c1 < DEP_NCELL) cstart[c1] = excl + n0;
         }
         __syncthreads();
-        // 3. counting sort of record indexes by cell
+        // 3. counting sort of record indexes by cell; records take their fixed-point scales
         for (int j = t; j < n; j += DEP_NT) {
             const uint16_t lc = rcell[j];
-            if (lc != DEP_SKIP) order[cstart[lc] + rslot[j]] = (uint16_t)j;
+            if (lc != DEP_SKIP) {
+                order[cstart[lc] + rslot[j]] = (uint16_t)j;
+                scale_record<R, KIND>(rec + (size_t)j * NFP, scl_s);
+            }
         }
         __syncthreads();
         // 4. gather: the vertex receives from the cells v - b, b in {0,1}^3
-        R scl[NC];
-#pragma unroll
-        for (int c = 0; c < NC; c++) scl[c] = scl_s[c];
 #pragma unroll 1
         for (int b = 0; b < 8; b++) {
             const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
@@ -377,7 +399,7 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
             for (int k = k0; k < k1; k++) {
                 R r[NFP];
                 load_record<R, NFP>(rec + (size_t)order[k] * NFP, r);
-                gather_one<R, KIND, USE_PHI>(r, bx, by, bz, phv, phx, phy, phz, scl, acc);
+                gather_one<R, KIND, USE_PHI>(r, bx, by, bz, phv, phx, phy, phz, acc);
             }
         }
         __syncthreads();

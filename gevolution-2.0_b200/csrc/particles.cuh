@@ -28,46 +28,21 @@ struct Buckets {
     const uint32_t *start;   // nb + 1 entries (exclusive scan of counts)
 };
 
-// Gather the particle ranges a tile's deposit needs: its own 8 class buckets
-// (one contiguous range) and, from each of the 7 lower neighbour tiles, the
-// classes whose cells lie on the shared faces.  Ranges are written to
-// seg_lo/seg_hi; returns their number (at most 20).
-__device__ __forceinline__ int tile_segments(const uint32_t *bstart, int nt, int tx, int ty, int tz,
-                                             uint32_t *seg_lo, uint32_t *seg_hi)
-{
-    int ns = 0;
-    uint32_t tile = (uint32_t)tx + (uint32_t)nt * ((uint32_t)ty + (uint32_t)nt * (uint32_t)tz);
-    seg_lo[ns] = bstart[8 * tile];
-    seg_hi[ns] = bstart[8 * tile + 8];
-    if (seg_hi[ns] > seg_lo[ns]) ns++;
-    for (int m = 1; m < 8; m++) {
-        int dx = m & 1, dy = (m >> 1) & 1, dz = (m >> 2) & 1;
-        int nx = tx - dx < 0 ? nt - 1 : tx - dx;
-        int ny = ty - dy < 0 ? nt - 1 : ty - dy;
-        int nz = tz - dz < 0 ? nt - 1 : tz - dz;
-        uint32_t nb = (uint32_t)nx + (uint32_t)nt * ((uint32_t)ny + (uint32_t)nt * (uint32_t)nz);
-        for (int c = 0; c < 8; c++) {
-            if ((c & m) != m) continue;
-            uint32_t lo = bstart[8 * nb + c], hi = bstart[8 * nb + c + 1];
-            if (hi <= lo) continue;
-            if (ns > 0 && seg_hi[ns - 1] == lo) seg_hi[ns - 1] = hi;   // merge adjacent classes
-            else { seg_lo[ns] = lo; seg_hi[ns] = hi; ns++; }
-        }
-    }
-    return ns;
-}
-
-// Block-cooperative form of tile_segments: 64 threads read the 64 candidate
-// (neighbour, class) bucket ranges in parallel, thread 0 merges the non-empty
-// ones (in the same order) and builds the prefix sums.  Arrays hold 64 (+1)
-// entries.  Contains a __syncthreads(); every thread of the block must call it.
+// Particle ranges a tile's deposit needs: its own 8 class buckets and, from
+// each of the 7 lower neighbour tiles, the classes whose cells lie on the
+// shared faces.  Block-cooperative: thread k < 64 reads candidate k =
+// (neighbour offset m = k >> 3, class c = k & 7), the range of that class in
+// the neighbour tile when the class lies on the faces shared with this tile
+// (c & m == m) and an empty range otherwise; warp 0 then forms the exclusive
+// prefix sums of the 64 range lengths.  seg_lo/seg_hi hold 64 entries and
+// seg_pre 65; the particle at position i of the concatenation is found with
+// seg_find.  Contains __syncthreads(); every thread of the block must call it.
 __device__ __forceinline__ void tile_segments_block(const uint32_t *bstart, int nt, int tx, int ty, int tz,
-                                                    uint32_t *cand_lo, uint32_t *cand_hi, uint32_t *seg_lo,
-                                                    uint32_t *seg_hi, uint32_t *seg_pre, int *nseg)
+                                                    uint32_t *seg_lo, uint32_t *seg_hi, uint32_t *seg_pre)
 {
     const int t = threadIdx.x;
     if (t < 64) {
-        const int m = t >> 3, c = t & 7;   // neighbour offset bits, class
+        const int m = t >> 3, c = t & 7;
         uint32_t lo = 0, hi = 0;
         if ((c & m) == m) {
             const int dx = m & 1, dy = (m >> 1) & 1, dz = (m >> 2) & 1;
@@ -78,30 +53,33 @@ __device__ __forceinline__ void tile_segments_block(const uint32_t *bstart, int 
             lo = bstart[8 * nb + c];
             hi = bstart[8 * nb + c + 1];
         }
-        cand_lo[t] = lo;
-        cand_hi[t] = hi;
+        seg_lo[t] = lo;
+        seg_hi[t] = hi > lo ? hi : lo;
     }
     __syncthreads();
-    if (t == 0) {
-        int ns = 0;
-        for (int k = 0; k < 64; k++) {
-            const uint32_t lo = cand_lo[k], hi = cand_hi[k];
-            if (hi <= lo) continue;
-            if (ns > 0 && seg_hi[ns - 1] == lo) seg_hi[ns - 1] = hi;
-            else { seg_lo[ns] = lo; seg_hi[ns] = hi; ns++; }
+    if (t < 32) {
+        const uint32_t n0 = seg_hi[2 * t] - seg_lo[2 * t], n1 = seg_hi[2 * t + 1] - seg_lo[2 * t + 1];
+        uint32_t s = n0 + n1, incl = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (t >= o) incl += u;
         }
-        seg_pre[0] = 0;
-        for (int s = 0; s < ns; s++) seg_pre[s + 1] = seg_pre[s] + (seg_hi[s] - seg_lo[s]);
-        *nseg = ns;
+        seg_pre[2 * t] = incl - s;
+        seg_pre[2 * t + 1] = incl - s + n0;
+        if (t == 31) seg_pre[64] = incl;
     }
+    __syncthreads();
 }
 
-// map a position inside the concatenated segment list to a particle index
-__device__ __forceinline__ uint32_t seg_map(int ns, const uint32_t *seg_lo, const uint32_t *seg_pre, uint32_t i)
+// position i (< seg_pre[64]) of the concatenated candidate ranges -> particle index
+__device__ __forceinline__ uint32_t seg_find(const uint32_t *seg_lo, const uint32_t *seg_pre, uint32_t i)
 {
-    int s = 0;
-    while (s + 1 < ns && seg_pre[s + 1] <= i) s++;
-    return seg_lo[s] + (i - seg_pre[s]);
+    int lo = 0;
+#pragma unroll
+    for (int step = 32; step > 0; step >>= 1)
+        if (seg_pre[lo + step] <= i) lo += step;
+    return seg_lo[lo] + (i - seg_pre[lo]);
 }
 
 // relative coordinate of cell coordinate c to a tile origin o, in [-1, N-2]

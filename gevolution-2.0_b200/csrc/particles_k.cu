@@ -1,7 +1,8 @@
 // particles_k.cu -- geodesic kick + drift, tile re-bucketing, particle I/O.
 //
 // Kick and drift follow update_q (gevolution.hpp:888-1011, GRADIENT_ORDER 2)
-// and update_pos (:1162-1232) term by term in FP64.  One CTA handles one
+// and update_pos (:1162-1232) term by term, in the field precision R (FP32 in
+// mixed mode) with the in-cell offsets updated in FP64.  One CTA handles one
 // tile's particles and stages phi, chi and B_i over the tile plus the stencil
 // reach ([-1, 10)^3 relative to the tile origin) in shared memory, so every
 // gather is a shared-memory read.  The drift moves the cell index and the FP64
@@ -19,9 +20,9 @@ constexpr int KD_NT = 256;
 constexpr int KD_W = 11;   // staged extent per axis
 
 template <class R>
-__device__ __forceinline__ double SF(const R *s, int rx, int ry, int rz, int dx, int dy, int dz)
+__device__ __forceinline__ R SF(const R *s, int rx, int ry, int rz, int dx, int dy, int dz)
 {
-    return (double)s[(rx + 1 + dx) + KD_W * ((ry + 1 + dy) + KD_W * (rz + 1 + dz))];
+    return s[(rx + 1 + dx) + KD_W * ((ry + 1 + dy) + KD_W * (rz + 1 + dz))];
 }
 
 __device__ __forceinline__ uint32_t lanemask_lt()
@@ -44,7 +45,7 @@ __device__ __forceinline__ uint32_t bucket_slot(uint32_t b, uint32_t *counts)
 }
 
 template <class R>
-__global__ void __launch_bounds__(KD_NT) k_kick_drift(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt,
+__global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt,
                                                       const R *__restrict__ phi, const R *__restrict__ chi,
                                                       const R *__restrict__ Bi, int64_t n3, KickDriftParams kp,
                                                       uint32_t *counts, uint32_t *bucket, uint32_t *rank,
@@ -110,32 +111,35 @@ __global__ void __launch_bounds__(KD_NT) k_kick_drift(PView<R> p, const uint32_t
         const bool ok = !(rx < 0 || rx > 7 || ry < 0 || ry > 7 || rz < 0 || rz > 7);
         if (!ok) atomicOr(err, ERR_BAD_CELL);
         if (!ok) { rx = ry = rz = 0; cx = x0; cy = y0; cz = z0; }
-        double d[3] = {p.off[i], p.off[p.cap + i], p.off[2 * p.cap + i]};
-        double v[3] = {(double)p.q[i], (double)p.q[p.cap + i], (double)p.q[2 * p.cap + i]};
-        double w8[8];
+        // FP64 offsets for the position update; the interpolation weights and the
+        // geodesic arithmetic run in the field precision R
+        const double dd[3] = {p.off[i], p.off[p.cap + i], p.off[2 * p.cap + i]};
+        const R d[3] = {(R)dd[0], (R)dd[1], (R)dd[2]};
+        R v[3] = {p.q[i], p.q[p.cap + i], p.q[2 * p.cap + i]};
+        R w8[8];
 #pragma unroll
         for (int k = 0; k < 8; k++)
-            w8[k] = (((k >> 2) & 1) ? d[0] : 1.0 - d[0]) * (((k >> 1) & 1) ? d[1] : 1.0 - d[1]) * ((k & 1) ? d[2] : 1.0 - d[2]);
+            w8[k] = (((k >> 2) & 1) ? d[0] : (R)1 - d[0]) * (((k >> 1) & 1) ? d[1] : (R)1 - d[1]) * ((k & 1) ? d[2] : (R)1 - d[2]);
 
         if (kp.do_kick && ok) {
             // update_q, gevolution.hpp:888-1011
-            const double a = kp.a_k;
-            double gradphi[3];
-            double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-            double e2 = v2 + a * a;
-            double phiint = 0.0;
+            const R a = (R)kp.a_k;
+            R gradphi[3];
+            R v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+            R e2 = v2 + a * a;
+            R phiint = 0;
 #pragma unroll
             for (int k = 0; k < 8; k++) phiint += w8[k] * SF(P_, rx, ry, rz, (k >> 2) & 1, (k >> 1) & 1, k & 1);
             phiint /= e2;
-            phiint = 4. * phiint * v2 + (1. + a * a * phiint) * (v2 + e2) / e2;
+            phiint = (R)4 * phiint * v2 + ((R)1 + a * a * phiint) * (v2 + e2) / e2;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 const int ex = c == 0, ey = c == 1, ez = c == 2;
-                double g = 0.0;
+                R g = 0;
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
                     int bx = (k >> 2) & 1, by = (k >> 1) & 1, bz = k & 1;
-                    g += 0.5 * w8[k] * (SF(P_, rx, ry, rz, bx + ex, by + ey, bz + ez) - SF(P_, rx, ry, rz, bx - ex, by - ey, bz - ez));
+                    g += (R)0.5 * w8[k] * (SF(P_, rx, ry, rz, bx + ex, by + ey, bz + ez) - SF(P_, rx, ry, rz, bx - ex, by - ey, bz - ez));
                 }
                 gradphi[c] = g * phiint;
             }
@@ -156,7 +160,7 @@ __global__ void __launch_bounds__(KD_NT) k_kick_drift(PView<R> p, const uint32_t
             e2 = sqrt(e2);
             if (kp.nfield_k >= 3) {
                 // gevolution.hpp:970-993
-                double pg[3];
+                R pg[3];
                 pg[0] = ((1 - d[2]) * (SF(B1, rx, ry, rz, 1, 0, 0) - SF(B1, rx, ry, rz, 0, 0, 0)) + d[2] * (SF(B1, rx, ry, rz, 1, 0, 1) - SF(B1, rx, ry, rz, 0, 0, 1))) * v[1];
                 pg[0] += ((1 - d[1]) * (SF(B2, rx, ry, rz, 1, 0, 0) - SF(B2, rx, ry, rz, 0, 0, 0)) + d[1] * (SF(B2, rx, ry, rz, 1, 1, 0) - SF(B2, rx, ry, rz, 0, 1, 0))) * v[2];
                 pg[0] += (1 - d[1]) * (1 - d[2]) * ((d[0] - 1) * SF(B0, rx, ry, rz, -1, 0, 0) + (1 - 2 * d[0]) * SF(B0, rx, ry, rz, 0, 0, 0) + d[0] * SF(B0, rx, ry, rz, 1, 0, 0)) * v[0];
@@ -178,28 +182,28 @@ __global__ void __launch_bounds__(KD_NT) k_kick_drift(PView<R> p, const uint32_t
                 pg[2] += (1 - d[0]) * d[1] * ((d[2] - 1) * SF(B2, rx, ry, rz, 0, 1, -1) + (1 - 2 * d[2]) * SF(B2, rx, ry, rz, 0, 1, 0) + d[2] * SF(B2, rx, ry, rz, 0, 1, 1)) * v[2];
                 pg[2] += d[0] * d[1] * ((d[2] - 1) * SF(B2, rx, ry, rz, 1, 1, -1) + (1 - 2 * d[2]) * SF(B2, rx, ry, rz, 1, 1, 0) + d[2] * SF(B2, rx, ry, rz, 1, 1, 1)) * v[2];
 #pragma unroll
-                for (int c = 0; c < 3; c++) gradphi[c] += pg[c] / kp.b_k / e2;
+                for (int c = 0; c < 3; c++) gradphi[c] += pg[c] / (R)kp.b_k / e2;
             }
-            v2 = 0.0;
+            v2 = 0;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                v[c] -= kp.dtau_k * e2 * gradphi[c] * (double)N;
+                v[c] -= (R)kp.dtau_k * e2 * gradphi[c] * (R)N;
                 v2 += v[c] * v[c];
             }
-            lmax = fmax(lmax, v2 / a / a);
+            lmax = fmax(lmax, (double)(v2 / a / a));
 #pragma unroll
-            for (int c = 0; c < 3; c++) p.q[c * p.cap + i] = (R)v[c];
+            for (int c = 0; c < 3; c++) p.q[c * p.cap + i] = v[c];
         }
 
         if (kp.do_drift && ok) {
             // update_pos, gevolution.hpp:1162-1232 (drift uses the kicked momentum,
             // rounded to the storage precision as the reference stores it first)
 #pragma unroll
-            for (int c = 0; c < 3; c++) v[c] = (double)p.q[c * p.cap + i];
-            const double a = kp.a_d;
-            double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-            double e2 = v2 + a * a;
-            double ph = 0.0, ch = 0.0;
+            for (int c = 0; c < 3; c++) v[c] = p.q[c * p.cap + i];
+            const R a = (R)kp.a_d;
+            R v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+            R e2 = v2 + a * a;
+            R ph = 0, ch = 0;
             if (kp.nfield_d >= 1) {
 #pragma unroll
                 for (int k = 0; k < 8; k++) ph += w8[k] * SF(P_, rx, ry, rz, (k >> 2) & 1, (k >> 1) & 1, k & 1);
@@ -208,24 +212,24 @@ __global__ void __launch_bounds__(KD_NT) k_kick_drift(PView<R> p, const uint32_t
 #pragma unroll
                 for (int k = 0; k < 8; k++) ch += w8[k] * SF(X_, rx, ry, rz, (k >> 2) & 1, (k >> 1) & 1, k & 1);
             }
-            v2 = (1. + (3. - v2 / e2) * ph - ch) / sqrt(e2);
-            double dp[3] = {v[0] * v2, v[1] * v2, v[2] * v2};
+            v2 = ((R)1 + ((R)3 - v2 / e2) * ph - ch) / sqrt(e2);
+            R dp[3] = {v[0] * v2, v[1] * v2, v[2] * v2};
             if (kp.nfield_d >= 3) {
-                double b0 = SF(B0, rx, ry, rz, 0, 0, 0) * (1 - d[1]) * (1 - d[2]) + SF(B0, rx, ry, rz, 0, 1, 0) * d[1] * (1 - d[2]) +
+                R b0 = SF(B0, rx, ry, rz, 0, 0, 0) * (1 - d[1]) * (1 - d[2]) + SF(B0, rx, ry, rz, 0, 1, 0) * d[1] * (1 - d[2]) +
                             SF(B0, rx, ry, rz, 0, 0, 1) * (1 - d[1]) * d[2] + SF(B0, rx, ry, rz, 0, 1, 1) * d[1] * d[2];
-                double b1 = SF(B1, rx, ry, rz, 0, 0, 0) * (1 - d[0]) * (1 - d[2]) + SF(B1, rx, ry, rz, 1, 0, 0) * d[0] * (1 - d[2]) +
+                R b1 = SF(B1, rx, ry, rz, 0, 0, 0) * (1 - d[0]) * (1 - d[2]) + SF(B1, rx, ry, rz, 1, 0, 0) * d[0] * (1 - d[2]) +
                             SF(B1, rx, ry, rz, 0, 0, 1) * (1 - d[0]) * d[2] + SF(B1, rx, ry, rz, 1, 0, 1) * d[0] * d[2];
-                double b2 = SF(B2, rx, ry, rz, 0, 0, 0) * (1 - d[0]) * (1 - d[1]) + SF(B2, rx, ry, rz, 1, 0, 0) * d[0] * (1 - d[1]) +
+                R b2 = SF(B2, rx, ry, rz, 0, 0, 0) * (1 - d[0]) * (1 - d[1]) + SF(B2, rx, ry, rz, 1, 0, 0) * d[0] * (1 - d[1]) +
                             SF(B2, rx, ry, rz, 0, 1, 0) * (1 - d[0]) * d[1] + SF(B2, rx, ry, rz, 1, 1, 0) * d[0] * d[1];
-                dp[0] += b0 / kp.b_d;
-                dp[1] += b1 / kp.b_d;
-                dp[2] += b2 / kp.b_d;
+                dp[0] += b0 / (R)kp.b_d;
+                dp[1] += b1 / (R)kp.b_d;
+                dp[2] += b2 / (R)kp.b_d;
             }
             int cc[3] = {cx, cy, cz};
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                double o = d[c] + kp.dtau_d * dp[c] * (double)N;   // box units -> cell units
-                if (!isfinite(o)) { atomicOr(err, ERR_NONFINITE); o = d[c]; }
+                double o = dd[c] + kp.dtau_d * (double)dp[c] * (double)N;   // box units -> cell units
+                if (!isfinite(o)) { atomicOr(err, ERR_NONFINITE); o = dd[c]; }
                 double s = floor(o);
                 o -= s;
                 if (o >= 1.0) { o = 0.0; s += 1.0; }
