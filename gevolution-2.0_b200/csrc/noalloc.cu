@@ -1,0 +1,133 @@
+// noalloc.cu -- gev_poisson_noalloc: the Poisson solve of the phi update on
+// caller-owned device arrays, with all scratch in static device memory.
+//
+// Why it exists: gev_solve_phi works on fields that a context allocated.  Some
+// callers cannot allocate device memory at the point where they want the
+// solve: a host code that owns every device buffer through its own memory
+// pool (a caching allocator that must see every allocation), or a caller in
+// the middle of recording work into a stream where a cudaMalloc would either
+// synchronise the device or be refused.  This entry point takes the source and
+// the output as plain device pointers and keeps its one large temporary -- the
+// complex half spectrum of the transform -- in a file-scope __device__ array
+// of fixed size, so a call launches kernels and nothing else.
+//
+// Limits and rules (the same text is in include/gev.h):
+//   * N in {16, 32, 64, 128}: the static scratch holds the half spectrum of a
+//     128^3 grid in FP64 (N/2+1)*N*N*16 bytes = 17,039,360 bytes, plus the FFT
+//     and k tables.  Larger N is rejected with GEV_ERR_SIZE.
+//   * Nothing in the scratch has to start at zero: every call first writes the
+//     tables and then the whole spectrum before any of it is read.
+//   * There is one scratch per device, shared by every caller of this entry
+//     point in the process: two calls on the same device whose work overlaps
+//     in time (different streams, no ordering between them) race on it.
+//     Order such calls on one stream or synchronise between them.
+//   * The first call on each device resolves the device address of the
+//     scratch (cudaGetSymbolAddress, which can also load the library's device
+//     code); make that first call before any stream capture begins.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "gev.h"
+#include "kernels.h"
+
+namespace gev {
+namespace {
+
+constexpr int NA_MAX_N = 128;
+constexpr size_t na_align(size_t b) { return (b + 255) & ~(size_t)255; }
+constexpr size_t NA_SPEC_BYTES = na_align((size_t)(NA_MAX_N / 2 + 1) * NA_MAX_N * NA_MAX_N * sizeof(double2));
+constexpr size_t NA_TWF_BYTES = na_align((size_t)NA_MAX_N * sizeof(double2));
+constexpr size_t NA_TWH_BYTES = na_align((size_t)(NA_MAX_N / 2) * sizeof(double2));
+constexpr size_t NA_K2_BYTES = na_align((size_t)NA_MAX_N * sizeof(double));
+constexpr size_t NA_KS_BYTES = na_align((size_t)NA_MAX_N * sizeof(double2));
+constexpr size_t NA_SCRATCH_BYTES = NA_SPEC_BYTES + NA_TWF_BYTES + NA_TWH_BYTES + NA_K2_BYTES + NA_KS_BYTES;
+
+static __device__ __align__(256) unsigned char na_scratch[NA_SCRATCH_BYTES];
+
+constexpr int NA_MAX_DEVICES = 64;
+std::mutex na_mutex;
+void *na_ptr[NA_MAX_DEVICES] = {};
+
+// FFT twiddles and the k tables of gevolution.hpp:269-275 for grid size N
+template <class R>
+__global__ void k_na_tables(int N, typename CT<R>::C *tw_full, typename CT<R>::C *tw_half, double *k2, double2 *ks)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N) return;
+    double s, c;
+    sincospi(2.0 * (double)k / (double)N, &s, &c);   // exp(-2 pi i k / N)
+    tw_full[k] = mk((R)c, (R)-s);
+    if (k < N / 2) {
+        sincospi(4.0 * (double)k / (double)N, &s, &c);   // exp(-2 pi i k / (N/2))
+        tw_half[k] = mk((R)c, (R)-s);
+    }
+    sincospi((double)k / (double)N, &s, &c);
+    const double gk = 2.0 * (double)N * s;
+    k2[k] = gk * gk;
+    ks[k] = make_double2(gk * c, -gk * s);
+}
+
+template <class R>
+int na_solve(int N, const R *src, R *dst, double coeff, double modif, unsigned char *base, cudaStream_t st)
+{
+    using C = typename CT<R>::C;
+    C *spec = reinterpret_cast<C *>(base);
+    C *twf = reinterpret_cast<C *>(base + NA_SPEC_BYTES);
+    C *twh = reinterpret_cast<C *>(base + NA_SPEC_BYTES + NA_TWF_BYTES);
+    double *k2 = reinterpret_cast<double *>(base + NA_SPEC_BYTES + NA_TWF_BYTES + NA_TWH_BYTES);
+    double2 *ks = reinterpret_cast<double2 *>(base + NA_SPEC_BYTES + NA_TWF_BYTES + NA_TWH_BYTES + NA_K2_BYTES);
+    const int64_t n3 = (int64_t)N * N * N, nk = (int64_t)(N / 2 + 1) * N * N;
+
+    k_na_tables<R><<<cdiv(N, 128), 128, 0, st>>>(N, twf, twh, k2, ks);
+    const FftTables<R> tb{twf, twh, k2, ks};
+    // same pass sequence as the context's phi update without prepareFTsource
+    fx_forward<R>(N, FX_COPY, src, n3, 1, 0, nullptr, nullptr, 0.0, 0.0, 0.0, 0.0, spec, nk, nullptr, tb, st);
+    fy_pass<R>(N, -1, spec, nk, 1, tb, st);
+    FzParams fp{};
+    fp.op = OP_POISSON;
+    fp.p0 = coeff / -((double)N * (double)N * (double)N);
+    fp.p1 = modif;
+    fp.phi_hom = nullptr;
+    fz_pass<R>(N, fp, spec, nk, nullptr, nullptr, nullptr, tb, st);
+    fy_pass<R>(N, 1, spec, nk, 1, tb, st);
+    fx_inverse<R>(N, spec, nk, dst, n3, 1, tb, st);
+    return cudaGetLastError() == cudaSuccess ? GEV_OK : GEV_ERR_CUDA;
+}
+
+}  // namespace
+}  // namespace gev
+
+extern "C" int gev_poisson_noalloc(int32_t N, int32_t precision, const void *source, void *phi, double poisson_coeff,
+                                   double modif, void *stream)
+{
+    using namespace gev;
+    if (!source || !phi || (precision != GEV_FP64 && precision != GEV_MIXED)) return GEV_ERR_ARG;
+    if (N != 16 && N != 32 && N != 64 && N != 128) {
+        if (N == 256 || N == 384 || N == 512 || N == 768) return GEV_ERR_SIZE;
+        return GEV_ERR_ARG;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return GEV_ERR_CUDA;
+    if (dev < 0 || dev >= NA_MAX_DEVICES) return GEV_ERR_ARG;
+    unsigned char *base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(na_mutex);
+        if (!na_ptr[dev]) {
+            void *p = nullptr;
+            if (cudaGetSymbolAddress(&p, na_scratch) != cudaSuccess || !p) return GEV_ERR_CUDA;
+            na_ptr[dev] = p;
+        }
+        base = static_cast<unsigned char *>(na_ptr[dev]);
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    try {
+        if (precision == GEV_FP64)
+            return na_solve<double>(N, static_cast<const double *>(source), static_cast<double *>(phi), poisson_coeff,
+                                    modif, base, st);
+        return na_solve<float>(N, static_cast<const float *>(source), static_cast<float *>(phi), poisson_coeff, modif,
+                               base, st);
+    } catch (...) {
+        return GEV_ERR_CUDA;
+    }
+}

@@ -31,6 +31,7 @@ _lib = ctypes.CDLL(LIB_PATH)
 
 GEV_OK = 0
 GEV_ERR_ARG, GEV_ERR_CUDA, GEV_ERR_STATE, GEV_ERR_DEVICE, GEV_ERR_NOMEM, GEV_ERR_CAPACITY = 1, 2, 3, 4, 5, 6
+GEV_ERR_SIZE = 7
 FP64, MIXED = 0, 1
 VECTOR_PARABOLIC, VECTOR_ELLIPTIC = 0, 1
 FIELD_PHI, FIELD_CHI, FIELD_SOURCE, FIELD_SIJ, FIELD_BI, FIELD_HIJ_FT, FIELD_HIJP_FT, FIELD_BI_FT = range(8)
@@ -103,6 +104,17 @@ def rungekutta4bg(a, fourpiG, cosmo, dtau):
 
 def version():
     return _version().decode()
+
+
+_poisson_noalloc = _sig("gev_poisson_noalloc", [_i, _i, _p, _p, _d, _d, _p])
+
+
+def poisson_noalloc(N, precision, source_ptr, phi_ptr, poisson_coeff, modif, stream=None):
+    """gev_poisson_noalloc on device pointers (ints); returns the status code.
+    Queues the work on `stream` (a raw cudaStream_t handle, None = default
+    stream) without synchronising."""
+    return _poisson_noalloc(int(N), int(precision), _p(source_ptr), _p(phi_ptr), float(poisson_coeff),
+                            float(modif), _p(stream) if stream else None)
 
 
 class GevError(RuntimeError):

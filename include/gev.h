@@ -39,6 +39,7 @@ typedef struct gev_ctx gev_ctx;
 #define GEV_ERR_DEVICE  4   /* a kernel raised its device error word */
 #define GEV_ERR_NOMEM   5   /* device allocation failed */
 #define GEV_ERR_CAPACITY 6  /* output buffer too small */
+#define GEV_ERR_SIZE    7   /* grid larger than a fixed-size scratch allows */
 
 /* precision modes: FP64 everywhere, or FP32 fields/FFTs with particle
  * positions kept as cell index + FP64 offset and FP64 reductions */
@@ -211,6 +212,27 @@ int gev_step(gev_ctx *ctx, const gev_cosmo *cosmo, gev_state *st);
 double gev_hconf(double a, double fourpiG, const gev_cosmo *cosmo);
 void gev_rungekutta4bg(double *a, double fourpiG, const gev_cosmo *cosmo, double dtau);
 double gev_particle_horizon(double a, double fourpiG, const gev_cosmo *cosmo);
+
+/* Poisson solve on caller-owned device arrays, allocating no device memory.
+ * No counterpart in the reference: it serves host codes that cannot allocate
+ * at the point of the solve (their own memory pool owns every device buffer,
+ * or they are recording work into a stream).  source and phi are device
+ * arrays of N^3 values, double for GEV_FP64 and float for GEV_MIXED, layout
+ * x + N*(y + N*z); phi receives the inverse transform of
+ * coeff * FT(source) / (-N^3 (k^2 + modif)) -- the pass sequence of
+ * gev_solve_phi with prepare == 0 (solveModifiedPoissonFT, gevolution.hpp:806).
+ * Work is queued on `stream` (a cudaStream_t; NULL = the legacy default
+ * stream) and the call does not synchronise.
+ *   - N must be 16, 32, 64 or 128: the spectrum scratch is a static device
+ *     array sized for N = 128 in FP64 (about 17 MB); N = 256..768 returns
+ *     GEV_ERR_SIZE, other N and null pointers GEV_ERR_ARG.
+ *   - No part of the scratch has to start at zero.
+ *   - All callers on one device share that scratch: calls whose work overlaps
+ *     in time (unordered streams) race.  Order them on one stream.
+ *   - The first call on each device looks up the scratch address (and may
+ *     load the library's device code); make it before any stream capture. */
+int gev_poisson_noalloc(int32_t N, int32_t precision, const void *source, void *phi,
+                        double poisson_coeff, double modif, void *stream);
 
 /* Stream and synchronisation helpers for callers that time or overlap work.
  * gev_kernel_launches counts the kernels this context has launched so far. */
