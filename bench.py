@@ -128,6 +128,27 @@ def lightcone_args(gev, d):
     return gev.LightconeArgs((0.0, 0.0, 0.0), (1.0 / math.sqrt(3),) * 3, -1.0, (1.0, 0.5), d, 1, 0)
 
 
+def workload_config(N, box, world):
+    return {"workload": "PM cycle, box %g Mpc/h, grid %d^3, %d^3 particles, mixed precision, GR, elliptic B, "
+                        "full-sky lightcone shell 0.5-1.0 box lengths" % (box, N, N),
+            "N": N, "particles": N ** 3, "boxsize_mpc_h": box, "parallelism": "replicas" if world > 1 else "single GPU",
+            "l2": "inputs larger than L2 (particles %.1f GB, fields %.1f GB)" % (N ** 3 * 48 / 1e9, N ** 3 * 12 * 4 / 1e9)}
+
+
+def max_over_ranks(ms, world, device):
+    """The slowest rank's duration: every rank takes part in the same all-reduce."""
+    import torch
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, particles_per_rank, cycles, ms_max):
+    """Whole-job Mpart-steps/s: every replica advances its own particles."""
+    return world * particles_per_rank * cycles / (ms_max * 1e-3) / 1e6
+
+
 def run_gpu(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -208,11 +229,8 @@ def run_gpu(args, rank, world, local_rank):
 
     # ---- mixed precision: the headline ----
     c, st, ms, launches, clk, stream = timed_run(gev.MIXED, args.steps, args.warmup)
-    t = torch.tensor([ms], device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * np_ * args.steps / (ms_max * 1e-3) / 1e6
+    ms_max = max_over_ranks(ms, world, dev)
+    value = job_rate(world, np_, args.steps, ms_max)
 
     # ---- per-stage breakdown on the final state (CUDA events on the context stream) ----
     log("mixed: %.3f ms/cycle; stage breakdown" % (ms_max / args.steps))
@@ -304,11 +322,8 @@ def run_gpu(args, rank, world, local_rank):
         ev1.record(stream)
         ev1.synchronize()
         ms_e2e = ev0.elapsed_time(ev1)
-        t = torch.tensor([ms_e2e], device=dev)
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-        e2e = {"value": world * np_ * args.e2e_steps / (ms_e2e * 1e-3) / 1e6, "unit": "Mpart-steps/s",
+        ms_e2e = max_over_ranks(ms_e2e, world, dev)
+        e2e = {"value": job_rate(world, np_, args.e2e_steps, ms_e2e), "unit": "Mpart-steps/s",
                "h2d_bytes_per_step": int(np_ * 56), "d2h_bytes_per_step": int(np_ * 56 + lc_bytes // max(args.e2e_steps, 1)),
                "steps": args.e2e_steps}
         c.close()
@@ -326,10 +341,7 @@ def run_gpu(args, rank, world, local_rank):
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 fields/FFT + f64 particle offsets, background and reductions",
             "data": "synthetic: seeded Zel'dovich ICs (EH no-wiggle P(k)) at z=%g" % args.z_in,
-            "config": {"workload": "PM cycle, box %g Mpc/h, grid %d^3, %d^3 particles, mixed precision, GR, elliptic B, "
-                                   "full-sky lightcone shell 0.5-1.0 box lengths" % (box, N, N),
-                       "N": N, "particles": np_, "boxsize_mpc_h": box, "parallelism": "replicas" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (particles %.1f GB, fields %.1f GB)" % (np_ * 48 / 1e9, N ** 3 * 12 * 4 / 1e9)},
+            "config": workload_config(N, box, world),
             "gpu_launches": launches,
             "stage_ms": stages,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -409,10 +421,10 @@ def run_reference(args, rank):
             "warmup": 1, "ms_per_step": dt / max(1, min(args.steps, 3)) * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: seeded perturbed lattice",
-            "config": {"workload": "PM cycle sample: box %g Mpc/h, grid %d^3, %d^3 particles (same physics and cell size as "
-                                   "the 512^3 workload)" % (5.0 * Ns, Ns, Ns), "N": Ns},
+            "config": workload_config(args.N, args.boxsize or 5.0 * args.N, args.gpus),
             "cpu_baseline": {"value": rate, "unit": "Mpart-steps/s", "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
-                             "sample": "FP64 oracle cycle, %d^3, %.1f s" % (Ns, dt)},
+                             "sample": "FP64 oracle cycle (orc_step) on a %d^3 box with %d^3 particles, the same physics and "
+                                       "cell size as the workload, %d cycles in %.1f s" % (Ns, Ns, max(1, min(args.steps, 3)), dt)},
             "e2e": {"value": rate, "unit": "Mpart-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
