@@ -56,6 +56,37 @@ struct Geom {
 
 __host__ __device__ __forceinline__ int wrapi(int i, int N) { return i < 0 ? i + N : (i >= N ? i - N : i); }
 
+// Division of 32-bit unsigned values by a divisor fixed at launch time, as a
+// multiply-high and a shift (Granlund & Montgomery, "Division by invariant
+// integers using multiplication", 1994: with l = ceil(log2 d) and
+// m = floor(2^32 (2^l - d) / d) + 1, n / d = (umulhi(m, n) + n) >> l, exact
+// for every 32-bit n).  Replaces the runtime-divisor division sequence in the
+// per-particle cell decode.
+struct FastDiv {
+    uint32_t d, m;
+    int l;
+    FastDiv() = default;
+    __host__ explicit FastDiv(uint32_t div) : d(div)
+    {
+        l = 0;
+        while ((1ull << l) < div) l++;
+        m = (uint32_t)((((1ull << l) - div) << 32) / div + 1);
+    }
+    __device__ __forceinline__ uint32_t div(uint32_t n) const
+    {
+        return (uint32_t)(((uint64_t)__umulhi(m, n) + n) >> l);
+    }
+};
+
+// cell index x + N*(y + N*z) -> (x, y, z)
+__device__ __forceinline__ void decode_cell(uint32_t cell, const FastDiv &fN, int &x, int &y, int &z)
+{
+    const uint32_t q = fN.div(cell);
+    x = (int)(cell - q * fN.d);
+    z = (int)fN.div(q);
+    y = (int)(q - (uint32_t)z * fN.d);
+}
+
 __host__ __device__ __forceinline__ int64_t sidx(int N, int x, int y, int z)
 {
     return (int64_t)x + (int64_t)N * ((int64_t)y + (int64_t)N * (int64_t)z);

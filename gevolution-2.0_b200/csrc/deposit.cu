@@ -66,13 +66,13 @@ __device__ __forceinline__ int phi_slot(int vx, int vy, int vz) { return (vx + 1
 // divisions by e = sqrt(q^2 + a^2) are taken as one reciprocal, and
 // f2 / (1 + f2/a^2) as f2 a^2 / e^2 (the same quantity).
 template <class R, int KIND, bool USE_PHI>
-__device__ __forceinline__ bool make_record(const PView<R> &p, uint32_t i, int N, int x0, int y0, int z0,
+__device__ __forceinline__ bool make_record(const PView<R> &p, uint32_t i, int N, const FastDiv &fN, int x0, int y0, int z0,
                                             const R *phis, R a, R m00, R mij, R (&v)[DepShape<KIND>::NF], int &lc,
                                             R (&bnd)[DepShape<KIND>::NC])
 {
     using S = DepShape<KIND>;
-    const uint32_t cell = p.cell[i];
-    const int cx = (int)(cell % (uint32_t)N), cy = (int)((cell / (uint32_t)N) % (uint32_t)N), cz = (int)(cell / ((uint32_t)N * (uint32_t)N));
+    int cx, cy, cz;
+    decode_cell(p.cell[i], fN, cx, cy, cz);
     const int rx = rel_coord(cx, x0, N), ry = rel_coord(cy, y0, N), rz = rel_coord(cz, z0, N);
     if (rx < -1 || rx > 7 || ry < -1 || ry > 7 || rz < -1 || rz > 7) return false;
     lc = (rx + 1) + 9 * ((ry + 1) + 9 * (rz + 1));
@@ -211,7 +211,7 @@ __host__ __device__ constexpr size_t dep_smem_bytes()
 template <class R, int KIND, bool USE_PHI>
 __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt,
                                                        const R *__restrict__ phi, DepOut<R> out, double a, double m00,
-                                                       double mij, int accumulate)
+                                                       double mij, int accumulate, FastDiv fN)
 {
     using S = DepShape<KIND>;
     constexpr int NC = S::NC, NF = S::NF, NFP = S::NFP;
@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
             const uint32_t i = seg_find(seg_lo, seg_pre, j);
             R v[NF], b[NC];
             int lc;
-            if (make_record<R, KIND, USE_PHI>(p, i, N, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
+            if (make_record<R, KIND, USE_PHI>(p, i, N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
 #pragma unroll
                 for (int c = 0; c < NC; c++) lb[c] = fmax(lb[c], b[c]);
             }
@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
                 const uint32_t i = seg_find(seg_lo, seg_pre, base + (uint32_t)j);
                 R v[NF], b[NC];
                 int lc;
-                if (make_record<R, KIND, USE_PHI>(p, i, N, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
+                if (make_record<R, KIND, USE_PHI>(p, i, N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
                     R *dst = rec + (size_t)j * NFP;
 #pragma unroll
                     for (int k = 0; k < NF; k++) dst[k] = v[k];
@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
         }
         __syncthreads();
         // 4. gather: the vertex receives from the cells v - b, b in {0,1}^3
-#pragma unroll 1
+#pragma unroll
         for (int b = 0; b < 8; b++) {
             const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
             const int lc = (vx - bx + 1) + 9 * ((vy - by + 1) + 9 * (vz - bz + 1));
@@ -429,7 +429,8 @@ static void launch_k(const PView<R> &p, const uint32_t *bstart, int N, const R *
     }
     const int nt = N / 8;
     const unsigned grid = (unsigned)nt * nt * nt;
-    k_deposit<R, KIND, USE_PHI><<<grid, DEP_NT, smem, st>>>(p, bstart, N, nt, phi, out, a, m00, mij, accumulate);
+    k_deposit<R, KIND, USE_PHI><<<grid, DEP_NT, smem, st>>>(p, bstart, N, nt, phi, out, a, m00, mij, accumulate,
+                                                                      FastDiv((uint32_t)N));
 }
 
 template <class R>

@@ -69,20 +69,38 @@ __device__ __forceinline__ double gphi(const R *phi, int N, int x, int y, int z)
 template <class R>
 __global__ void k_lightcone(PView<R> p, int N, const R *__restrict__ phi, LcKernelArgs la, float *opos, float *ovel,
                             int64_t *oid, unsigned long long *count, unsigned long long *newlog, int64_t newlog_cap,
-                            int *err)
+                            int *err, FastDiv fN)
 {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= p.n) return;
-    const int64_t id = p.id[i];
-    if (la.tracer_factor > 1 && id % la.tracer_factor != 0) return;
+    if (la.tracer_factor > 1 && p.id[i] % la.tracer_factor != 0) return;
     const uint32_t cell = p.cell[i];
     if ((int64_t)cell >= (int64_t)N * N * N) { atomicOr(err, ERR_BAD_CELL); return; }
-    const int c[3] = {(int)(cell % (uint32_t)N), (int)((cell / (uint32_t)N) % (uint32_t)N), (int)(cell / ((uint32_t)N * (uint32_t)N))};
+    int c[3];
+    decode_cell(cell, fN, c[0], c[1], c[2]);
     const double fr[3] = {p.off[i], p.off[p.cap + i], p.off[2 * p.cap + i]};
+
+    // FP32 pre-test of the shell radius with a margin far above the FP32
+    // rounding of |x - V|^2 (|x - V| < 4 box lengths): only particles that may
+    // lie in the shell take the exact FP64 test below
+    const float invN = 1.0f / (float)N;
+    const float xf[3] = {((float)c[0] + (float)fr[0]) * invN, ((float)c[1] + (float)fr[1]) * invN,
+                         ((float)c[2] + (float)fr[2]) * invN};
+    const float in2 = (float)(la.inner * la.inner) * (1.0f - 1e-4f) - 1e-5f;
+    const float out2 = (float)(la.outer * la.outer) * (1.0f + 1e-4f) + 1e-5f;
+    int v = 0;
+    for (; v < la.nvtx; v++) {
+        const float r0 = xf[0] - (float)la.vtx[v][0], r1 = xf[1] - (float)la.vtx[v][1], r2 = xf[2] - (float)la.vtx[v][2];
+        const float d2 = r0 * r0 + r1 * r1 + r2 * r2;
+        if (d2 >= in2 && d2 < out2) break;
+    }
+    if (v == la.nvtx) return;
+
+    const int64_t id = p.id[i];
     const double x[3] = {(c[0] + fr[0]) / N, (c[1] + fr[1]) / N, (c[2] + fr[2]) / N};
     const double q[3] = {(double)p.q[i], (double)p.q[p.cap + i], (double)p.q[2 * p.cap + i]};
 
-    for (int v = 0; v < la.nvtx; v++) {
+    for (; v < la.nvtx; v++) {
         const double *V = la.vtx[v];
         double r[3] = {x[0] - V[0], x[1] - V[1], x[2] - V[2]};
         double d = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
@@ -140,7 +158,8 @@ void launch_lightcone(const PView<R> &p, int N, const R *phi, const LcKernelArgs
                       cudaStream_t st)
 {
     if (p.n > 0)
-        k_lightcone<R><<<cdiv(p.n, 256), 256, 0, st>>>(p, N, phi, la, pos, vel, ids, count, newlog, newlog_cap, err);
+        k_lightcone<R><<<cdiv(p.n, 256), 256, 0, st>>>(p, N, phi, la, pos, vel, ids, count, newlog, newlog_cap, err,
+                                                        FastDiv((uint32_t)N));
 }
 
 template void launch_lightcone<float>(const PView<float> &, int, const float *, const LcKernelArgs &, float *, float *,

@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
                                                       const R *__restrict__ phi, const R *__restrict__ chi,
                                                       const R *__restrict__ Bi, int64_t n3, KickDriftParams kp,
                                                       uint32_t *counts, uint32_t *bucket, uint32_t *rank,
-                                                      unsigned long long *vmax_bits, int *err)
+                                                      unsigned long long *vmax_bits, int *err, FastDiv fN)
 {
     extern __shared__ __align__(16) unsigned char kd_smem[];
     R(*sf)[KD_W * KD_W * KD_W] = reinterpret_cast<R(*)[KD_W * KD_W * KD_W]>(kd_smem);
@@ -103,8 +103,8 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
     for (uint32_t base = lo; base < hi; base += KD_NT) {
         uint32_t i = base + threadIdx.x;
         if (i >= hi) continue;
-        uint32_t cell = p.cell[i];
-        int cx = (int)(cell % (uint32_t)N), cy = (int)((cell / (uint32_t)N) % (uint32_t)N), cz = (int)(cell / ((uint32_t)N * (uint32_t)N));
+        int cx, cy, cz;
+        decode_cell(p.cell[i], fN, cx, cy, cz);
         int rx = cx - x0, ry = cy - y0, rz = cz - z0;
         // a particle outside this tile means the bucket order is stale: flag it, leave it
         // unmoved (never read outside the stage) and still give it a bucket slot
@@ -234,8 +234,11 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
                 o -= s;
                 if (o >= 1.0) { o = 0.0; s += 1.0; }
                 long long sh = (long long)s;
-                long long nc = ((long long)cc[c] + sh) % N;
-                if (nc < 0) nc += N;
+                long long nc = (long long)cc[c] + sh;
+                if (nc < 0 || nc >= N) {   // crossed the periodic boundary (or moved far)
+                    nc %= N;
+                    if (nc < 0) nc += N;
+                }
                 cc[c] = (int)nc;
                 p.off[c * p.cap + i] = o;
             }
@@ -272,7 +275,7 @@ void launch_kick_drift(const PView<R> &p, const uint32_t *bstart, int N, const R
         attr_set = true;
     }
     k_kick_drift<R><<<(unsigned)nt * nt * nt, KD_NT, smem, st>>>(p, bstart, N, nt, phi, chi, Bi, n3, kp, counts,
-                                                                bucket, rank, vmax_bits, err);
+                                                                bucket, rank, vmax_bits, err, FastDiv((uint32_t)N));
 }
 
 // ---- particle I/O: host layout (box-unit positions, AoS triples) <-> cell + offset ----
