@@ -128,6 +128,15 @@ def lightcone_args(gev, d):
     return gev.LightconeArgs((0.0, 0.0, 0.0), (1.0 / math.sqrt(3),) * 3, -1.0, (1.0, 0.5), d, 1, 0)
 
 
+# DRAM bytes per launch measured by ncu at 256^3 (mixed precision), per stage kernel
+NCU_TRAFFIC_256 = {"deposit_T00_Tij": 0.743822e9 + 0.443273e9, "deposit_T0i": 0.742488e9 + 0.188677e9}
+
+
+def ncu_traffic(stage, N):
+    t = NCU_TRAFFIC_256.get(stage)
+    return None if t is None else t * (N / 256.0) ** 3
+
+
 def workload_config(N, box, world):
     return {"workload": "PM cycle, box %g Mpc/h, grid %d^3, %d^3 particles, mixed precision, GR, elliptic B, "
                         "full-sky lightcone shell 0.5-1.0 box lengths" % (box, N, N),
@@ -345,7 +354,9 @@ def run_gpu(args, rank, world, local_rank):
             "gpu_launches": launches,
             "stage_ms": stages,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": ncu_traffic(dom, N),
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same kernel at 256^3 "
+                                           "(profiles/deposit_kick_256_mixed_ncu.md), scaled by the particle count",
                          "algorithmic_bytes_per_launch": dom_bytes,
                          "step_algorithmic_bytes": step_alg, "step_achieved_gbs": step_gbs, "step_frac": step_gbs / peak},
             "clocks": clk,
