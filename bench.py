@@ -53,6 +53,10 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    p.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-run measurement")
+    p.add_argument("--adj-N", type=int, default=128)
+    p.add_argument("--adj-steps", type=int, default=32)
+    p.add_argument("--adj-modes", type=int, default=64)
     p.add_argument("--cpu-sample-N", type=int, default=128)
     p.add_argument("--cpu-sample-steps", type=int, default=2)
     return p.parse_args()
@@ -337,6 +341,12 @@ def run_gpu(args, rank, world, local_rank):
                "steps": args.e2e_steps}
         c.close()
 
+    # ---- differentiable run: adjoint cost and gradient checks, rank 0 only ----
+    adj = None
+    if rank == 0 and not args.no_adjoint:
+        log("adjoint")
+        adj = adjoint_block(args, dev)
+
     # ---- CPU baseline: the oracle on a bounded sample, rank 0 only ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -363,6 +373,7 @@ def run_gpu(args, rank, world, local_rank):
             "fp64": fp64,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "adjoint": adj,
         }
         print(json.dumps(line), flush=True)
 
@@ -408,6 +419,93 @@ def oracle_cycle_rate(Ns, steps, seed):
         o.lib.orc_step(ctypes.byref(sim), ctypes.byref(st), len(pos), ptr(pos), ptr(q), ptr(phi), ptr(chi), ptr(Bi))
     dt = time.perf_counter() - t0
     return Ns ** 3 * steps / dt / 1e6, dt
+
+
+def adjoint_block(args, dev):
+    """Differentiable Newtonian run (box 640 Mpc/h at 128^3, 32 steps from z = 50
+    to 0, checkpoints every 8 steps): forward and adjoint device times, their
+    ratio, and the gradient checks (central differences on random white-noise
+    modes, FP64 adjoint against the mixed-precision one)."""
+    import numpy as np
+    import torch
+
+    import gevb200 as gev
+    from gevb200 import pm as gpm
+
+    N, nsteps = args.adj_N, args.adj_steps
+    box = 5.0 * N
+    fourpiG = 1.5 * box * box / C_LIGHT ** 2
+    a_in = 1.0 / 51.0
+    coef, _ = gpm.schedule(N, fourpiG, OMEGA_M, OMEGA_L, a_in, 1.0, nsteps)
+    g = torch.Generator(device="cpu").manual_seed(args.seed + 77)
+    noise = torch.randn(N ** 3, generator=g, dtype=torch.float64).to(dev)
+    target = 0.5 * torch.randn(N ** 3, generator=g, dtype=torch.float64).to(dev)
+    mass = OMEGA_M / N ** 3
+
+    def run(precision, w, timed=False):
+        p = gpm.PM(N, N ** 3, mass, precision, checkpoint_every=8)
+        x0, q0 = gpm.zeldovich_map(w, N, box, a_in, fourpiG, OMEGA_M, OMEGA_L, H_LITTLE)
+        x0, q0 = x0.detach().contiguous(), q0.detach().contiguous()
+        delta = torch.empty(N ** 3, dtype=torch.float64, device=dev)
+        st = torch.cuda.ExternalStream(p.stream())
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        torch.cuda.synchronize()
+        e[0].record(st)
+        p.forward(coef, x0, q0, delta)
+        e[1].record(st)
+        gd = (2.0 * (delta - target)).contiguous()
+        gx = torch.empty_like(x0)
+        gq = torch.empty_like(q0)
+        torch.cuda.synchronize()
+        e[2].record(st)
+        p.adjoint(gd, gx, gq)
+        e[3].record(st)
+        torch.cuda.synchronize()
+        loss = float(((delta - target) ** 2).sum())
+        return loss, gx, gq, e[0].elapsed_time(e[1]), e[2].elapsed_time(e[3]), p
+
+    def grad_modes(precision, w):
+        wv = w.clone().requires_grad_(True)
+        x0, q0 = gpm.zeldovich_map(wv, N, box, a_in, fourpiG, OMEGA_M, OMEGA_L, H_LITTLE)
+        p = gpm.PM(N, N ** 3, mass, precision, checkpoint_every=8)
+        delta = gpm.run_function().apply(x0, q0, p, coef)
+        ((delta - target) ** 2).sum().backward()
+        return wv.grad.detach()
+
+    def loss_of(w):
+        p = gpm.PM(N, N ** 3, mass, gev.FP64, checkpoint_every=8)
+        x0, q0 = gpm.zeldovich_map(w, N, box, a_in, fourpiG, OMEGA_M, OMEGA_L, H_LITTLE)
+        delta = torch.empty(N ** 3, dtype=torch.float64, device=dev)
+        p.forward(coef, x0.contiguous(), q0.contiguous(), delta)
+        return float(((delta - target) ** 2).sum())
+
+    out = {"config": {"workload": "differentiable Newtonian PM run (main.cu gr_flag = 0): box %g Mpc/h, grid %d^3, "
+                                  "%d^3 particles, %d steps z = 50 -> 0, loss sum (delta_CIC - target)^2, checkpoints "
+                                  "every 8 steps" % (box, N, N, nsteps), "N": N, "steps": nsteps}}
+    for name, prec in (("mixed", gev.MIXED), ("fp64", gev.FP64)):
+        run(prec, noise)                       # warm-up
+        times = [run(prec, noise)[3:5] for _ in range(3)]
+        fwd = min(t[0] for t in times)
+        adjm = min(t[1] for t in times)
+        out[name] = {"fwd_ms": fwd, "adjoint_ms": adjm, "grad_fwd_ratio": adjm / fwd,
+                     "fwd_mpart_steps_s": N ** 3 * nsteps / (fwd * 1e-3) / 1e6}
+    g64 = grad_modes(gev.FP64, noise)
+    g32 = grad_modes(gev.MIXED, noise)
+    rng = np.random.default_rng(args.seed)
+    modes = rng.choice(N ** 3, size=args.adj_modes, replace=False)
+    eps = 1e-4
+    fd = []
+    for m in modes:
+        d = torch.zeros_like(noise)
+        d[int(m)] = eps
+        fd.append((loss_of(noise + d) - loss_of(noise - d)) / (2 * eps))
+    fd = np.array(fd)
+    ad = g64.cpu().numpy()[modes]
+    out["checks"] = {"fd_modes": int(args.adj_modes), "fd_eps": eps,
+                     "fd_vs_fp64_adjoint_rel_err": float(np.linalg.norm(fd - ad) / np.linalg.norm(ad)),
+                     "mixed_vs_fp64_adjoint_rel_err": float(torch.linalg.norm(g32 - g64) / torch.linalg.norm(g64))}
+    out["grad_fwd_ratio"] = out["mixed"]["grad_fwd_ratio"]
+    return out
 
 
 def cpu_sample(args):

@@ -234,6 +234,39 @@ double gev_particle_horizon(double a, double fourpiG, const gev_cosmo *cosmo);
 int gev_poisson_noalloc(int32_t N, int32_t precision, const void *source, void *phi,
                         double poisson_coeff, double modif, void *stream);
 
+/* ---- Differentiable Newtonian PM run and its adjoint ----
+ * A run of nsteps Newtonian particle-mesh steps, main.cu's gr_flag == 0 branch
+ * for CDM: scalarProjectionCIC_project (gevolution.hpp:1902), FFT,
+ * solveModifiedPoissonFT(src, pot, pc_n) (:806; main.cu:765), FFT^-1,
+ * update_q_Newton (:1051, GRADIENT_ORDER 2; main.cu:1238) and update_pos_Newton
+ * (:1270; main.cu:1264), followed by the CIC density contrast of the final
+ * positions.  gev_pm_adjoint is the hand-written reverse of that run: it
+ * returns d(loss)/d(x0), d(loss)/d(q0) for a given d(loss)/d(delta), recomputing
+ * the states from checkpoints (x, q) kept every checkpoint_every steps.  No
+ * counterpart in the reference (gevolution has no adjoint).
+ * Particles are in ID order: x0, q0 are device arrays of np*3 doubles (box units,
+ * unwrapped; momentum per unit mass), delta N^3 doubles.  coef holds 3 host
+ * doubles per step: kq_n = dtau_kick * a * N (update_q_Newton's dtau * a / dx),
+ * kx_n = dtau / a_half (update_pos_Newton's dtau / a), pc_n = fourpiG / a (the
+ * Poisson coefficient).  Both calls synchronise. */
+typedef struct gev_pm gev_pm;
+typedef struct {
+    int32_t N;                 /* grid points per side (as gev_config) */
+    int32_t precision;         /* GEV_FP64 or GEV_MIXED (FP32 fields and FFTs) */
+    int64_t np;                /* number of particles */
+    double mass;               /* per-particle mass of the Poisson source (part_simple_info.mass) */
+    int32_t checkpoint_every;  /* steps between stored (x, q) checkpoints */
+    int32_t device;
+} gev_pm_config;
+
+int gev_pm_create(const gev_pm_config *cfg, gev_pm **out);
+int gev_pm_destroy(gev_pm *pm);
+const char *gev_pm_last_error(const gev_pm *pm);
+int gev_pm_forward(gev_pm *pm, int32_t nsteps, const double *coef, const double *x0, const double *q0,
+                   double *delta, double *x_out, double *q_out);
+int gev_pm_adjoint(gev_pm *pm, const double *ddelta, double *gx0, double *gq0);
+void *gev_pm_stream(gev_pm *pm);
+
 /* Stream and synchronisation helpers for callers that time or overlap work.
  * gev_kernel_launches counts the kernels this context has launched so far. */
 int gev_synchronize(gev_ctx *ctx);

@@ -655,6 +655,43 @@ double orc_update_q(int N, int64_t np, const double *pos, double *q, const doubl
     return sqrt(vmax);
 }
 
+/* update_q_Newton: gevolution.hpp:1051-1118 (GRADIENT_ORDER 2, nfield 1):
+ * q -= dtau * a * grad psi / dx; returns max q^2 / a^2 over the particles */
+double orc_update_q_newton(int N, int64_t np, const double *pos, double *q, const double *psi, double dtau,
+                           double a)
+{
+    const double dx = 1.0 / N;
+    double vmax = 0;
+#pragma omp parallel for reduction(max : vmax) schedule(static)
+    for (int64_t p = 0; p < np; p++) {
+        int c[3]; double d[3];
+        locate(N, pos + 3 * p, c, d);
+        double *v = q + 3 * p;
+        double v2 = 0;
+        for (int i = 0; i < 3; i++) {
+            int ei[3] = {i == 0, i == 1, i == 2};
+            double g = 0;
+            for (int k = 0; k < 8; k++) {
+                int bx = (k >> 2) & 1, by = (k >> 1) & 1, bz = k & 1;
+                g += 0.5 * cicw(d, k) * (F(psi, N, c, bx + ei[0], by + ei[1], bz + ei[2]) -
+                                         F(psi, N, c, bx - ei[0], by - ei[1], bz - ei[2]));
+            }
+            v[i] -= dtau * a * g / dx;
+            v2 += v[i] * v[i];
+        }
+        if (v2 / a / a > vmax) vmax = v2 / a / a;
+    }
+    return vmax;
+}
+
+/* update_pos_Newton: gevolution.hpp:1270-1273, pos += dtau q / a (positions
+ * left unwrapped: the differentiable run keeps continuous coordinates) */
+void orc_update_pos_newton(int64_t np, double *pos, const double *q, double dtau, double a)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < 3 * np; p++) pos[p] += dtau * q[p] / a;
+}
+
 /* update_pos: gevolution.hpp:1162-1232; positions wrapped into [0,1) as
  * LATfield2's moveParticles re-bins them on the periodic lattice. */
 void orc_update_pos(int N, int64_t np, double *pos, const double *q, const double *phi,

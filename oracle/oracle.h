@@ -65,6 +65,11 @@ void orc_update_pos(int N, int64_t np, double *pos, const double *q, const doubl
                     const double *chi, const double *Bi, int nfield, double dtau,
                     double a, double bcoeff);
 
+/* ---- Newtonian kick and drift (main.cu's gr_flag == 0 branch) ---- */
+double orc_update_q_newton(int N, int64_t np, const double *pos, double *q, const double *psi, double dtau,
+                           double a);
+void orc_update_pos_newton(int64_t np, double *pos, const double *q, double dtau, double a);
+
 /* ---- background (CDM + Lambda + radiation, no ncdm / fluid) ---- */
 typedef struct {
     double Omega_m, Omega_Lambda, Omega_rad;

@@ -222,6 +222,29 @@ void ref_update_pos(int N, int64_t np, double * pos, const double * q, const dou
 		for (int i = 0; i < 3; i++) pos[3 * p + i] = ps.parts[p].pos[i];
 }
 
+// update_q_Newton (gevolution.hpp:1051-1118) through perfParticles::updateVel
+double ref_update_q_newton(int N, int64_t np, const double * pos, double * q, const double * psi, double dtau, double a)
+{
+	ParticleSet ps(N, np, pos, q, 0.);
+	Field<Real> fpsi(ps.lat, const_cast<double *>(psi), 1);
+	Field<Real> * fields[2] = {&fpsi, nullptr};
+	double params[7] = {a, 0, 0, 0, 0, 0, 0};
+	double vmax = ps.pcls.updateVel(update_q_Newton_functor(), dtau, fields, 1, params);
+	for (int64_t p = 0; p < np; p++)
+		for (int i = 0; i < 3; i++) q[3 * p + i] = ps.parts[p].vel[i];
+	return vmax;
+}
+
+// update_pos_Newton (gevolution.hpp:1270-1273) through perfParticles::moveParticles
+void ref_update_pos_newton(int N, int64_t np, double * pos, const double * q, double dtau, double a)
+{
+	ParticleSet ps(N, np, pos, q, 0.);
+	double params[7] = {a, 0, 0, 0, 0, 0, 0};
+	ps.pcls.moveParticles(update_pos_Newton_functor(), dtau, nullptr, 0, params);
+	for (int64_t p = 0; p < np; p++)
+		for (int i = 0; i < 3; i++) pos[3 * p + i] = ps.parts[p].pos[i];
+}
+
 // background.hpp:200-291
 double ref_hconf(double a, double fourpiG, double Om, double OL, double Orad)
 {

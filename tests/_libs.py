@@ -39,6 +39,7 @@ _SIGS = {
     "update_q": ([_i, _l, _p, _p, _p, _p, _p, _i, _d, _d, _d], _d),
     "update_pos": ([_i, _l, _p, _p, _p, _p, _p, _i, _d, _d, _d], None),
     "power_spectrum": ([_i, _p, _i, _p, _p, _p, _p, _p], None),
+    "update_q_newton": ([_i, _l, _p, _p, _p, _d, _d], _d),
 }
 
 
@@ -62,8 +63,10 @@ _ORC_EXTRA = {
     "particle_horizon": ([_d, _d, _p], _d),
     "lightcone_select": ([_i, _l, _p, _p, _p, _p, _p, _d, _d, _d, _d, _d, _l, _p, _p, _p, _d], _l),
     "find_intersecting": ([_p, _p, _d, _d, _d, _p, _p], _i),
+    "update_pos_newton": ([_l, _p, _p, _d, _d], None),
 }
 _REF_EXTRA = {
+    "update_pos_newton": ([_i, _l, _p, _p, _d, _d], None),
     "hconf": ([_d, _d, _d, _d, _d], _d),
     "rk4bg": ([_d, _d, _d, _d, _d, _d], _d),
     "particle_horizon": ([_d, _d, _d, _d, _d], _d),

@@ -157,6 +157,25 @@ def test_kick_drift_match_reference(libs, nfield):
         assert np.abs(d).max() < 1e-15
 
 
+def test_newton_kick_drift_match_reference(libs):
+    """update_q_Newton / update_pos_Newton (main.cu's gr_flag == 0 branch)."""
+    o, r = libs
+    N = 16
+    pos, q, _ = particles(N, n=2000, seed=8)
+    psi = trough_phi(N)
+    qa, qb = q.copy(), q.copy()
+    va = o.update_q_newton(N, len(pos), ptr(pos), ptr(qa), ptr(psi), 0.05, 0.3)
+    vb = r.update_q_newton(N, len(pos), ptr(pos), ptr(qb), ptr(psi), 0.05, 0.3)
+    assert rel_err(qa, qb) < 1e-14
+    assert abs(va / vb - 1) < 1e-14 or abs(np.sqrt(va) / vb - 1) < 1e-14
+    pa, pb = pos.copy(), pos.copy()
+    o.update_pos_newton(len(pos), ptr(pa), ptr(qa), 0.3, 0.31)
+    r.update_pos_newton(N, len(pos), ptr(pb), ptr(qa), 0.3, 0.31)
+    d = pa - pb
+    d -= np.round(d)          # the oracle keeps unwrapped positions, the reference wraps
+    assert np.abs(d).max() < 1e-15
+
+
 def test_background_matches_reference(libs):
     o, r = libs
     c = OrcCosmo(0.32, 0.68, 8.5e-5)
