@@ -176,11 +176,88 @@ __global__ void __launch_bounds__(NT) k_fx_fwd(FxArgs<R> a, int64_t in_stride, i
     }
 }
 
+// prepareFTsource_Tij for all six components at one point from the ten
+// potential values they share; the arithmetic of each component is that of
+// prep_tij (same expressions, same order), so the results are identical.
+template <class R>
+__device__ __forceinline__ void prep_tij6(const R *T, int64_t n3, const R *phi, R coeff, int N, int x, int y, int z,
+                                          R o[6])
+{
+    const int64_t i = sidx(N, x, y, z);
+    const R p0 = __ldg(phi + i);
+    const R pxp = ldr(phi, N, x + 1, y, z), pxm = ldr(phi, N, x - 1, y, z);
+    const R pyp = ldr(phi, N, x, y + 1, z), pym = ldr(phi, N, x, y - 1, z);
+    const R pzp = ldr(phi, N, x, y, z + 1), pzm = ldr(phi, N, x, y, z - 1);
+    const R pxy = ldr(phi, N, x + 1, y + 1, z), pxz = ldr(phi, N, x + 1, y, z + 1), pyz = ldr(phi, N, x, y + 1, z + 1);
+    R t[6];
+#pragma unroll
+    for (int c = 0; c < 6; c++) t[c] = __ldg(T + c * n3 + i);
+    R g;
+    g = pxp - pxm; o[0] = (R)0.5 * g * g + coeff * t[0];
+    g = pyp - pym; o[3] = (R)0.5 * g * g + coeff * t[3];
+    g = pzp - pzm; o[5] = (R)0.5 * g * g + coeff * t[5];
+    R u, v, w;
+    u = pxp - p0; v = pyp - p0; w = (pxy - pxp) - (pyp - p0);
+    o[1] = (R)2 * u * v + w * (u + v + (R)0.5 * w) + coeff * t[1];
+    u = pxp - p0; v = pzp - p0; w = (pxz - pxp) - (pzp - p0);
+    o[2] = (R)2 * u * v + w * (u + v + (R)0.5 * w) + coeff * t[2];
+    u = pyp - p0; v = pzp - p0; w = (pyz - pyp) - (pzp - p0);
+    o[4] = (R)2 * u * v + w * (u + v + (R)0.5 * w) + coeff * t[4];
+}
+
+// x pass, forward, for the six Tij components at once: each potential value
+// is loaded once for all six sources.  grid (N/T, N)
+template <class R, int N, int T, int NT>
+__global__ void __launch_bounds__(NT) k_fx_fwd_tij6(const R *__restrict__ Tij, int64_t n3, const R *__restrict__ phi,
+                                                    double coeff, typename CT<R>::C *out, int64_t out_stride,
+                                                    const typename CT<R>::C *__restrict__ tw_half,
+                                                    const typename CT<R>::C *__restrict__ tw_full)
+{
+    using C = typename CT<R>::C;
+    constexpr int M = N / 2, P = N / 2 + 1, LD = T + 1, CS = M * LD;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *buf = reinterpret_cast<C *>(smem_raw);   // 6 component buffers of CS
+    const int y0 = blockIdx.x * T, z = blockIdx.y;
+    const R rc = (R)coeff;
+    struct Six { C v[6]; };
+    staged_fill<M * T, NT, 2, Six>(
+        [&](int idx) {
+            const int n = idx % M, t = idx / M, y = y0 + t;
+            R a0[6], a1[6];
+            prep_tij6(Tij, n3, phi, rc, N, 2 * n, y, z, a0);
+            prep_tij6(Tij, n3, phi, rc, N, 2 * n + 1, y, z, a1);
+            Six s;
+#pragma unroll
+            for (int c = 0; c < 6; c++) s.v[c] = mk(a0[c], a1[c]);
+            return s;
+        },
+        [&](int idx, Six s) {
+            const int o = (idx % M) * LD + idx / M;
+#pragma unroll
+            for (int c = 0; c < 6; c++) buf[c * CS + o] = s.v[c];
+        });
+    __syncthreads();
+#pragma unroll 1
+    for (int c = 0; c < 6; c++) fft_lines<M, -1, T, NT>(buf + c * CS, LD, tw_half);
+    for (int idx = threadIdx.x; idx < 6 * P * T; idx += NT) {
+        const int k = idx % P, r = idx / P, t = r % T, c = r / T, y = y0 + t;
+        const C *b = buf + c * CS;
+        C zk = b[(k == M ? 0 : k) * LD + t];
+        C zm = b[(k == 0 ? 0 : M - k) * LD + t];
+        zm.y = -zm.y;
+        C ze = cscale(cadd(zk, zm), R(0.5));
+        C d = csub(zk, zm);
+        C zo = mk(R(0.5) * d.y, R(-0.5) * d.x);
+        C w = __ldg(tw_full + k);
+        out[c * out_stride + k + (int64_t)P * (y + (int64_t)N * z)] = cadd(ze, cmul(w, zo));
+    }
+}
+
 // ---------------------------------------------------------------------------
 // y pass (in place), complex.  grid (ceil(P/T), N, ncomp)
 // ---------------------------------------------------------------------------
 template <class R, int N, int T, int NT, int S>
-__global__ void __launch_bounds__(NT, 4) k_fy(typename CT<R>::C *data, int64_t stride,
+__global__ void __launch_bounds__(NT, 1024 / NT) k_fy(typename CT<R>::C *data, int64_t stride,
                                            const typename CT<R>::C *__restrict__ tw)
 {
     using C = typename CT<R>::C;
@@ -302,6 +379,10 @@ __device__ __forceinline__ void tt_num(const double *g, const double2 *k, double
 template <int OP, int EXTRA> struct OpShape {
     static constexpr int CIN = (OP == OP_POISSON || OP == OP_BIN) ? 1 : (OP == OP_SCALAR ? 6 : 3);
     static constexpr int COUT = (OP == OP_BIN) ? 0 : ((OP == OP_POISSON) ? 1 : (OP == OP_SCALAR ? ((EXTRA & EXTRA_VECTOR_EVOLVE) ? 4 : 1) : 3));
+    // projectFTscalar alone needs only three kz-independent combinations of the
+    // six S_ij (see k_fz), so the z pass transforms three columns instead of six
+    static constexpr bool CONTRACT = (OP == OP_SCALAR && EXTRA == 0);
+    static constexpr int CBUF = CONTRACT ? 3 : CIN;
 };
 
 // Element-wise solver for one (kx, ky, kz): reads CIN values from v, writes
@@ -431,41 +512,102 @@ __device__ __forceinline__ void fz_apply(const FzArgs<R> &a, int N, int kx, int 
 }
 
 // grid (ceil(P/T), N); T kx-columns at one ky, all CIN components of the solve.
+//
+// projectFTscalar (gevolution.hpp:251-340) without tensor or vector extras:
+//   chi 2 k^4 N = S00 (g1+g2-2g0) + S11 (g0+g2-2g1) + S22 (g0+g1-2g2)
+//                 - 6 (k0 k1 S01 + k0 k2 S02 + k1 k2 S12)
+//               = A + g2 B - 6 k2 C, with
+//   A = S00 (g1-2g0) + S11 (g0-2g1) + S22 (g0+g1) - 6 k0 k1 S01,
+//   B = S00 + S11 - 2 S22,   C = k0 S02 + k1 S12.
+// A, B, C have coefficients that depend on kx, ky only, so they are formed
+// (in FP64) while the pencils load and the z transform -- linear, along kz --
+// acts on three columns instead of six.
 template <class R, int N, int T, int NT, int OP, int EXTRA>
-__global__ void __launch_bounds__(NT, 2) k_fz(FzArgs<R> a, const typename CT<R>::C *__restrict__ tw)
+__global__ void __launch_bounds__(NT, 512 / NT) k_fz(FzArgs<R> a, const typename CT<R>::C *__restrict__ tw)
 {
     using C = typename CT<R>::C;
     constexpr int P = N / 2 + 1;
     constexpr int CIN = OpShape<OP, EXTRA>::CIN, COUT = OpShape<OP, EXTRA>::COUT;
-    constexpr int LD = CIN * T + 1;
+    constexpr bool CONTRACT = OpShape<OP, EXTRA>::CONTRACT;
+    constexpr int CBUF = OpShape<OP, EXTRA>::CBUF;
+    constexpr int LD = CBUF * T + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *buf = reinterpret_cast<C *>(smem_raw);
     const int kx0 = blockIdx.x * T, ky = blockIdx.y;
 
-    staged_fill<N * CIN * T, NT, 8, C>(
-        [&](int idx) {
-            const int t = idx % T, r = idx / T, c = r % CIN, n = r / CIN, kx = kx0 + t;
-            return (kx < P) ? a.data[c * a.stride + kx + (int64_t)P * (ky + (int64_t)N * n)] : mk(R(0), R(0));
-        },
-        [&](int idx, C v) {
-            const int t = idx % T, r = idx / T, c = r % CIN, n = r / CIN;
-            buf[n * LD + c * T + t] = v;
-        });
+    if constexpr (CONTRACT) {
+        struct ABC { C v[3]; };
+        staged_fill<N * T, NT, 2, ABC>(
+            [&](int idx) {
+                const int t = idx % T, n = idx / T, kx = kx0 + t;
+                ABC o;
+                if (kx >= P) {
+                    o.v[0] = o.v[1] = o.v[2] = mk(R(0), R(0));
+                    return o;
+                }
+                const int64_t k = kx + (int64_t)P * (ky + (int64_t)N * n);
+                double2 S[6];
+#pragma unroll
+                for (int c = 0; c < 6; c++) S[c] = z2d(a.data[c * a.stride + k]);
+                const double g0 = __ldg(a.k2 + kx), g1 = __ldg(a.k2 + ky);
+                const double2 k0 = __ldg(a.ks + kx), k1 = __ldg(a.ks + ky);
+                const double2 A = zsub(zadd(zadd(zsc(S[0], g1 - 2.0 * g0), zsc(S[3], g0 - 2.0 * g1)), zsc(S[5], g0 + g1)),
+                                       zsc(zmul(zmul(k0, k1), S[1]), 6.0));
+                const double2 B = zsub(zadd(S[0], S[3]), zsc(S[5], 2.0));
+                const double2 Cc = zadd(zmul(k0, S[2]), zmul(k1, S[4]));
+                o.v[0] = mk(R(A.x), R(A.y));
+                o.v[1] = mk(R(B.x), R(B.y));
+                o.v[2] = mk(R(Cc.x), R(Cc.y));
+                return o;
+            },
+            [&](int idx, ABC o) {
+                const int t = idx % T, n = idx / T;
+#pragma unroll
+                for (int c = 0; c < 3; c++) buf[n * LD + c * T + t] = o.v[c];
+            });
+    } else {
+        staged_fill<N * CIN * T, NT, 8, C>(
+            [&](int idx) {
+                const int t = idx % T, r = idx / T, c = r % CIN, n = r / CIN, kx = kx0 + t;
+                return (kx < P) ? a.data[c * a.stride + kx + (int64_t)P * (ky + (int64_t)N * n)] : mk(R(0), R(0));
+            },
+            [&](int idx, C v) {
+                const int t = idx % T, r = idx / T, c = r % CIN, n = r / CIN;
+                buf[n * LD + c * T + t] = v;
+            });
+    }
     __syncthreads();
     // one component at a time keeps the butterfly registers per thread small
 #pragma unroll 1
-    for (int c = 0; c < CIN; c++) fft_lines<N, -1, T, NT>(buf + c * T, LD, tw);
+    for (int c = 0; c < CBUF; c++) fft_lines<N, -1, T, NT>(buf + c * T, LD, tw);
 
-    for (int idx = threadIdx.x; idx < N * T; idx += NT) {
-        int t = idx % T, n = idx / T, kx = kx0 + t;
-        if (kx >= P) continue;
-        double2 v[6];
+    if constexpr (CONTRACT) {
+        for (int idx = threadIdx.x; idx < N * T; idx += NT) {
+            const int t = idx % T, n = idx / T, kx = kx0 + t;
+            if (kx >= P) continue;
+            const double g0 = __ldg(a.k2 + kx), g1 = __ldg(a.k2 + ky), g2 = __ldg(a.k2 + n);
+            const double2 k2c = __ldg(a.ks + n);
+            const double k2 = g0 + g1 + g2;
+            double2 chi = make_double2(0.0, 0.0);
+            if (k2 > 0.0) {
+                const double2 A = z2d(buf[n * LD + t]), B = z2d(buf[n * LD + T + t]), Cc = z2d(buf[n * LD + 2 * T + t]);
+                chi = zsub(zadd(A, zsc(B, g2)), zsc(zmul(k2c, Cc), 6.0));
+                chi = zsc(chi, 1.0 / (2.0 * k2 * k2 * N));
+            }
+            buf[n * LD + t] = mk(R(chi.x), R(chi.y));
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < N * T; idx += NT) {
+            int t = idx % T, n = idx / T, kx = kx0 + t;
+            if (kx >= P) continue;
+            double2 v[6];
 #pragma unroll
-        for (int c = 0; c < CIN; c++) v[c] = z2d(buf[n * LD + c * T + t]);
-        int64_t kidx = kx + (int64_t)P * (ky + (int64_t)N * n);
-        fz_apply<R, OP, EXTRA>(a, N, kx, ky, n, kidx, v);
+            for (int c = 0; c < CIN; c++) v[c] = z2d(buf[n * LD + c * T + t]);
+            int64_t kidx = kx + (int64_t)P * (ky + (int64_t)N * n);
+            fz_apply<R, OP, EXTRA>(a, N, kx, ky, n, kidx, v);
 #pragma unroll
-        for (int c = 0; c < COUT; c++) buf[n * LD + c * T + t] = mk(R(v[c].x), R(v[c].y));
+            for (int c = 0; c < COUT; c++) buf[n * LD + c * T + t] = mk(R(v[c].x), R(v[c].y));
+        }
     }
     if constexpr (COUT > 0) {
         __syncthreads();

@@ -9,12 +9,36 @@
 
 namespace gev {
 
+// Tile shapes of the pencil passes (FP32 values; FP64 uses half the columns).
+#ifndef GEV_TX_F
+#define GEV_TX_F 16
+#endif
+#ifndef GEV_TY_F
+#define GEV_TY_F 16
+#endif
+#ifndef GEV_TZ1_F
+#define GEV_TZ1_F 8
+#endif
+#ifndef GEV_TZ3_F
+#define GEV_TZ3_F 4
+#endif
+#ifndef GEV_TZ6_F
+#define GEV_TZ6_F 4
+#endif
+#ifndef GEV_NT_Y
+#define GEV_NT_Y 512
+#endif
+#ifndef GEV_NT_Z
+#define GEV_NT_Z 256
+#endif
 template <class R> struct PassCfg {
-    static constexpr int TX = sizeof(R) == 4 ? 16 : 8;   // rows per x-pass CTA
-    static constexpr int TY = sizeof(R) == 4 ? 8 : 4;    // columns per y-pass CTA
-    static constexpr int TZ1 = sizeof(R) == 4 ? 8 : 4;   // Poisson
-    static constexpr int TZ3 = sizeof(R) == 4 ? 4 : 2;   // vector
-    static constexpr int TZ6 = sizeof(R) == 4 ? 4 : 2;   // scalar / tensor
+    static constexpr int TX = sizeof(R) == 4 ? GEV_TX_F : GEV_TX_F / 2;     // rows per x-pass CTA
+    static constexpr int TY = sizeof(R) == 4 ? GEV_TY_F : GEV_TY_F / 2;     // columns per y-pass CTA
+    static constexpr int TZ1 = sizeof(R) == 4 ? GEV_TZ1_F : GEV_TZ1_F / 2;  // Poisson
+    static constexpr int TZ3 = sizeof(R) == 4 ? GEV_TZ3_F : GEV_TZ3_F / 2;  // vector
+    static constexpr int TZ6 = sizeof(R) == 4 ? GEV_TZ6_F : GEV_TZ6_F / 2;  // scalar / tensor
+    static constexpr int NTY = GEV_NT_Y;                                    // threads per y-pass CTA
+    static constexpr int NTZ = GEV_NT_Z;                                    // threads per z-pass CTA
 };
 
 template <class K> inline void set_smem(K kernel, size_t bytes)
@@ -46,6 +70,17 @@ void fx_fwd_n(const FxArgs<R> &a, int ncomp, int64_t in_stride, int64_t out_stri
     k<<<dim3(N / T, N, ncomp), NT, smem, st>>>(a, in_stride, out_stride, tb.tw_half, tb.tw_full);
 }
 
+template <class R, int N>
+void fx_tij6_n(const FxArgs<R> &a, int64_t in_stride, int64_t out_stride, const FftTables<R> &tb, cudaStream_t st)
+{
+    using C = typename CT<R>::C;
+    constexpr int T = PassCfg<R>::TX / 2, NT = 256;
+    size_t smem = (size_t)6 * (N / 2) * (T + 1) * sizeof(C);
+    auto k = k_fx_fwd_tij6<R, N, T, NT>;
+    set_smem(k, smem);
+    k<<<dim3(N / T, N), NT, smem, st>>>(a.in, in_stride, a.phi, a.c, a.out, out_stride, tb.tw_half, tb.tw_full);
+}
+
 template <class R>
 void fx_forward(int N, int mode, const R *in, int64_t in_stride, int ncomp, int comp0, const R *phi, const R *chi,
                 double bg, double c, double c2, double c3, typename CT<R>::C *out, int64_t out_stride,
@@ -57,6 +92,7 @@ void fx_forward(int N, int mode, const R *in, int64_t in_stride, int ncomp, int 
     a.comp0 = comp0; a.out = out; a.partial = partial;
     if (mode == FX_COPY) { GEV_SWITCH_N(N, (fx_fwd_n<R, NN, FX_COPY>(a, ncomp, in_stride, out_stride, tb, st))) }
     else if (mode == FX_PREP_T00) { GEV_SWITCH_N(N, (fx_fwd_n<R, NN, FX_PREP_T00>(a, ncomp, in_stride, out_stride, tb, st))) }
+    else if (ncomp == 6 && comp0 == 0) { GEV_SWITCH_N(N, (fx_tij6_n<R, NN>(a, in_stride, out_stride, tb, st))) }
     else { GEV_SWITCH_N(N, (fx_fwd_n<R, NN, FX_PREP_TIJ>(a, ncomp, in_stride, out_stride, tb, st))) }
 }
 
@@ -64,7 +100,7 @@ template <class R, int N, int S>
 void fy_n(typename CT<R>::C *data, int64_t stride, int ncomp, const FftTables<R> &tb, cudaStream_t st)
 {
     using C = typename CT<R>::C;
-    constexpr int T = PassCfg<R>::TY, NT = 256;
+    constexpr int T = PassCfg<R>::TY, NT = PassCfg<R>::NTY;
     size_t smem = (size_t)N * (T + 1) * sizeof(C);
     auto k = k_fy<R, N, T, NT, S>;
     set_smem(k, smem);
@@ -102,10 +138,12 @@ template <class R, int N, int OP, int EXTRA>
 void fz_n(const FzArgs<R> &a, const FftTables<R> &tb, cudaStream_t st)
 {
     using C = typename CT<R>::C;
-    constexpr int T = (OP == OP_POISSON || OP == OP_BIN) ? PassCfg<R>::TZ1 : (OP == OP_VECTOR ? PassCfg<R>::TZ3 : PassCfg<R>::TZ6);
-    constexpr int NT = 256;
-    constexpr int CIN = OpShape<OP, EXTRA>::CIN;
-    size_t smem = (size_t)N * (CIN * T + 1) * sizeof(C);
+    constexpr int CBUF = OpShape<OP, EXTRA>::CBUF;
+    constexpr int T = (OP == OP_POISSON || OP == OP_BIN || OpShape<OP, EXTRA>::CONTRACT)
+                          ? PassCfg<R>::TZ1
+                          : (OP == OP_VECTOR ? PassCfg<R>::TZ3 : PassCfg<R>::TZ6);
+    constexpr int NT = PassCfg<R>::NTZ;
+    size_t smem = (size_t)N * (CBUF * T + 1) * sizeof(C);
     auto k = k_fz<R, N, T, NT, OP, EXTRA>;
     set_smem(k, smem);
     k<<<dim3((N / 2 + 1 + T - 1) / T, N), NT, smem, st>>>(a, tb.tw_full);
