@@ -8,17 +8,20 @@
 //   1. turns each particle into a short record of per-particle factors (in the
 //      field precision R) and counts it into one of the 9^3 cells of the
 //      tile's reach (relative cell -1..7 per axis);
-//   2. scans the cell counts, sorts record indexes by cell (counting sort) and
-//      pre-multiplies each record by the fixed-point scales;
+//   2. scans the cell counts and sorts record indexes by cell (counting sort);
 //   3. lets every vertex thread walk the 8 cells whose stencil covers it and
-//      add the contributions into 64-bit fixed-point accumulators held in
-//      registers -- no shared-memory atomics on the accumulation path.
-// The fixed-point scale of each component comes from an upper bound of the
-// per-particle contribution and the particle count, so the sum is exact
-// integer arithmetic and the result does not depend on particle order or
-// thread scheduling (bitwise reproducible).  Each output vertex is written
-// exactly once with plain stores -- no global atomics and no halo fold
-// (projection_comm1, gevolution.hpp:1543, is not needed on one GPU).
+//      accumulate the contributions in registers -- no shared-memory atomics
+//      on the accumulation path, each output vertex written once with plain
+//      stores, no global atomics and no halo fold (projection_comm1,
+//      gevolution.hpp:1543, is not needed on one GPU).
+// The result does not depend on the order of the particles in memory
+// (bitwise reproducible, for unique particle IDs):
+//   - when the tile's reach fits one chunk (the common case) the records of
+//     each cell are ordered by particle ID and each vertex sums in R in the
+//     fixed order (source cell, ID);
+//   - denser tiles take several chunks and accumulate 64-bit fixed point with
+//     a per-CTA, per-component scale from an upper bound of the contributions
+//     and the particle count, so the sum is exact integer arithmetic.
 //
 // Arithmetic follows the reference functors term by term:
 //   particle_T00_project  gevolution.hpp:1729-1854
@@ -183,6 +186,35 @@ __device__ __forceinline__ void gather_one(const R *r, int bx, int by, int bz, R
     }
 }
 
+// add the contributions of one (unscaled) record in the field precision
+template <class R, int KIND, bool USE_PHI>
+__device__ __forceinline__ void gather_sum(const R *r, int bx, int by, int bz, R phv, R phx, R phy, R phz,
+                                           R (&acc)[DepShape<KIND>::NC])
+{
+    using S = DepShape<KIND>;
+    const R wx = bx ? r[0] : (R)1 - r[0];
+    const R wy = by ? r[1] : (R)1 - r[1];
+    const R wz = bz ? r[2] : (R)1 - r[2];
+    const R w = wx * wy * wz;
+    if constexpr (S::HAS00) {
+        acc[0] += USE_PHI ? w * (r[S::F00] + (r[S::F00 + 1] + r[S::F00 + 2] * phv) * phv) : w * r[S::F00];
+    }
+    if constexpr (S::HASIJ) {
+        constexpr int C = S::CIJ;
+        acc[C + 0] += w * r[S::FIJ + 0];
+        acc[C + 3] += w * r[S::FIJ + 1];
+        acc[C + 5] += w * r[S::FIJ + 2];
+        if (!bx && !by) acc[C + 1] += wz * r[S::FIJ + 3];
+        if (!bx && !bz) acc[C + 2] += wy * r[S::FIJ + 4];
+        if (!by && !bz) acc[C + 4] += wx * r[S::FIJ + 5];
+    }
+    if constexpr (S::HAS0I) {
+        if (!bx) acc[0] += wy * wz * r[S::F0I + 0] * ((R)1 + phv + phx);
+        if (!by) acc[1] += wx * wz * r[S::F0I + 1] * ((R)1 + phv + phy);
+        if (!bz) acc[2] += wx * wy * r[S::F0I + 2] * ((R)1 + phv + phz);
+    }
+}
+
 template <class R, int NFP> __device__ __forceinline__ void load_record(const R *src, R (&dst)[NFP])
 {
     if constexpr (sizeof(R) == 4) {
@@ -230,6 +262,7 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
     __shared__ R scl_s[NC];
     __shared__ double iscl_s[NC];
     __shared__ int wsum[DEP_NT / 32];
+    __shared__ int64_t rid[CH];   // particle IDs of the records (single-chunk path)
 
     const int t = threadIdx.x;
     const int tile = blockIdx.x;
@@ -270,6 +303,111 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
         return;
     }
     const bool multi = total > (uint32_t)CH;
+
+    // exclusive scan of the 729 cell counts into cstart (two cells per thread)
+    auto scan_cells = [&]() {
+        const int c0 = 2 * t, c1 = 2 * t + 1;
+        const int n0 = c0 < DEP_NCELL ? ccount[c0] : 0;
+        const int n1 = c1 < DEP_NCELL ? ccount[c1] : 0;
+        int s = n0 + n1, incl = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int u = __shfl_up_sync(0xffffffffu, incl, o);
+            if ((t & 31) >= o) incl += u;
+        }
+        if ((t & 31) == 31) wsum[t >> 5] = incl;
+        __syncthreads();
+        if (t < 32) {
+            int w = t < DEP_NT / 32 ? wsum[t] : 0, wi = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int u = __shfl_up_sync(0xffffffffu, wi, o);
+                if (t >= o) wi += u;
+            }
+            if (t < DEP_NT / 32) wsum[t] = wi - w;   // exclusive warp offsets
+        }
+        __syncthreads();
+        const int excl = incl - s + wsum[t >> 5];
+        if (c0 < DEP_NCELL) cstart[c0] = excl;
+        if (c1 < DEP_NCELL) cstart[c1] = excl + n0;
+    };
+
+    // this thread's vertex and the phi values its contributions need
+    const int vx = t & 7, vy = (t >> 3) & 7, vz = t >> 6;
+    R phv = 0, phx = 0, phy = 0, phz = 0;
+    if (USE_PHI) {
+        phv = phis[phi_slot(vx, vy, vz)];
+        phx = phis[phi_slot(vx + 1, vy, vz)];
+        phy = phis[phi_slot(vx, vy + 1, vz)];
+        phz = phis[phi_slot(vx, vy, vz + 1)];
+    }
+    const int64_t gout = sidx(N, x0 + vx, y0 + vy, z0 + vz);
+
+    if (!multi) {
+        // Single chunk (the common case): records are sorted by cell and, inside
+        // each cell, by particle ID; every vertex then sums its contributions in
+        // the field precision in a fixed order (source cell, then ID), so the
+        // result is again independent of the particle order in memory.
+        const int n = (int)total;
+        for (int j = t; j < n; j += DEP_NT) {
+            const uint32_t i = seg_find(seg_lo, seg_pre, (uint32_t)j);
+            R v[NF], b[NC];
+            int lc;
+            if (make_record<R, KIND, USE_PHI>(p, i, N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
+                R *dst = rec + (size_t)j * NFP;
+#pragma unroll
+                for (int k = 0; k < NF; k++) dst[k] = v[k];
+                rid[j] = p.id[i];
+                rcell[j] = (uint16_t)lc;
+                rslot[j] = (uint16_t)atomicAdd(&ccount[lc], 1);
+            } else {
+                rcell[j] = DEP_SKIP;
+            }
+        }
+        __syncthreads();
+        scan_cells();
+        __syncthreads();
+        for (int j = t; j < n; j += DEP_NT) {
+            const uint16_t lc = rcell[j];
+            if (lc != DEP_SKIP) order[cstart[lc] + rslot[j]] = (uint16_t)j;
+        }
+        __syncthreads();
+        // insertion sort by ID inside each cell (cells hold a few particles)
+        for (int c = t; c < DEP_NCELL; c += DEP_NT) {
+            const int k0 = cstart[c], m = ccount[c];
+            for (int a1 = 1; a1 < m; a1++) {
+                const uint16_t key = order[k0 + a1];
+                const int64_t kid = rid[key];
+                int b1 = a1 - 1;
+                while (b1 >= 0 && rid[order[k0 + b1]] > kid) {
+                    order[k0 + b1 + 1] = order[k0 + b1];
+                    b1--;
+                }
+                order[k0 + b1 + 1] = key;
+            }
+        }
+        __syncthreads();
+        R acc[NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++) acc[c] = 0;
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
+            const int lc = (vx - bx + 1) + 9 * ((vy - by + 1) + 9 * (vz - bz + 1));
+            const int k0 = cstart[lc], k1 = k0 + ccount[lc];
+            for (int k = k0; k < k1; k++) {
+                R r[NFP];
+                load_record<R, NFP>(rec + (size_t)order[k] * NFP, r);
+                gather_sum<R, KIND, USE_PHI>(r, bx, by, bz, phv, phx, phy, phz, acc);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+            R *o = out.p[c];
+            o[gout] = accumulate ? (R)(o[gout] + acc[c]) : acc[c];
+        }
+        return;
+    }
 
     auto reduce_bounds = [&](R (&lb)[NC]) {
 #pragma unroll
@@ -313,15 +451,6 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
         set_scales();
     }
 
-    // this thread's vertex and the phi values its contributions need
-    const int vx = t & 7, vy = (t >> 3) & 7, vz = t >> 6;
-    R phv = 0, phx = 0, phy = 0, phz = 0;
-    if (USE_PHI) {
-        phv = phis[phi_slot(vx, vy, vz)];
-        phx = phis[phi_slot(vx + 1, vy, vz)];
-        phy = phis[phi_slot(vx, vy + 1, vz)];
-        phz = phis[phi_slot(vx, vy, vz + 1)];
-    }
     long long acc[NC];
 #pragma unroll
     for (int c = 0; c < NC; c++) acc[c] = 0;
@@ -330,9 +459,6 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
         const int n = (int)min((uint32_t)CH, total - base);
         // 1. records and cell counts
         {
-            R lb[NC];
-#pragma unroll
-            for (int c = 0; c < NC; c++) lb[c] = 0;
             for (int j = t; j < n; j += DEP_NT) {
                 const uint32_t i = seg_find(seg_lo, seg_pre, base + (uint32_t)j);
                 R v[NF], b[NC];
@@ -341,45 +467,16 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
                     R *dst = rec + (size_t)j * NFP;
 #pragma unroll
                     for (int k = 0; k < NF; k++) dst[k] = v[k];
-#pragma unroll
-                    for (int c = 0; c < NC; c++) lb[c] = fmax(lb[c], b[c]);
                     rcell[j] = (uint16_t)lc;
                     rslot[j] = (uint16_t)atomicAdd(&ccount[lc], 1);
                 } else {
                     rcell[j] = DEP_SKIP;
                 }
             }
-            if (!multi) reduce_bounds(lb);
         }
         __syncthreads();
-        if (!multi) set_scales();
-        // 2. exclusive scan of the 729 cell counts (two cells per thread)
-        {
-            const int c0 = 2 * t, c1 = 2 * t + 1;
-            const int n0 = c0 < DEP_NCELL ? ccount[c0] : 0;
-            const int n1 = c1 < DEP_NCELL ? ccount[c1] : 0;
-            int s = n0 + n1, incl = s;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                int u = __shfl_up_sync(0xffffffffu, incl, o);
-                if ((t & 31) >= o) incl += u;
-            }
-            if ((t & 31) == 31) wsum[t >> 5] = incl;
-            __syncthreads();
-            if (t < 32) {
-                int w = t < DEP_NT / 32 ? wsum[t] : 0, wi = w;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    int u = __shfl_up_sync(0xffffffffu, wi, o);
-                    if (t >= o) wi += u;
-                }
-                if (t < DEP_NT / 32) wsum[t] = wi - w;   // exclusive warp offsets
-            }
-            __syncthreads();
-            const int excl = incl - s + wsum[t >> 5];
-            if (c0 < DEP_NCELL) cstart[c0] = excl;
-            if (c1 < DEP_NCELL) cstart[c1] = excl + n0;
-        }
+        // 2. exclusive scan of the 729 cell counts
+        scan_cells();
         __syncthreads();
         // 3. counting sort of record indexes by cell; records take their fixed-point scales
         for (int j = t; j < n; j += DEP_NT) {

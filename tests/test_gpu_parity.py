@@ -87,10 +87,13 @@ def test_project_cic_mass_and_accumulate(prec):
 
 
 @pytest.mark.parametrize("prec", PRECS)
-def test_deposit_is_order_independent_and_bitwise_reproducible(prec):
-    """The fixed-point tile reduction gives identical bits for any particle order."""
+@pytest.mark.parametrize("n", [30000, 60000])
+def test_deposit_is_order_independent_and_bitwise_reproducible(prec, n):
+    """Identical bits for any particle order: tiles whose reach holds up to one
+    chunk of records (n = 30000) sum in a fixed (cell, particle ID) order,
+    denser tiles (n = 60000) in 64-bit fixed point."""
     N = 32
-    pos, q, ids = particles(N, n=60000, seed=6)
+    pos, q, ids = particles(N, n=n, seed=6)
     phi = trough_phi(N)
     perm = np.random.default_rng(0).permutation(len(pos))
     outs = []
@@ -103,6 +106,37 @@ def test_deposit_is_order_independent_and_bitwise_reproducible(prec):
     for other in outs[1:]:
         for x, y in zip(outs[0], other):
             assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_deposit_clustered_particles(prec):
+    """A dense clump (thousands of particles in a few tiles, several chunks per
+    tile) next to a sparse background, against the oracle."""
+    N = 32
+    rng = np.random.default_rng(12)
+    blob = 0.5 + 0.02 * rng.standard_normal((30000, 3))
+    pos = np.concatenate([blob, rng.random((20000, 3))])
+    pos -= np.floor(pos)
+    q = rng.uniform(-0.02, 0.02, pos.shape)
+    ids = np.arange(len(pos), dtype=np.int64)
+    phi = trough_phi(N)
+    o = oracle()
+    a = 0.45
+    T00 = np.zeros(N ** 3); Tij = np.zeros(6 * N ** 3); T0i = np.zeros(3 * N ** 3)
+    o.project_T00(N, len(pos), ptr(pos), ptr(q), MASS, ptr(phi), a, 1.0, ptr(T00))
+    o.project_Tij(N, len(pos), ptr(pos), ptr(q), MASS, ptr(phi), a, 1.0, ptr(Tij))
+    o.project_T0i(N, len(pos), ptr(pos), ptr(q), MASS, ptr(phi), 1.0, ptr(T0i))
+    with make_ctx(N, prec, len(pos)) as c:
+        c.set_particles(pos, q, ids, MASS)
+        c.set_field(gev.FIELD_PHI, phi)
+        c.project(gev.PROJ_T00 | gev.PROJ_TIJ | gev.PROJ_T0I, a, 1.0, True)
+        assert rel_err(c.get_field(gev.FIELD_SOURCE), T00) < TOL[prec]
+        g = c.get_field(gev.FIELD_SIJ)
+        for k in range(6):
+            assert rel_err(g[k], Tij[k * N ** 3:(k + 1) * N ** 3]) < TOL[prec], k
+        g = c.get_field(gev.FIELD_BI)
+        for k in range(3):
+            assert rel_err(g[k], T0i[k * N ** 3:(k + 1) * N ** 3]) < TOL[prec], k
 
 
 @pytest.mark.parametrize("prec", PRECS)
