@@ -715,7 +715,7 @@ template <class R> struct Ctx final : CtxBase {
         la.capacity = lcap;
         if ((int64_t)lc_id.n < lcap) { lc_pos.alloc(3 * lcap, "lightcone"); lc_vel.alloc(3 * lcap, "lightcone"); lc_id.alloc(lcap, "lightcone"); }
         ck(cudaMemsetAsync(u64.p + 1, 0, sizeof(unsigned long long), st), "memset");
-        launch_lightcone<R>(cur(), N, phi.p, la, lc_pos.p, lc_vel.p, lc_id.p, u64.p + 1, newer, idset_cap, derr.p, st);
+        launch_lightcone<R>(cur(), bstart.p, N, phi.p, la, lc_pos.p, lc_vel.p, lc_id.p, u64.p + 1, newer, idset_cap, derr.p, st);
         launched("lightcone");
         // the IDs logged near the inner edge become the next cycle's backlog
         idset_cur[s] = 1 - idset_cur[s];

@@ -95,7 +95,7 @@ struct LcKernelArgs {
 constexpr unsigned long long LC_EMPTY = ~0ull;   // free slot of an ID set (tables are filled with 0xff bytes)
 constexpr int64_t LC_MAX_PROBES = 4096;          // bound on linear probing (load factor stays below 1/4)
 template <class R>
-void launch_lightcone(const PView<R> &p, int N, const R *phi, const LcKernelArgs &la, float *pos, float *vel,
+void launch_lightcone(const PView<R> &p, const uint32_t *bstart, int N, const R *phi, const LcKernelArgs &la, float *pos, float *vel,
                       int64_t *ids, unsigned long long *count, unsigned long long *newlog, int64_t newlog_cap, int *err,
                       cudaStream_t st);
 

@@ -1,9 +1,10 @@
 // lightcone.cu -- particle lightcone crossing for one shell and one cycle.
 //
-// One thread per particle, one pass: the shell and cone test of
-// count_tracer_particles / buffer_tracer_particles
-// (Particles_gevolution.hpp:1271-1345, :1381-1466) against the periodic images
-// of the vertex, the ID-backlog de-duplication of the check zone
+// One CTA per tile of particles: the tile first culls the periodic images of
+// the vertex whose shell cannot reach it, then every particle takes the shell
+// and cone test of count_tracer_particles / buffer_tracer_particles
+// (Particles_gevolution.hpp:1271-1345, :1381-1466) against the kept images,
+// the ID-backlog de-duplication of the check zone
 // (count_lightcone_duplicate_ids / mark_lightcone_kept_particles, :1468-1510),
 // the interpolation to the crossing time (bufferTracerParticle with
 // EXACT_OUTPUT_REDSHIFTS, :500-560) and the logging of IDs near the inner edge
@@ -66,42 +67,20 @@ __device__ __forceinline__ double gphi(const R *phi, int N, int x, int y, int z)
     return (double)phi[sidx(N, wrapi(x, N), wrapi(y, N), wrapi(z, N))];
 }
 
+// the reference's exact test and output for one particle, starting at kept image kv
 template <class R>
-__global__ void k_lightcone(PView<R> p, int N, const R *__restrict__ phi, LcKernelArgs la, float *opos, float *ovel,
-                            int64_t *oid, unsigned long long *count, unsigned long long *newlog, int64_t newlog_cap,
-                            int *err, FastDiv fN)
+__device__ __forceinline__ void lc_particle(const PView<R> &p, int64_t i, int N, const int c[3], const double fr[3],
+                                            const R *__restrict__ phi, const LcKernelArgs &la, const int *vlist,
+                                            int kv, int nkeep, float *opos, float *ovel, int64_t *oid,
+                                            unsigned long long *count, unsigned long long *newlog,
+                                            int64_t newlog_cap, int *err)
 {
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= p.n) return;
-    if (la.tracer_factor > 1 && p.id[i] % la.tracer_factor != 0) return;
-    const uint32_t cell = p.cell[i];
-    if ((int64_t)cell >= (int64_t)N * N * N) { atomicOr(err, ERR_BAD_CELL); return; }
-    int c[3];
-    decode_cell(cell, fN, c[0], c[1], c[2]);
-    const double fr[3] = {p.off[i], p.off[p.cap + i], p.off[2 * p.cap + i]};
-
-    // FP32 pre-test of the shell radius with a margin far above the FP32
-    // rounding of |x - V|^2 (|x - V| < 4 box lengths): only particles that may
-    // lie in the shell take the exact FP64 test below
-    const float invN = 1.0f / (float)N;
-    const float xf[3] = {((float)c[0] + (float)fr[0]) * invN, ((float)c[1] + (float)fr[1]) * invN,
-                         ((float)c[2] + (float)fr[2]) * invN};
-    const float in2 = (float)(la.inner * la.inner) * (1.0f - 1e-4f) - 1e-5f;
-    const float out2 = (float)(la.outer * la.outer) * (1.0f + 1e-4f) + 1e-5f;
-    int v = 0;
-    for (; v < la.nvtx; v++) {
-        const float r0 = xf[0] - (float)la.vtx[v][0], r1 = xf[1] - (float)la.vtx[v][1], r2 = xf[2] - (float)la.vtx[v][2];
-        const float d2 = r0 * r0 + r1 * r1 + r2 * r2;
-        if (d2 >= in2 && d2 < out2) break;
-    }
-    if (v == la.nvtx) return;
-
     const int64_t id = p.id[i];
     const double x[3] = {(c[0] + fr[0]) / N, (c[1] + fr[1]) / N, (c[2] + fr[2]) / N};
     const double q[3] = {(double)p.q[i], (double)p.q[p.cap + i], (double)p.q[2 * p.cap + i]};
 
-    for (; v < la.nvtx; v++) {
-        const double *V = la.vtx[v];
+    for (; kv < nkeep; kv++) {
+        const double *V = la.vtx[vlist[kv]];
         double r[3] = {x[0] - V[0], x[1] - V[1], x[2] - V[2]};
         double d = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
         if (!(d >= la.inner && d < la.outer)) continue;
@@ -152,19 +131,100 @@ __global__ void k_lightcone(PView<R> p, int N, const R *__restrict__ phi, LcKern
     }
 }
 
+constexpr int LC_NT = 256;
+
+// One CTA per tile of 8^3 cells (particles are in bucket order).  The CTA
+// first keeps the vertex images whose shell [inner, outer) can reach the
+// tile's bounding box -- in vertex order, so the first image a particle
+// matches is the same as in a test against all images -- and exits when none
+// does.  Each particle then takes an FP32 pre-test of its radius against the
+// kept images (margin far above the FP32 rounding of |x - V|^2, |x - V| < 4
+// box lengths) and the exact FP64 test of the reference only near the shell.
 template <class R>
-void launch_lightcone(const PView<R> &p, int N, const R *phi, const LcKernelArgs &la, float *pos, float *vel,
+__global__ void __launch_bounds__(LC_NT) k_lightcone(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt,
+                                                     const R *__restrict__ phi, const __grid_constant__ LcKernelArgs la,
+                                                     float *opos,
+                                                     float *ovel, int64_t *oid, unsigned long long *count,
+                                                     unsigned long long *newlog, int64_t newlog_cap, int *err,
+                                                     FastDiv fN)
+{
+    __shared__ int vlist[64];
+    __shared__ unsigned int vmask[2];
+    const int tile = blockIdx.x;
+    const int tx = tile % nt, ty = (tile / nt) % nt, tz = tile / (nt * nt);
+    if (threadIdx.x < 64) {
+        bool hit = false;
+        const int v = threadIdx.x;
+        if (v < la.nvtx) {
+            const double lo[3] = {tx * 8.0 / N, ty * 8.0 / N, tz * 8.0 / N};
+            double dmin2 = 0.0, dmax2 = 0.0;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const double V = la.vtx[v][k], h = lo[k] + 8.0 / N;
+                const double c = V < lo[k] ? lo[k] : (V > h ? h : V);
+                dmin2 += (c - V) * (c - V);
+                const double f = fmax(fabs(V - lo[k]), fabs(V - h));
+                dmax2 += f * f;
+            }
+            hit = sqrt(dmax2) + 1e-9 >= la.inner && sqrt(dmin2) - 1e-9 < la.outer;
+        }
+        const unsigned int m = __ballot_sync(0xffffffffu, hit);
+        if ((threadIdx.x & 31) == 0) vmask[threadIdx.x >> 5] = m;
+    }
+    __syncthreads();
+    const unsigned int m0 = vmask[0], m1 = vmask[1];
+    const int nkeep = __popc(m0) + __popc(m1);
+    if (nkeep == 0) return;
+    if (threadIdx.x < 64) {
+        const int v = threadIdx.x;
+        const unsigned int mine = v < 32 ? m0 : m1;
+        if ((mine >> (v & 31)) & 1u) {
+            const unsigned int below = (v & 31) ? (mine & ((1u << (v & 31)) - 1u)) : 0u;
+            vlist[(v < 32 ? 0 : __popc(m0)) + __popc(below)] = v;
+        }
+    }
+    __syncthreads();
+
+    const float invN = 1.0f / (float)N;
+    const float in2 = (float)(la.inner * la.inner) * (1.0f - 1e-4f) - 1e-5f;
+    const float out2 = (float)(la.outer * la.outer) * (1.0f + 1e-4f) + 1e-5f;
+    const uint32_t plo = bstart[8 * tile], phi_ = bstart[8 * tile + 8];
+    for (uint32_t ii = plo + threadIdx.x; ii < phi_; ii += LC_NT) {
+        const int64_t i = ii;
+        if (la.tracer_factor > 1 && p.id[i] % la.tracer_factor != 0) continue;
+        const uint32_t cell = p.cell[i];
+        if ((int64_t)cell >= (int64_t)N * N * N) { atomicOr(err, ERR_BAD_CELL); continue; }
+        int c[3];
+        decode_cell(cell, fN, c[0], c[1], c[2]);
+        const double fr[3] = {p.off[i], p.off[p.cap + i], p.off[2 * p.cap + i]};
+        const float xf[3] = {((float)c[0] + (float)fr[0]) * invN, ((float)c[1] + (float)fr[1]) * invN,
+                             ((float)c[2] + (float)fr[2]) * invN};
+        int kv = 0;
+        for (; kv < nkeep; kv++) {
+            const int v = vlist[kv];
+            const float r0 = xf[0] - (float)la.vtx[v][0], r1 = xf[1] - (float)la.vtx[v][1], r2 = xf[2] - (float)la.vtx[v][2];
+            const float d2 = r0 * r0 + r1 * r1 + r2 * r2;
+            if (d2 >= in2 && d2 < out2) break;
+        }
+        if (kv == nkeep) continue;
+        lc_particle(p, i, N, c, fr, phi, la, vlist, kv, nkeep, opos, ovel, oid, count, newlog, newlog_cap, err);
+    }
+}
+
+
+template <class R>
+void launch_lightcone(const PView<R> &p, const uint32_t *bstart, int N, const R *phi, const LcKernelArgs &la, float *pos, float *vel,
                       int64_t *ids, unsigned long long *count, unsigned long long *newlog, int64_t newlog_cap, int *err,
                       cudaStream_t st)
 {
     if (p.n > 0)
-        k_lightcone<R><<<cdiv(p.n, 256), 256, 0, st>>>(p, N, phi, la, pos, vel, ids, count, newlog, newlog_cap, err,
-                                                        FastDiv((uint32_t)N));
+        k_lightcone<R><<<(unsigned)((N / 8) * (N / 8) * (N / 8)), LC_NT, 0, st>>>(
+            p, bstart, N, N / 8, phi, la, pos, vel, ids, count, newlog, newlog_cap, err, FastDiv((uint32_t)N));
 }
 
-template void launch_lightcone<float>(const PView<float> &, int, const float *, const LcKernelArgs &, float *, float *,
+template void launch_lightcone<float>(const PView<float> &, const uint32_t *, int, const float *, const LcKernelArgs &, float *, float *,
                                       int64_t *, unsigned long long *, unsigned long long *, int64_t, int *, cudaStream_t);
-template void launch_lightcone<double>(const PView<double> &, int, const double *, const LcKernelArgs &, float *,
+template void launch_lightcone<double>(const PView<double> &, const uint32_t *, int, const double *, const LcKernelArgs &, float *,
                                        float *, int64_t *, unsigned long long *, unsigned long long *, int64_t, int *,
                                        cudaStream_t);
 
