@@ -69,18 +69,18 @@ __device__ __forceinline__ int phi_slot(int vx, int vy, int vz) { return (vx + 1
 // divisions by e = sqrt(q^2 + a^2) are taken as one reciprocal, and
 // f2 / (1 + f2/a^2) as f2 a^2 / e^2 (the same quantity).
 template <class R, int KIND, bool USE_PHI>
-__device__ __forceinline__ bool make_record(const PView<R> &p, uint32_t i, int N, const FastDiv &fN, int x0, int y0, int z0,
+__device__ __forceinline__ bool make_record(const RawParticle<R> &pr, int N, const FastDiv &fN, int x0, int y0, int z0,
                                             const R *phis, R a, R m00, R mij, R (&v)[DepShape<KIND>::NF], int &lc,
                                             R (&bnd)[DepShape<KIND>::NC])
 {
     using S = DepShape<KIND>;
     int cx, cy, cz;
-    decode_cell(p.cell[i], fN, cx, cy, cz);
+    decode_cell(pr.cell, fN, cx, cy, cz);
     const int rx = rel_coord(cx, x0, N), ry = rel_coord(cy, y0, N), rz = rel_coord(cz, z0, N);
     if (rx < -1 || rx > 7 || ry < -1 || ry > 7 || rz < -1 || rz > 7) return false;
     lc = (rx + 1) + 9 * ((ry + 1) + 9 * (rz + 1));
-    const R d[3] = {(R)p.off[i], (R)p.off[p.cap + i], (R)p.off[2 * p.cap + i]};
-    const R q[3] = {p.q[i], p.q[p.cap + i], p.q[2 * p.cap + i]};
+    const R d[3] = {(R)pr.off[0], (R)pr.off[1], (R)pr.off[2]};
+    const R q[3] = {pr.q[0], pr.q[1], pr.q[2]};
     v[0] = d[0]; v[1] = d[1]; v[2] = d[2];
     R pm = 0, pint = 0;
     if (USE_PHI) {
@@ -349,19 +349,36 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
         // the field precision in a fixed order (source cell, then ID), so the
         // result is again independent of the particle order in memory.
         const int n = (int)total;
-        for (int j = t; j < n; j += DEP_NT) {
-            const uint32_t i = seg_find(seg_lo, seg_pre, (uint32_t)j);
-            R v[NF], b[NC];
-            int lc;
-            if (make_record<R, KIND, USE_PHI>(p, i, N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
-                R *dst = rec + (size_t)j * NFP;
+        {
+            // at most two particles per thread (n <= CH <= 2 DEP_NT): both loads first
+            constexpr int PP = (CH + DEP_NT - 1) / DEP_NT;
+            RawParticle<R> raw[PP];
+            int64_t pid[PP];
 #pragma unroll
-                for (int k = 0; k < NF; k++) dst[k] = v[k];
-                rid[j] = p.id[i];
-                rcell[j] = (uint16_t)lc;
-                rslot[j] = (uint16_t)atomicAdd(&ccount[lc], 1);
-            } else {
-                rcell[j] = DEP_SKIP;
+            for (int u = 0; u < PP; u++) {
+                const int j = t + u * DEP_NT;
+                if (j < n) {
+                    const uint32_t i = seg_index(seg_lo, seg_pre, (uint32_t)j);
+                    raw[u] = load_particle(p, i);
+                    pid[u] = p.id[i];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < PP; u++) {
+                const int j = t + u * DEP_NT;
+                if (j >= n) continue;
+                R v[NF], b[NC];
+                int lc;
+                if (make_record<R, KIND, USE_PHI>(raw[u], N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
+                    R *dst = rec + (size_t)j * NFP;
+#pragma unroll
+                    for (int k = 0; k < NF; k++) dst[k] = v[k];
+                    rid[j] = pid[u];
+                    rcell[j] = (uint16_t)lc;
+                    rslot[j] = (uint16_t)atomicAdd(&ccount[lc], 1);
+                } else {
+                    rcell[j] = DEP_SKIP;
+                }
             }
         }
         __syncthreads();
@@ -438,10 +455,10 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
 #pragma unroll
         for (int c = 0; c < NC; c++) lb[c] = 0;
         for (uint32_t j = t; j < total; j += DEP_NT) {
-            const uint32_t i = seg_find(seg_lo, seg_pre, j);
+            const uint32_t i = seg_index(seg_lo, seg_pre, j);
             R v[NF], b[NC];
             int lc;
-            if (make_record<R, KIND, USE_PHI>(p, i, N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
+            if (make_record<R, KIND, USE_PHI>(load_particle(p, i), N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
 #pragma unroll
                 for (int c = 0; c < NC; c++) lb[c] = fmax(lb[c], b[c]);
             }
@@ -460,10 +477,10 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
         // 1. records and cell counts
         {
             for (int j = t; j < n; j += DEP_NT) {
-                const uint32_t i = seg_find(seg_lo, seg_pre, base + (uint32_t)j);
+                const uint32_t i = seg_index(seg_lo, seg_pre, base + (uint32_t)j);
                 R v[NF], b[NC];
                 int lc;
-                if (make_record<R, KIND, USE_PHI>(p, i, N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
+                if (make_record<R, KIND, USE_PHI>(load_particle(p, i), N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
                     R *dst = rec + (size_t)j * NFP;
 #pragma unroll
                     for (int k = 0; k < NF; k++) dst[k] = v[k];

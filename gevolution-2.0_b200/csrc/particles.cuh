@@ -82,6 +82,35 @@ __device__ __forceinline__ uint32_t seg_find(const uint32_t *seg_lo, const uint3
     return seg_lo[lo] + (i - seg_pre[lo]);
 }
 
+// As seg_find, with the tile's own 8 class buckets (candidates 0..7, one
+// contiguous range that holds most of the tile's reach) resolved without the
+// search.
+__device__ __forceinline__ uint32_t seg_index(const uint32_t *seg_lo, const uint32_t *seg_pre, uint32_t i)
+{
+    if (i < seg_pre[8]) return seg_lo[0] + i;
+    return seg_find(seg_lo, seg_pre, i);
+}
+
+// The per-particle words a kernel reads, loaded together so that the loads of
+// several particles can be in flight at once.
+template <class R> struct RawParticle {
+    uint32_t cell;
+    double off[3];
+    R q[3];
+};
+
+template <class R> __device__ __forceinline__ RawParticle<R> load_particle(const PView<R> &p, int64_t i)
+{
+    RawParticle<R> r;
+    r.cell = p.cell[i];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        r.off[k] = p.off[k * p.cap + i];
+        r.q[k] = p.q[k * p.cap + i];
+    }
+    return r;
+}
+
 // relative coordinate of cell coordinate c to a tile origin o, in [-1, N-2]
 __device__ __forceinline__ int rel_coord(int c, int o, int N)
 {

@@ -100,11 +100,21 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
 
     const uint32_t lo = bstart[8 * tile], hi = bstart[8 * tile + 8];
     double lmax = 0.0;
-    for (uint32_t base = lo; base < hi; base += KD_NT) {
-        uint32_t i = base + threadIdx.x;
+    for (uint32_t base = lo; base < hi; base += 2 * KD_NT) {
+        // two particles per thread and pass: both loads are issued before either is used
+        RawParticle<R> raw[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const uint32_t i = base + threadIdx.x + u * KD_NT;
+            if (i < hi) raw[u] = load_particle(p, i);
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+        const uint32_t i = base + threadIdx.x + u * KD_NT;
         if (i >= hi) continue;
+        const RawParticle<R> &pr = raw[u];
         int cx, cy, cz;
-        decode_cell(p.cell[i], fN, cx, cy, cz);
+        decode_cell(pr.cell, fN, cx, cy, cz);
         int rx = cx - x0, ry = cy - y0, rz = cz - z0;
         // a particle outside this tile means the bucket order is stale: flag it, leave it
         // unmoved (never read outside the stage) and still give it a bucket slot
@@ -113,9 +123,9 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
         if (!ok) { rx = ry = rz = 0; cx = x0; cy = y0; cz = z0; }
         // FP64 offsets for the position update; the interpolation weights and the
         // geodesic arithmetic run in the field precision R
-        const double dd[3] = {p.off[i], p.off[p.cap + i], p.off[2 * p.cap + i]};
+        const double dd[3] = {pr.off[0], pr.off[1], pr.off[2]};
         const R d[3] = {(R)dd[0], (R)dd[1], (R)dd[2]};
-        R v[3] = {p.q[i], p.q[p.cap + i], p.q[2 * p.cap + i]};
+        R v[3] = {pr.q[0], pr.q[1], pr.q[2]};
         R w8[8];
 #pragma unroll
         for (int k = 0; k < 8; k++)
@@ -249,6 +259,7 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
             uint32_t b = bucket_of_cell(N, nt, cx, cy, cz);
             bucket[i] = b;
             rank[i] = bucket_slot(b, counts);
+        }
         }
     }
 
