@@ -38,7 +38,8 @@ template <int S, class C> __device__ __forceinline__ C cmul_si(C a)
 
 // ---------------------------------------------------------------------------
 // lattice geometry.  Real fields: x + N*(y + N*z).  Fourier fields (half
-// spectrum along x): kx + P*(ky + N*kz) with P = N/2 + 1.
+// spectrum along x): kx + PP*(ky + N*kz), kx < P = N/2 + 1, with the even row
+// pitch PP = N/2 + 2.
 // Particle tiles: 8^3 cells; a particle's bucket is 8*tile + class, where the
 // class bits mark cells on the tile's upper faces (x, y, z == 7) whose
 // particles also deposit into the next tile along that axis.
@@ -48,9 +49,10 @@ constexpr int TILE = 8;
 struct Geom {
     int N;
     int P;        // N/2 + 1
+    int PP;       // N/2 + 2, row pitch of the Fourier arrays
     int nt;       // tiles per side
     int64_t n3;   // N^3
-    int64_t nk;   // P*N*N
+    int64_t nk;   // PP*N*N
     int64_t ntiles;
 };
 

@@ -61,6 +61,16 @@ template <class T> struct DBuf {
     ~DBuf() { free(); }
 };
 
+// rows of `width` values between arrays with row pitches sp and dp
+template <class A, class B>
+__global__ void k_convert_rows(const A *src, int sp, B *dst, int dp, int width, int64_t rows)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= rows * width) return;
+    const int64_t r = i / width, c = i - r * width;
+    dst[r * dp + c] = (B)src[r * sp + c];
+}
+
 template <class A, class B>
 __global__ void k_convert(const A *src, B *dst, int64_t n)
 {
@@ -222,7 +232,8 @@ template <class R> struct Ctx final : CtxBase {
         g.P = N / 2 + 1;
         g.nt = N / 8;
         g.n3 = (int64_t)N * N * N;
-        g.nk = (int64_t)g.P * N * N;
+        g.PP = N / 2 + 2;
+        g.nk = (int64_t)g.PP * N * N;
         g.ntiles = (int64_t)g.nt * g.nt * g.nt;
         ck(cudaSetDevice(c.device), "cudaSetDevice");
         ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -447,11 +458,16 @@ template <class R> struct Ctx final : CtxBase {
         void *p; int planes; bool cplx;
         field_ref(f, &p, &planes, &cplx);
         if (!host) throw ArgError("null host pointer");
-        const int64_t n = cplx ? 2 * g.nk : g.n3;
+        // host planes are dense (Fourier rows of P complex values); device
+        // Fourier rows have the pitch PP
+        const int64_t n = cplx ? 2 * (int64_t)g.P * g.N * g.N : g.n3;
+        const int64_t dn = cplx ? 2 * g.nk : g.n3;
+        const int w = cplx ? 2 * g.P : (int)g.n3, dw = cplx ? 2 * g.PP : (int)g.n3;
+        const int64_t rows = cplx ? (int64_t)g.N * g.N : 1;
         ensure_stage(n, 0);
         for (int c = 0; c < planes; c++) {
-            const R *src = (const R *)p + (int64_t)c * n;
-            k_convert<R, double><<<cdiv(n, 256), 256, 0, st>>>(src, stage.p, n);
+            const R *src = (const R *)p + (int64_t)c * dn;
+            k_convert_rows<R, double><<<cdiv(n, 256), 256, 0, st>>>(src, dw, stage.p, w, w, rows);
             launched("convert");
             ck(cudaMemcpyAsync(host + (int64_t)c * n, stage.p, n * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
             ck(cudaStreamSynchronize(st), "synchronize");
@@ -463,11 +479,14 @@ template <class R> struct Ctx final : CtxBase {
         void *p; int planes; bool cplx;
         field_ref(f, &p, &planes, &cplx);
         if (!host) throw ArgError("null host pointer");
-        const int64_t n = cplx ? 2 * g.nk : g.n3;
+        const int64_t n = cplx ? 2 * (int64_t)g.P * g.N * g.N : g.n3;
+        const int64_t dn = cplx ? 2 * g.nk : g.n3;
+        const int w = cplx ? 2 * g.P : (int)g.n3, dw = cplx ? 2 * g.PP : (int)g.n3;
+        const int64_t rows = cplx ? (int64_t)g.N * g.N : 1;
         ensure_stage(n, 0);
         for (int c = 0; c < planes; c++) {
             ck(cudaMemcpyAsync(stage.p, host + (int64_t)c * n, n * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
-            k_convert<double, R><<<cdiv(n, 256), 256, 0, st>>>(stage.p, (R *)p + (int64_t)c * n, n);
+            k_convert_rows<double, R><<<cdiv(n, 256), 256, 0, st>>>(stage.p, w, (R *)p + (int64_t)c * dn, dw, w, rows);
             launched("convert");
             ck(cudaStreamSynchronize(st), "synchronize");
         }

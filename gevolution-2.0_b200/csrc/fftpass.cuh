@@ -1,7 +1,9 @@
 // fftpass.cuh -- pencil passes of the 3-D real-to-complex transforms with the
 // reference's pointwise physics fused into their load and solve stages.
 //
-// Fourier layout: kx + P*(ky + N*kz), P = N/2 + 1 (half spectrum along x).
+// Fourier layout: kx + PP*(ky + N*kz) for kx < P = N/2 + 1 (half spectrum
+// along x); the row pitch PP = N/2 + 2 is even so that every row starts on a
+// 16-byte boundary (tensor-memory-access copies need 16-byte-aligned strides).
 //   fx_fwd : R2C along x for T rows (y0..y0+T-1, z); fused prepareFTsource
 //   fy     : complex FFT along y for T kx-columns at one z (in place)
 //   fz     : FFT along z, pointwise Fourier-space solver, inverse FFT along z,
@@ -13,6 +15,14 @@
 #include "fft.cuh"
 
 namespace gev {
+
+// occupancy the z pass and the six-component x pass are compiled for
+#ifndef GEV_FZ_MINB
+#define GEV_FZ_MINB 3   // resident CTAs of 256 threads per SM
+#endif
+#ifndef GEV_TIJ6_MINB
+#define GEV_TIJ6_MINB 3
+#endif
 
 // ---------------------------------------------------------------------------
 // fused source preparation (PHINONLINEAR): T00 in FP64, Tij in the field precision
@@ -119,7 +129,7 @@ __global__ void __launch_bounds__(NT) k_fx_fwd(FxArgs<R> a, int64_t in_stride, i
                                                const typename CT<R>::C *__restrict__ tw_full)
 {
     using C = typename CT<R>::C;
-    constexpr int M = N / 2, P = N / 2 + 1, LD = T + 1;
+    constexpr int M = N / 2, P = N / 2 + 1, PP = N / 2 + 2, LD = T + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *buf = reinterpret_cast<C *>(smem_raw);
     __shared__ double red[NT / 32];
@@ -161,7 +171,7 @@ __global__ void __launch_bounds__(NT) k_fx_fwd(FxArgs<R> a, int64_t in_stride, i
         C d = csub(zk, zm);
         C zo = mk(R(0.5) * d.y, R(-0.5) * d.x);        // (zk - conj(zm)) / (2i)
         C w = __ldg(tw_full + k);
-        out[k + (int64_t)P * (y + (int64_t)N * z)] = cadd(ze, cmul(w, zo));
+        out[k + (int64_t)PP * (y + (int64_t)N * z)] = cadd(ze, cmul(w, zo));
     }
 
     if constexpr (MODE == FX_PREP_T00) {
@@ -208,13 +218,13 @@ __device__ __forceinline__ void prep_tij6(const R *T, int64_t n3, const R *phi, 
 // x pass, forward, for the six Tij components at once: each potential value
 // is loaded once for all six sources.  grid (N/T, N)
 template <class R, int N, int T, int NT>
-__global__ void __launch_bounds__(NT) k_fx_fwd_tij6(const R *__restrict__ Tij, int64_t n3, const R *__restrict__ phi,
+__global__ void __launch_bounds__(NT, GEV_TIJ6_MINB) k_fx_fwd_tij6(const R *__restrict__ Tij, int64_t n3, const R *__restrict__ phi,
                                                     double coeff, typename CT<R>::C *out, int64_t out_stride,
                                                     const typename CT<R>::C *__restrict__ tw_half,
                                                     const typename CT<R>::C *__restrict__ tw_full)
 {
     using C = typename CT<R>::C;
-    constexpr int M = N / 2, P = N / 2 + 1, LD = T + 1, CS = M * LD;
+    constexpr int M = N / 2, P = N / 2 + 1, PP = N / 2 + 2, LD = T + 1, CS = M * LD;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *buf = reinterpret_cast<C *>(smem_raw);   // 6 component buffers of CS
     const int y0 = blockIdx.x * T, z = blockIdx.y;
@@ -249,7 +259,7 @@ __global__ void __launch_bounds__(NT) k_fx_fwd_tij6(const R *__restrict__ Tij, i
         C d = csub(zk, zm);
         C zo = mk(R(0.5) * d.y, R(-0.5) * d.x);
         C w = __ldg(tw_full + k);
-        out[c * out_stride + k + (int64_t)P * (y + (int64_t)N * z)] = cadd(ze, cmul(w, zo));
+        out[c * out_stride + k + (int64_t)PP * (y + (int64_t)N * z)] = cadd(ze, cmul(w, zo));
     }
 }
 
@@ -261,7 +271,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_fy(typename CT<R>::C *data, i
                                            const typename CT<R>::C *__restrict__ tw)
 {
     using C = typename CT<R>::C;
-    constexpr int P = N / 2 + 1, LD = T + 1;
+    constexpr int P = N / 2 + 1, PP = N / 2 + 2, LD = T + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *buf = reinterpret_cast<C *>(smem_raw);
     const int kx0 = blockIdx.x * T, z = blockIdx.y;
@@ -269,14 +279,14 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_fy(typename CT<R>::C *data, i
     staged_fill<N * T, NT, 8, C>(
         [&](int idx) {
             const int t = idx % T, n = idx / T, kx = kx0 + t;
-            return (kx < P) ? d[kx + (int64_t)P * (n + (int64_t)N * z)] : mk(R(0), R(0));
+            return (kx < P) ? d[kx + (int64_t)PP * (n + (int64_t)N * z)] : mk(R(0), R(0));
         },
         [&](int idx, C v) { buf[(idx / T) * LD + idx % T] = v; });
     __syncthreads();
     fft_lines<N, S, T, NT>(buf, LD, tw);
     for (int idx = threadIdx.x; idx < N * T; idx += NT) {
         int t = idx % T, n = idx / T, kx = kx0 + t;
-        if (kx < P) d[kx + (int64_t)P * (n + (int64_t)N * z)] = buf[n * LD + t];
+        if (kx < P) d[kx + (int64_t)PP * (n + (int64_t)N * z)] = buf[n * LD + t];
     }
 }
 
@@ -291,7 +301,7 @@ __global__ void __launch_bounds__(NT) k_fx_inv(const typename CT<R>::C *in, int6
                                                const typename CT<R>::C *__restrict__ tw_full)
 {
     using C = typename CT<R>::C;
-    constexpr int M = N / 2, P = N / 2 + 1, LD = T + 1;
+    constexpr int M = N / 2, PP = N / 2 + 2, LD = T + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *buf = reinterpret_cast<C *>(smem_raw);
     const int y0 = blockIdx.x * T, z = blockIdx.y;
@@ -300,7 +310,7 @@ __global__ void __launch_bounds__(NT) k_fx_inv(const typename CT<R>::C *in, int6
     staged_fill<M * T, NT, 4, C>(
         [&](int idx) {
             const int k = idx % M, t = idx / M, y = y0 + t;
-            const C *row = src + (int64_t)P * (y + (int64_t)N * z);
+            const C *row = src + (int64_t)PP * (y + (int64_t)N * z);
             C A = __ldg(row + k), B = __ldg(row + M - k);
             if (k == 0) { A.y = R(0); B.y = R(0); }
             B.y = -B.y;
@@ -523,10 +533,10 @@ __device__ __forceinline__ void fz_apply(const FzArgs<R> &a, int N, int kx, int 
 // (in FP64) while the pencils load and the z transform -- linear, along kz --
 // acts on three columns instead of six.
 template <class R, int N, int T, int NT, int OP, int EXTRA>
-__global__ void __launch_bounds__(NT, 512 / NT) k_fz(FzArgs<R> a, const typename CT<R>::C *__restrict__ tw)
+__global__ void __launch_bounds__(NT, GEV_FZ_MINB * 256 / NT) k_fz(FzArgs<R> a, const typename CT<R>::C *__restrict__ tw)
 {
     using C = typename CT<R>::C;
-    constexpr int P = N / 2 + 1;
+    constexpr int P = N / 2 + 1, PP = N / 2 + 2;
     constexpr int CIN = OpShape<OP, EXTRA>::CIN, COUT = OpShape<OP, EXTRA>::COUT;
     constexpr bool CONTRACT = OpShape<OP, EXTRA>::CONTRACT;
     constexpr int CBUF = OpShape<OP, EXTRA>::CBUF;
@@ -545,7 +555,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_fz(FzArgs<R> a, const typename
                     o.v[0] = o.v[1] = o.v[2] = mk(R(0), R(0));
                     return o;
                 }
-                const int64_t k = kx + (int64_t)P * (ky + (int64_t)N * n);
+                const int64_t k = kx + (int64_t)PP * (ky + (int64_t)N * n);
                 double2 S[6];
 #pragma unroll
                 for (int c = 0; c < 6; c++) S[c] = z2d(a.data[c * a.stride + k]);
@@ -569,7 +579,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_fz(FzArgs<R> a, const typename
         staged_fill<N * CIN * T, NT, 8, C>(
             [&](int idx) {
                 const int t = idx % T, r = idx / T, c = r % CIN, n = r / CIN, kx = kx0 + t;
-                return (kx < P) ? a.data[c * a.stride + kx + (int64_t)P * (ky + (int64_t)N * n)] : mk(R(0), R(0));
+                return (kx < P) ? a.data[c * a.stride + kx + (int64_t)PP * (ky + (int64_t)N * n)] : mk(R(0), R(0));
             },
             [&](int idx, C v) {
                 const int t = idx % T, r = idx / T, c = r % CIN, n = r / CIN;
@@ -603,7 +613,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_fz(FzArgs<R> a, const typename
             double2 v[6];
 #pragma unroll
             for (int c = 0; c < CIN; c++) v[c] = z2d(buf[n * LD + c * T + t]);
-            int64_t kidx = kx + (int64_t)P * (ky + (int64_t)N * n);
+            int64_t kidx = kx + (int64_t)PP * (ky + (int64_t)N * n);
             fz_apply<R, OP, EXTRA>(a, N, kx, ky, n, kidx, v);
 #pragma unroll
             for (int c = 0; c < COUT; c++) buf[n * LD + c * T + t] = mk(R(v[c].x), R(v[c].y));
@@ -615,7 +625,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_fz(FzArgs<R> a, const typename
         for (int c = 0; c < COUT; c++) fft_lines<N, 1, T, NT>(buf + c * T, LD, tw);
         for (int idx = threadIdx.x; idx < N * COUT * T; idx += NT) {
             int t = idx % T, r = idx / T, c = r % COUT, n = r / COUT, kx = kx0 + t;
-            if (kx < P) a.data[c * a.stride + kx + (int64_t)P * (ky + (int64_t)N * n)] = buf[n * LD + c * T + t];
+            if (kx < P) a.data[c * a.stride + kx + (int64_t)PP * (ky + (int64_t)N * n)] = buf[n * LD + c * T + t];
         }
     }
 }

@@ -13,7 +13,7 @@
 //
 // Limits and rules (the same text is in include/gev.h):
 //   * N in {16, 32, 64, 128}: the static scratch holds the half spectrum of a
-//     128^3 grid in FP64 (N/2+1)*N*N*16 bytes = 17,039,360 bytes, plus the FFT
+//     128^3 grid in FP64 (N/2+2)*N*N*16 bytes = 17,301,504 bytes, plus the FFT
 //     and k tables.  Larger N is rejected with GEV_ERR_SIZE.
 //   * Nothing in the scratch has to start at zero: every call first writes the
 //     tables and then the whole spectrum before any of it is read.
@@ -36,7 +36,7 @@ namespace {
 
 constexpr int NA_MAX_N = 128;
 constexpr size_t na_align(size_t b) { return (b + 255) & ~(size_t)255; }
-constexpr size_t NA_SPEC_BYTES = na_align((size_t)(NA_MAX_N / 2 + 1) * NA_MAX_N * NA_MAX_N * sizeof(double2));
+constexpr size_t NA_SPEC_BYTES = na_align((size_t)(NA_MAX_N / 2 + 2) * NA_MAX_N * NA_MAX_N * sizeof(double2));
 constexpr size_t NA_TWF_BYTES = na_align((size_t)NA_MAX_N * sizeof(double2));
 constexpr size_t NA_TWH_BYTES = na_align((size_t)(NA_MAX_N / 2) * sizeof(double2));
 constexpr size_t NA_K2_BYTES = na_align((size_t)NA_MAX_N * sizeof(double));
@@ -77,7 +77,7 @@ int na_solve(int N, const R *src, R *dst, double coeff, double modif, unsigned c
     C *twh = reinterpret_cast<C *>(base + NA_SPEC_BYTES + NA_TWF_BYTES);
     double *k2 = reinterpret_cast<double *>(base + NA_SPEC_BYTES + NA_TWF_BYTES + NA_TWH_BYTES);
     double2 *ks = reinterpret_cast<double2 *>(base + NA_SPEC_BYTES + NA_TWF_BYTES + NA_TWH_BYTES + NA_K2_BYTES);
-    const int64_t n3 = (int64_t)N * N * N, nk = (int64_t)(N / 2 + 1) * N * N;
+    const int64_t n3 = (int64_t)N * N * N, nk = (int64_t)(N / 2 + 2) * N * N;   // Fourier rows of pitch N/2+2
 
     k_na_tables<R><<<cdiv(N, 128), 128, 0, st>>>(N, twf, twh, k2, ks);
     const FftTables<R> tb{twf, twh, k2, ks};

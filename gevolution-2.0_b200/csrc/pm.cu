@@ -281,7 +281,7 @@ template <class R> struct Pm final : PmBase {
         pck(cudaSetDevice(cfg.device), "cudaSetDevice");
         pck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
         n3 = (int64_t)N * N * N;
-        nk = (int64_t)(N / 2 + 1) * N * N;
+        nk = (int64_t)(N / 2 + 2) * N * N;   // Fourier rows of pitch N/2+2
         rho.alloc(n3, "fields");
         lam.alloc(3 * n3, "fields");
         W.alloc(nk, "spectrum");

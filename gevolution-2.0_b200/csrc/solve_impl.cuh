@@ -31,6 +31,12 @@ namespace gev {
 #ifndef GEV_NT_Z
 #define GEV_NT_Z 256
 #endif
+#ifndef GEV_TZC_F
+#define GEV_TZC_F 8      // columns of the contracted scalar z pass
+#endif
+#ifndef GEV_TIJ6_T_F
+#define GEV_TIJ6_T_F 4   // rows of the six-component Tij x pass
+#endif
 template <class R> struct PassCfg {
     static constexpr int TX = sizeof(R) == 4 ? GEV_TX_F : GEV_TX_F / 2;     // rows per x-pass CTA
     static constexpr int TY = sizeof(R) == 4 ? GEV_TY_F : GEV_TY_F / 2;     // columns per y-pass CTA
@@ -39,6 +45,8 @@ template <class R> struct PassCfg {
     static constexpr int TZ6 = sizeof(R) == 4 ? GEV_TZ6_F : GEV_TZ6_F / 2;  // scalar / tensor
     static constexpr int NTY = GEV_NT_Y;                                    // threads per y-pass CTA
     static constexpr int NTZ = GEV_NT_Z;                                    // threads per z-pass CTA
+    static constexpr int TZC = sizeof(R) == 4 ? GEV_TZC_F : GEV_TZC_F / 2;  // contracted scalar
+    static constexpr int TIJ6 = sizeof(R) == 4 ? GEV_TIJ6_T_F : GEV_TIJ6_T_F / 2;
 };
 
 template <class K> inline void set_smem(K kernel, size_t bytes)
@@ -74,7 +82,7 @@ template <class R, int N>
 void fx_tij6_n(const FxArgs<R> &a, int64_t in_stride, int64_t out_stride, const FftTables<R> &tb, cudaStream_t st)
 {
     using C = typename CT<R>::C;
-    constexpr int T = PassCfg<R>::TX / 2, NT = 256;
+    constexpr int T = PassCfg<R>::TIJ6, NT = 256;
     size_t smem = (size_t)6 * (N / 2) * (T + 1) * sizeof(C);
     auto k = k_fx_fwd_tij6<R, N, T, NT>;
     set_smem(k, smem);
@@ -139,9 +147,9 @@ void fz_n(const FzArgs<R> &a, const FftTables<R> &tb, cudaStream_t st)
 {
     using C = typename CT<R>::C;
     constexpr int CBUF = OpShape<OP, EXTRA>::CBUF;
-    constexpr int T = (OP == OP_POISSON || OP == OP_BIN || OpShape<OP, EXTRA>::CONTRACT)
-                          ? PassCfg<R>::TZ1
-                          : (OP == OP_VECTOR ? PassCfg<R>::TZ3 : PassCfg<R>::TZ6);
+    constexpr int T = OpShape<OP, EXTRA>::CONTRACT ? PassCfg<R>::TZC
+                      : (OP == OP_POISSON || OP == OP_BIN) ? PassCfg<R>::TZ1
+                      : (OP == OP_VECTOR ? PassCfg<R>::TZ3 : PassCfg<R>::TZ6);
     constexpr int NT = PassCfg<R>::NTZ;
     size_t smem = (size_t)N * (CBUF * T + 1) * sizeof(C);
     auto k = k_fz<R, N, T, NT, OP, EXTRA>;

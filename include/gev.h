@@ -224,7 +224,7 @@ double gev_particle_horizon(double a, double fourpiG, const gev_cosmo *cosmo);
  * Work is queued on `stream` (a cudaStream_t; NULL = the legacy default
  * stream) and the call does not synchronise.
  *   - N must be 16, 32, 64 or 128: the spectrum scratch is a static device
- *     array sized for N = 128 in FP64 (about 17 MB); N = 256..768 returns
+ *     array sized for N = 128 in FP64 (about 17.3 MB); N = 256..768 returns
  *     GEV_ERR_SIZE, other N and null pointers GEV_ERR_ARG.
  *   - No part of the scratch has to start at zero.
  *   - All callers on one device share that scratch: calls whose work overlaps
