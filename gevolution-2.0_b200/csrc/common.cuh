@@ -113,6 +113,7 @@ enum { EXTRA_TENSOR_PROJECT = 1, EXTRA_TENSOR_EVOLVE = 2, EXTRA_VECTOR_EVOLVE = 
 constexpr int ERR_NONFINITE = 1;       // a particle coordinate became non-finite
 constexpr int ERR_LC_OVERFLOW = 2;     // lightcone output exceeded its capacity
 constexpr int ERR_BAD_CELL = 4;        // a particle cell index outside the lattice
+constexpr int ERR_TMA_TIMEOUT = 8;     // a bulk tensor copy did not complete within the wait limit
 
 // kernel launch helper
 inline unsigned int cdiv(int64_t a, int64_t b) { return (unsigned int)((a + b - 1) / b); }

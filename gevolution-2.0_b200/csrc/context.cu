@@ -341,8 +341,9 @@ template <class R> struct Ctx final : CtxBase {
         if (e) {
             ck(cudaMemsetAsync(derr.p, 0, sizeof(int), st), "memset");
             char buf[160];
-            snprintf(buf, sizeof buf, "device error word 0x%x (%s%s%s)", e, (e & ERR_NONFINITE) ? "non-finite particle coordinate " : "",
-                     (e & ERR_LC_OVERFLOW) ? "lightcone buffer overflow " : "", (e & ERR_BAD_CELL) ? "cell index out of range" : "");
+            snprintf(buf, sizeof buf, "device error word 0x%x (%s%s%s%s)", e, (e & ERR_NONFINITE) ? "non-finite particle coordinate " : "",
+                     (e & ERR_LC_OVERFLOW) ? "lightcone buffer overflow " : "", (e & ERR_BAD_CELL) ? "cell index out of range " : "",
+                     (e & ERR_TMA_TIMEOUT) ? "bulk tensor copy timed out" : "");
             throw DeviceError(buf);
         }
     }
@@ -554,6 +555,7 @@ template <class R> struct Ctx final : CtxBase {
         fy_pass<R>(N, -1, W.p, g.nk, 1, tb, st);
         launched("fy forward (phi)");
         FzParams fp{};
+        fp.err = derr.p;
         fp.op = OP_POISSON;
         fp.p0 = pc / -((double)N * (double)N * (double)N);
         fp.p1 = modif;
@@ -582,6 +584,7 @@ template <class R> struct Ctx final : CtxBase {
         fy_pass<R>(N, -1, W.p, g.nk, 6, tb, st);
         launched("fy forward (Sij)");
         FzParams fp{};
+        fp.err = derr.p;
         fp.op = OP_SCALAR;
         fp.extra = 0;
         if (cfg.tensor) fp.extra |= cycle0 ? EXTRA_TENSOR_PROJECT : EXTRA_TENSOR_EVOLVE;
@@ -610,6 +613,7 @@ template <class R> struct Ctx final : CtxBase {
         fy_pass<R>(N, -1, W.p, g.nk, 3, tb, st);
         launched("fy forward (T0i)");
         FzParams fp{};
+        fp.err = derr.p;
         fp.op = OP_VECTOR;
         fp.p0 = coeff;
         fp.p1 = modif;
@@ -658,6 +662,7 @@ template <class R> struct Ctx final : CtxBase {
         ck(cudaMemsetAsync(bins.p, 0, 4 * nb * sizeof(double), st), "memset");
         ck(cudaMemsetAsync(occ.p, 0, nb * sizeof(unsigned long long), st), "memset");
         FzParams fp{};
+        fp.err = derr.p;
         fp.op = OP_BIN;
         fp.p0 = nb;
         fp.p1 = kmax;

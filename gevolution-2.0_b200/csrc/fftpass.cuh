@@ -13,6 +13,7 @@
 
 #include "common.cuh"
 #include "fft.cuh"
+#include "tma.cuh"
 
 namespace gev {
 
@@ -353,6 +354,7 @@ template <class R> struct FzArgs {
     double *phi_hom;           // k = 0 mode after the Poisson solve
     double *bins;              // OP_BIN: 4*numbins accumulators (k, k^2, P, P^2)
     unsigned long long *occ;   // OP_BIN: mode counts
+    int *err;                  // device error word (may be null)
 };
 
 __device__ __forceinline__ double2 zmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
@@ -626,6 +628,121 @@ __global__ void __launch_bounds__(NT, GEV_FZ_MINB * 256 / NT) k_fz(FzArgs<R> a, 
         for (int idx = threadIdx.x; idx < N * COUT * T; idx += NT) {
             int t = idx % T, r = idx / T, c = r % COUT, n = r / COUT, kx = kx0 + t;
             if (kx < P) a.data[c * a.stride + kx + (int64_t)PP * (ky + (int64_t)N * n)] = buf[n * LD + c * T + t];
+        }
+    }
+}
+
+// z pass with tensor-memory-access staging: one elected thread loads the
+// CTA's T kx-columns of every input component over all kz as bulk tensor
+// copies (boxes of at most 256 kz) into dense per-component shared buffers,
+// the CTA transforms, solves and inverse-transforms them, and the results
+// leave by bulk tensor stores.  Columns kx >= P of the last CTA are zero-filled
+// on load and clipped on store.  Same arithmetic as k_fz.
+template <int N> struct ZBox {
+    static constexpr int ZB = N <= 256 ? N : (N % 256 == 0 ? 256 : 128);
+    static constexpr int NZB = N / ZB;
+};
+
+// the tensor extras keep six components in registers through the solve:
+// compiled for one resident CTA instead of GEV_FZ_MINB
+template <int OP, int EXTRA, int NT> struct FzMinBlocks {
+    static constexpr int v = (OpShape<OP, EXTRA>::CIN == 6 && !OpShape<OP, EXTRA>::CONTRACT) ? 1 : GEV_FZ_MINB * 256 / NT;
+};
+
+template <class R, int N, int T, int NT, int OP, int EXTRA>
+__global__ void __launch_bounds__(NT, (FzMinBlocks<OP, EXTRA, NT>::v))
+    k_fz_tma(FzArgs<R> a, const typename CT<R>::C *__restrict__ tw, const __grid_constant__ CUtensorMap tmap)
+{
+    using C = typename CT<R>::C;
+    constexpr int P = N / 2 + 1, PP = N / 2 + 2;
+    constexpr int CIN = OpShape<OP, EXTRA>::CIN, COUT = OpShape<OP, EXTRA>::COUT;
+    constexpr bool CONTRACT = OpShape<OP, EXTRA>::CONTRACT;
+    constexpr int CBUF = OpShape<OP, EXTRA>::CBUF;
+    constexpr int ZB = ZBox<N>::ZB, NZB = ZBox<N>::NZB;
+    constexpr int CS = N * T;   // one component: [kz][t], dense
+    // bulk tensor copies want 128-byte aligned shared addresses: the launch
+    // adds 128 bytes of slack and the buffers start at the next boundary
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *buf = reinterpret_cast<C *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
+    __shared__ __align__(8) uint64_t bar;
+    const int kx0 = blockIdx.x * T, ky = blockIdx.y;
+
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(&bar, (uint32_t)(CIN * CS * sizeof(C)));
+#pragma unroll 1
+        for (int c = 0; c < CIN; c++)
+#pragma unroll 1
+            for (int zc = 0; zc < NZB; zc++) tma_load_4d(buf + c * CS + zc * ZB * T, &tmap, 2 * kx0, ky, zc * ZB, c, &bar);
+    }
+    const bool ok = mbar_wait(&bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0 && a.err) atomicOr(a.err, ERR_TMA_TIMEOUT);
+        return;
+    }
+
+    if constexpr (CONTRACT) {
+        // A, B, C of k_fz's projectFTscalar factorisation, in place into buffers 0..2
+        for (int idx = threadIdx.x; idx < CS; idx += NT) {
+            const int t = idx % T, kx = kx0 + t;
+            double2 A = make_double2(0.0, 0.0), B = A, Cc = A;
+            if (kx < P) {
+                double2 S[6];
+#pragma unroll
+                for (int c = 0; c < 6; c++) S[c] = z2d(buf[c * CS + idx]);
+                const double g0 = __ldg(a.k2 + kx), g1 = __ldg(a.k2 + ky);
+                const double2 k0 = __ldg(a.ks + kx), k1 = __ldg(a.ks + ky);
+                A = zsub(zadd(zadd(zsc(S[0], g1 - 2.0 * g0), zsc(S[3], g0 - 2.0 * g1)), zsc(S[5], g0 + g1)),
+                         zsc(zmul(zmul(k0, k1), S[1]), 6.0));
+                B = zsub(zadd(S[0], S[3]), zsc(S[5], 2.0));
+                Cc = zadd(zmul(k0, S[2]), zmul(k1, S[4]));
+            }
+            buf[idx] = mk(R(A.x), R(A.y));
+            buf[CS + idx] = mk(R(B.x), R(B.y));
+            buf[2 * CS + idx] = mk(R(Cc.x), R(Cc.y));
+        }
+        __syncthreads();
+    }
+#pragma unroll 1
+    for (int c = 0; c < CBUF; c++) fft_lines<N, -1, T, NT>(buf + c * CS, T, tw);
+
+    for (int idx = threadIdx.x; idx < CS; idx += NT) {
+        const int t = idx % T, n = idx / T, kx = kx0 + t;
+        if (kx >= P) continue;
+        if constexpr (CONTRACT) {
+            const double g0 = __ldg(a.k2 + kx), g1 = __ldg(a.k2 + ky), g2 = __ldg(a.k2 + n);
+            const double2 k2c = __ldg(a.ks + n);
+            const double k2 = g0 + g1 + g2;
+            double2 chi = make_double2(0.0, 0.0);
+            if (k2 > 0.0) {
+                const double2 A = z2d(buf[idx]), B = z2d(buf[CS + idx]), Cc = z2d(buf[2 * CS + idx]);
+                chi = zsub(zadd(A, zsc(B, g2)), zsc(zmul(k2c, Cc), 6.0));
+                chi = zsc(chi, 1.0 / (2.0 * k2 * k2 * N));
+            }
+            buf[idx] = mk(R(chi.x), R(chi.y));
+        } else {
+            double2 v[6];
+#pragma unroll
+            for (int c = 0; c < CIN; c++) v[c] = z2d(buf[c * CS + idx]);
+            const int64_t kidx = kx + (int64_t)PP * (ky + (int64_t)N * n);
+            fz_apply<R, OP, EXTRA>(a, N, kx, ky, n, kidx, v);
+#pragma unroll
+            for (int c = 0; c < COUT; c++) buf[c * CS + idx] = mk(R(v[c].x), R(v[c].y));
+        }
+    }
+    if constexpr (COUT > 0) {
+        __syncthreads();
+#pragma unroll 1
+        for (int c = 0; c < COUT; c++) fft_lines<N, 1, T, NT>(buf + c * CS, T, tw);
+        fence_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+#pragma unroll 1
+            for (int c = 0; c < COUT; c++)
+#pragma unroll 1
+                for (int zc = 0; zc < NZB; zc++) tma_store_4d(&tmap, 2 * kx0, ky, zc * ZB, c, buf + c * CS + zc * ZB * T);
+            tma_store_drain();
         }
     }
 }

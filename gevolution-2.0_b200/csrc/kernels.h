@@ -72,6 +72,7 @@ struct FzParams {
     double *phi_hom;
     double *bins;
     unsigned long long *occ;
+    int *err;   // device error word for the transfer timeout (may be null)
 };
 template <class R>
 void fz_pass(int N, const FzParams &fp, typename CT<R>::C *data, int64_t stride, typename CT<R>::C *hij,

@@ -31,8 +31,11 @@ namespace gev {
 #ifndef GEV_NT_Z
 #define GEV_NT_Z 256
 #endif
+#ifndef GEV_FZ_TMA
+#define GEV_FZ_TMA 1     // z pass staged by bulk tensor copies
+#endif
 #ifndef GEV_TZC_F
-#define GEV_TZC_F 8      // columns of the contracted scalar z pass
+#define GEV_TZC_F 4      // columns of the contracted scalar z pass
 #endif
 #ifndef GEV_TIJ6_T_F
 #define GEV_TIJ6_T_F 4   // rows of the six-component Tij x pass
@@ -146,15 +149,25 @@ template <class R, int N, int OP, int EXTRA>
 void fz_n(const FzArgs<R> &a, const FftTables<R> &tb, cudaStream_t st)
 {
     using C = typename CT<R>::C;
-    constexpr int CBUF = OpShape<OP, EXTRA>::CBUF;
     constexpr int T = OpShape<OP, EXTRA>::CONTRACT ? PassCfg<R>::TZC
                       : (OP == OP_POISSON || OP == OP_BIN) ? PassCfg<R>::TZ1
                       : (OP == OP_VECTOR ? PassCfg<R>::TZ3 : PassCfg<R>::TZ6);
     constexpr int NT = PassCfg<R>::NTZ;
+#if GEV_FZ_TMA
+    static_assert(T % 2 == 0 || sizeof(R) == 8, "TMA boxes need 16-byte rows");
+    constexpr int CIN = OpShape<OP, EXTRA>::CIN;
+    const size_t smem = (size_t)CIN * N * T * sizeof(C) + 128;
+    const CUtensorMap map = fourier_tensor_map<R>(a.data, N, a.stride, CIN, T, ZBox<N>::ZB);
+    auto k = k_fz_tma<R, N, T, NT, OP, EXTRA>;
+    set_smem(k, smem);
+    k<<<dim3((N / 2 + 1 + T - 1) / T, N), NT, smem, st>>>(a, tb.tw_full, map);
+#else
+    constexpr int CBUF = OpShape<OP, EXTRA>::CBUF;
     size_t smem = (size_t)N * (CBUF * T + 1) * sizeof(C);
     auto k = k_fz<R, N, T, NT, OP, EXTRA>;
     set_smem(k, smem);
     k<<<dim3((N / 2 + 1 + T - 1) / T, N), NT, smem, st>>>(a, tb.tw_full);
+#endif
 }
 
 template <class R, int N>
@@ -189,6 +202,7 @@ void fz_pass(int N, const FzParams &fp, typename CT<R>::C *data, int64_t stride,
     a.phi_hom = fp.phi_hom;
     a.bins = fp.bins;
     a.occ = fp.occ;
+    a.err = fp.err;
     GEV_SWITCH_N(N, (fz_dispatch<R, NN>(fp, a, tb, st)))
 }
 
