@@ -747,4 +747,35 @@ __global__ void __launch_bounds__(NT, (FzMinBlocks<OP, EXTRA, NT>::v))
     }
 }
 
+// y pass with bulk-tensor-copy staging: T kx-columns over all ky at one kz,
+// in place.  grid (ceil(P/T), N, ncomp)
+template <class R, int N, int T, int NT, int S>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_fy_tma(const typename CT<R>::C *__restrict__ tw,
+                                                        const __grid_constant__ CUtensorMap tmap)
+{
+    using C = typename CT<R>::C;
+    constexpr int YB = ZBox<N>::ZB, NYB = ZBox<N>::NZB;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *buf = reinterpret_cast<C *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
+    __shared__ __align__(8) uint64_t bar;
+    const int kx0 = blockIdx.x * T, z = blockIdx.y, comp = blockIdx.z;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(&bar, (uint32_t)(N * T * sizeof(C)));
+#pragma unroll 1
+        for (int yc = 0; yc < NYB; yc++) tma_load_4d(buf + yc * YB * T, &tmap, 2 * kx0, yc * YB, z, comp, &bar);
+    }
+    const bool ok = mbar_wait(&bar, 0);
+    if (__syncthreads_or(!ok)) return;   // the data never arrived: leave the array untouched
+    fft_lines<N, S, T, NT>(buf, T, tw);
+    fence_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll 1
+        for (int yc = 0; yc < NYB; yc++) tma_store_4d(&tmap, 2 * kx0, yc * YB, z, comp, buf + yc * YB * T);
+        tma_store_drain();
+    }
+}
+
 }  // namespace gev

@@ -31,6 +31,9 @@ namespace gev {
 #ifndef GEV_NT_Z
 #define GEV_NT_Z 256
 #endif
+#ifndef GEV_FY_TMA
+#define GEV_FY_TMA 1     // y pass staged by bulk tensor copies
+#endif
 #ifndef GEV_FZ_TMA
 #define GEV_FZ_TMA 1     // z pass staged by bulk tensor copies
 #endif
@@ -112,10 +115,18 @@ void fy_n(typename CT<R>::C *data, int64_t stride, int ncomp, const FftTables<R>
 {
     using C = typename CT<R>::C;
     constexpr int T = PassCfg<R>::TY, NT = PassCfg<R>::NTY;
+#if GEV_FY_TMA
+    const size_t smem = (size_t)N * T * sizeof(C) + 128;
+    const CUtensorMap map = fourier_tensor_map<R>(data, N, stride, ncomp, T, ZBox<N>::ZB, 1);
+    auto k = k_fy_tma<R, N, T, NT, S>;
+    set_smem(k, smem);
+    k<<<dim3((N / 2 + 1 + T - 1) / T, N, ncomp), NT, smem, st>>>(tb.tw_full, map);
+#else
     size_t smem = (size_t)N * (T + 1) * sizeof(C);
     auto k = k_fy<R, N, T, NT, S>;
     set_smem(k, smem);
     k<<<dim3((N / 2 + 1 + T - 1) / T, N, ncomp), NT, smem, st>>>(data, stride, tb.tw_full);
+#endif
 }
 
 template <class R>
@@ -157,7 +168,7 @@ void fz_n(const FzArgs<R> &a, const FftTables<R> &tb, cudaStream_t st)
     static_assert(T % 2 == 0 || sizeof(R) == 8, "TMA boxes need 16-byte rows");
     constexpr int CIN = OpShape<OP, EXTRA>::CIN;
     const size_t smem = (size_t)CIN * N * T * sizeof(C) + 128;
-    const CUtensorMap map = fourier_tensor_map<R>(a.data, N, a.stride, CIN, T, ZBox<N>::ZB);
+    const CUtensorMap map = fourier_tensor_map<R>(a.data, N, a.stride, CIN, T, 1, ZBox<N>::ZB);
     auto k = k_fz_tma<R, N, T, NT, OP, EXTRA>;
     set_smem(k, smem);
     k<<<dim3((N / 2 + 1 + T - 1) / T, N), NT, smem, st>>>(a, tb.tw_full, map);

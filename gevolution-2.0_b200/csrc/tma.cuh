@@ -99,15 +99,15 @@ inline PFN_cuTensorMapEncodeTiled_v12000 tma_encoder()
 
 // A Fourier array (rows of P = N/2+1 complex values at the pitch N/2+2,
 // components `nk` complex values apart) as the 4-D tensor
-// {2P reals, ky, kz, component}; box {2T reals, 1, zb, 1}.
+// {2P reals, ky, kz, component}; box {2T reals, yb, zb, 1}.
 template <class R>
-CUtensorMap fourier_tensor_map(const void *base, int N, int64_t nk, int ncomp, int T, int zb)
+CUtensorMap fourier_tensor_map(const void *base, int N, int64_t nk, int ncomp, int T, int yb, int zb)
 {
     CUtensorMap m;
     const cuuint64_t row = (cuuint64_t)(N / 2 + 2) * 2 * sizeof(R);
     const cuuint64_t dims[4] = {(cuuint64_t)2 * (N / 2 + 1), (cuuint64_t)N, (cuuint64_t)N, (cuuint64_t)ncomp};
     const cuuint64_t strides[3] = {row, row * (cuuint64_t)N, (cuuint64_t)nk * 2 * sizeof(R)};
-    const cuuint32_t box[4] = {(cuuint32_t)(2 * T), 1, (cuuint32_t)zb, 1};
+    const cuuint32_t box[4] = {(cuuint32_t)(2 * T), (cuuint32_t)yb, (cuuint32_t)zb, 1};
     const cuuint32_t es[4] = {1, 1, 1, 1};
     const CUresult r = tma_encoder()(&m, sizeof(R) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
                                      4, const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
