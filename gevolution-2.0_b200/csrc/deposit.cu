@@ -349,47 +349,48 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
         // the field precision in a fixed order (source cell, then ID), so the
         // result is again independent of the particle order in memory.
         const int n = (int)total;
-        {
-            // at most two particles per thread (n <= CH <= 2 DEP_NT): both loads first
-            constexpr int PP = (CH + DEP_NT - 1) / DEP_NT;
-            RawParticle<R> raw[PP];
-            int64_t pid[PP];
+        // at most two particles per thread (n <= CH <= 2 DEP_NT); their loads are
+        // issued together and the raw words stay in registers until each
+        // record is written straight to its sorted position
+        constexpr int PP = (CH + DEP_NT - 1) / DEP_NT;
+        RawParticle<R> raw[PP];
+        int64_t pid[PP];
 #pragma unroll
-            for (int u = 0; u < PP; u++) {
-                const int j = t + u * DEP_NT;
-                if (j < n) {
-                    const uint32_t i = seg_index(seg_lo, seg_pre, (uint32_t)j);
-                    raw[u] = load_particle(p, i);
-                    pid[u] = p.id[i];
-                }
+        for (int u = 0; u < PP; u++) {
+            const int j = t + u * DEP_NT;
+            if (j < n) {
+                const uint32_t i = seg_index(seg_lo, seg_pre, (uint32_t)j);
+                raw[u] = load_particle(p, i);
+                pid[u] = p.id[i];
             }
+        }
+        // 1. cell of each record inside the tile's reach and its slot in that cell
 #pragma unroll
-            for (int u = 0; u < PP; u++) {
-                const int j = t + u * DEP_NT;
-                if (j >= n) continue;
-                R v[NF], b[NC];
-                int lc;
-                if (make_record<R, KIND, USE_PHI>(raw[u], N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
-                    R *dst = rec + (size_t)j * NFP;
-#pragma unroll
-                    for (int k = 0; k < NF; k++) dst[k] = v[k];
-                    rid[j] = pid[u];
-                    rcell[j] = (uint16_t)lc;
-                    rslot[j] = (uint16_t)atomicAdd(&ccount[lc], 1);
-                } else {
-                    rcell[j] = DEP_SKIP;
-                }
+        for (int u = 0; u < PP; u++) {
+            const int j = t + u * DEP_NT;
+            if (j >= n) continue;
+            int cx, cy, cz;
+            decode_cell(raw[u].cell, fN, cx, cy, cz);
+            const int rx = rel_coord(cx, x0, N), ry = rel_coord(cy, y0, N), rz = rel_coord(cz, z0, N);
+            if (rx < -1 || rx > 7 || ry < -1 || ry > 7 || rz < -1 || rz > 7) {
+                rcell[j] = DEP_SKIP;
+            } else {
+                const int lc = (rx + 1) + 9 * ((ry + 1) + 9 * (rz + 1));
+                rid[j] = pid[u];
+                rcell[j] = (uint16_t)lc;
+                rslot[j] = (uint16_t)atomicAdd(&ccount[lc], 1);
             }
         }
         __syncthreads();
         scan_cells();
         __syncthreads();
+        const int nvalid = cstart[DEP_NCELL - 1] + ccount[DEP_NCELL - 1];
         for (int j = t; j < n; j += DEP_NT) {
             const uint16_t lc = rcell[j];
             if (lc != DEP_SKIP) order[cstart[lc] + rslot[j]] = (uint16_t)j;
         }
         __syncthreads();
-        // insertion sort by ID inside each cell (cells hold a few particles)
+        // 2. insertion sort by ID inside each cell (cells hold a few particles)
         for (int c = t; c < DEP_NCELL; c += DEP_NT) {
             const int k0 = cstart[c], m = ccount[c];
             for (int a1 = 1; a1 < m; a1++) {
@@ -404,17 +405,41 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
             }
         }
         __syncthreads();
+        // 3. sorted position of every record (rslot is free again)
+        uint16_t *pos = rslot;
+        for (int k = t; k < nvalid; k += DEP_NT) pos[order[k]] = (uint16_t)k;
+        __syncthreads();
+        // 4. records written in (cell, ID) order
+#pragma unroll
+        for (int u = 0; u < PP; u++) {
+            const int j = t + u * DEP_NT;
+            if (j >= n || rcell[j] == DEP_SKIP) continue;
+            R v[NF], b[NC];
+            int lc;
+            make_record<R, KIND, USE_PHI>(raw[u], N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b);
+            R *dst = rec + (size_t)pos[j] * NFP;
+#pragma unroll
+            for (int k = 0; k < NF; k++) dst[k] = v[k];
+        }
+        __syncthreads();
+        // 5. gather: the 8 source-cell ranges first, then the contiguous records
+        int kb0[8], kb1[8];
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
+            const int lc = (vx - bx + 1) + 9 * ((vy - by + 1) + 9 * (vz - bz + 1));
+            kb0[b] = cstart[lc];
+            kb1[b] = kb0[b] + ccount[lc];
+        }
         R acc[NC];
 #pragma unroll
         for (int c = 0; c < NC; c++) acc[c] = 0;
 #pragma unroll
         for (int b = 0; b < 8; b++) {
             const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
-            const int lc = (vx - bx + 1) + 9 * ((vy - by + 1) + 9 * (vz - bz + 1));
-            const int k0 = cstart[lc], k1 = k0 + ccount[lc];
-            for (int k = k0; k < k1; k++) {
+            for (int k = kb0[b]; k < kb1[b]; k++) {
                 R r[NFP];
-                load_record<R, NFP>(rec + (size_t)order[k] * NFP, r);
+                load_record<R, NFP>(rec + (size_t)k * NFP, r);
                 gather_sum<R, KIND, USE_PHI>(r, bx, by, bz, phv, phx, phy, phz, acc);
             }
         }
