@@ -174,6 +174,7 @@ struct CtxBase {
     virtual void particles_set(const double *pos, const double *q, const int64_t *id, int64_t n, double mass) = 0;
     virtual void particles_get(double *pos, double *q, int64_t *id, int64_t cap, int64_t *n_out) = 0;
     virtual int64_t particles_count() const = 0;
+    virtual double particle_mass() const = 0;
     virtual void field_get(int f, double *host) = 0;
     virtual void field_set(int f, const double *host) = 0;
     virtual void project(uint32_t which, double a, double coeff, int use_phi, int accumulate) = 0;
@@ -435,6 +436,7 @@ template <class R> struct Ctx final : CtxBase {
     }
 
     int64_t particles_count() const override { return np; }
+    double particle_mass() const override { return mass; }
 
     // (device pointer, number of planes, complex?) of a field
     void field_ref(int f, void **p, int *planes, bool *cplx)
@@ -1032,5 +1034,100 @@ int gev_synchronize(gev_ctx *ctx)
 void *gev_stream(gev_ctx *ctx) { return (ctx && ctx->impl) ? (void *)ctx->impl->stream() : nullptr; }
 
 int64_t gev_kernel_launches(const gev_ctx *ctx) { return (ctx && ctx->impl) ? ctx->impl->kernel_launches() : -1; }
+
+
+// ---- checkpoint / restart ----
+// File: "GEVCKPT1", int32 {version, N, precision, vector_method, tensor, 0},
+// int64 np, double {mass, boxsize}, gev_state, particles (pos 3np, q 3np as
+// double, id np as int64), then the field planes as doubles: PHI, CHI, BI,
+// and HIJ_FT, HIJP_FT (tensor state) and BI_FT (parabolic B state) when the
+// context keeps them.  Fields are stored in FP64 whatever the precision mode.
+namespace {
+const char GEV_CKPT_MAGIC[8] = {'G', 'E', 'V', 'C', 'K', 'P', 'T', '1'};
+
+int64_t field_doubles(const gev_config &c, int f)
+{
+    const int64_t N = c.N, P = c.N / 2 + 1;
+    const bool ft = (f == GEV_FIELD_HIJ_FT || f == GEV_FIELD_HIJP_FT || f == GEV_FIELD_BI_FT);
+    return (int64_t)gev_field_components(f) * (ft ? 2 * P * N * N : N * N * N);
+}
+
+std::vector<int> ckpt_fields(const gev_config &c)
+{
+    std::vector<int> f = {GEV_FIELD_PHI, GEV_FIELD_CHI, GEV_FIELD_BI};
+    if (c.tensor) { f.push_back(GEV_FIELD_HIJ_FT); f.push_back(GEV_FIELD_HIJP_FT); }
+    if (c.vector_method == GEV_VECTOR_PARABOLIC) f.push_back(GEV_FIELD_BI_FT);
+    return f;
+}
+
+struct FileCloser {
+    FILE *f;
+    ~FileCloser() { if (f) fclose(f); }
+};
+}  // namespace
+
+int gev_checkpoint_write(gev_ctx *ctx, const char *path, const gev_state *st)
+{
+    if (!ctx || !ctx->impl || !path || !st) return GEV_ERR_ARG;
+    return guarded(ctx, [&](gev::CtxBase &c) {
+        const int64_t np = c.particles_count();
+        std::vector<double> pos(3 * (size_t)np), q(3 * (size_t)np);
+        std::vector<int64_t> id((size_t)np);
+        int64_t got = 0;
+        if (np > 0) c.particles_get(pos.data(), q.data(), id.data(), np, &got);
+        FileCloser fc{fopen(path, "wb")};
+        if (!fc.f) throw gev::ArgError(std::string("cannot open ") + path + " for writing");
+        const int32_t hdr[6] = {1, c.cfg.N, c.cfg.precision, c.cfg.vector_method, c.cfg.tensor, 0};
+        const double md[2] = {c.particle_mass(), c.cfg.boxsize};
+        bool ok = fwrite(GEV_CKPT_MAGIC, 8, 1, fc.f) == 1 && fwrite(hdr, sizeof hdr, 1, fc.f) == 1 &&
+                  fwrite(&np, 8, 1, fc.f) == 1 && fwrite(md, sizeof md, 1, fc.f) == 1 &&
+                  fwrite(st, sizeof(gev_state), 1, fc.f) == 1;
+        if (np > 0)
+            ok = ok && fwrite(pos.data(), 8, pos.size(), fc.f) == pos.size() && fwrite(q.data(), 8, q.size(), fc.f) == q.size() &&
+                 fwrite(id.data(), 8, id.size(), fc.f) == id.size();
+        for (int f : ckpt_fields(c.cfg)) {
+            std::vector<double> buf((size_t)field_doubles(c.cfg, f));
+            c.field_get(f, buf.data());
+            ok = ok && fwrite(buf.data(), 8, buf.size(), fc.f) == buf.size();
+        }
+        if (!ok) throw gev::ArgError(std::string("write error on ") + path);
+        if (fclose(fc.f) != 0) { fc.f = nullptr; throw gev::ArgError(std::string("write error on ") + path); }
+        fc.f = nullptr;
+    });
+}
+
+int gev_checkpoint_read(gev_ctx *ctx, const char *path, gev_state *st)
+{
+    if (!ctx || !ctx->impl || !path || !st) return GEV_ERR_ARG;
+    return guarded(ctx, [&](gev::CtxBase &c) {
+        FileCloser fc{fopen(path, "rb")};
+        if (!fc.f) throw gev::ArgError(std::string("cannot open ") + path);
+        char magic[8];
+        int32_t hdr[6];
+        int64_t np = 0;
+        double md[2];
+        gev_state s{};
+        if (fread(magic, 8, 1, fc.f) != 1 || memcmp(magic, GEV_CKPT_MAGIC, 8) != 0) throw gev::ArgError("not a checkpoint file");
+        if (fread(hdr, sizeof hdr, 1, fc.f) != 1 || fread(&np, 8, 1, fc.f) != 1 || fread(md, sizeof md, 1, fc.f) != 1 ||
+            fread(&s, sizeof s, 1, fc.f) != 1)
+            throw gev::ArgError("truncated checkpoint header");
+        if (hdr[0] != 1) throw gev::ArgError("unsupported checkpoint version");
+        if (hdr[1] != c.cfg.N || hdr[3] != c.cfg.vector_method || (hdr[4] != 0) != (c.cfg.tensor != 0))
+            throw gev::ArgError("checkpoint grid or metric configuration differs from the context");
+        if (np < 0 || np > c.cfg.capacity) throw gev::ArgError("checkpoint holds more particles than the context capacity");
+        std::vector<double> pos(3 * (size_t)np), q(3 * (size_t)np);
+        std::vector<int64_t> id((size_t)np);
+        if (np > 0 && (fread(pos.data(), 8, pos.size(), fc.f) != pos.size() || fread(q.data(), 8, q.size(), fc.f) != q.size() ||
+                       fread(id.data(), 8, id.size(), fc.f) != id.size()))
+            throw gev::ArgError("truncated checkpoint particles");
+        c.particles_set(pos.data(), q.data(), id.data(), np, md[0]);
+        for (int f : ckpt_fields(c.cfg)) {
+            std::vector<double> buf((size_t)field_doubles(c.cfg, f));
+            if (fread(buf.data(), 8, buf.size(), fc.f) != buf.size()) throw gev::ArgError("truncated checkpoint fields");
+            c.field_set(f, buf.data());
+        }
+        *st = s;
+    });
+}
 
 }  // extern "C"

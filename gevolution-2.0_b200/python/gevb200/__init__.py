@@ -107,6 +107,8 @@ def version():
 
 
 _poisson_noalloc = _sig("gev_poisson_noalloc", [_i, _i, _p, _p, _d, _d, _p])
+_ckw = _sig("gev_checkpoint_write", [_p, ctypes.c_char_p, ctypes.POINTER(State)])
+_ckr = _sig("gev_checkpoint_read", [_p, ctypes.c_char_p, ctypes.POINTER(State)])
 
 
 def poisson_noalloc(N, precision, source_ptr, phi_ptr, poisson_coeff, modif, stream=None):
@@ -273,3 +275,11 @@ class Context:
     def step(self, cosmo, state):
         self._ck(_step(self._h, ctypes.byref(cosmo), ctypes.byref(state)))
         return state
+
+    def checkpoint_write(self, path, state):
+        self._ck(_ckw(self._h, str(path).encode(), ctypes.byref(state)))
+
+    def checkpoint_read(self, path):
+        st = State()
+        self._ck(_ckr(self._h, str(path).encode(), ctypes.byref(st)))
+        return st

@@ -234,6 +234,55 @@ double gev_particle_horizon(double a, double fourpiG, const gev_cosmo *cosmo);
 int gev_poisson_noalloc(int32_t N, int32_t precision, const void *source, void *phi,
                         double poisson_coeff, double modif, void *stream);
 
+/* ---- Gadget-2 files (the lightcone output and snapshots) ----
+ * The header mirrors gadget2_header (metadata.hpp:159-178), 256 bytes.  Files
+ * hold four blocks with uint32 record lengths before and after each: header,
+ * POS (3n float), VEL (3n float), ID (n int64), as the reference's
+ * saveGadget2 writes them (Particles_gevolution.hpp:300-323, :826-840).
+ * npart[1], npartTotal[1] and npartTotalHW[1] are set from n; the other
+ * fields are the caller's (the reference fills them at output.hpp:2097-2123). */
+typedef struct {
+    uint32_t npart[6];
+    double mass[6];
+    double time;
+    double redshift;
+    int32_t flag_sfr;
+    int32_t flag_feedback;
+    uint32_t npartTotal[6];
+    int32_t flag_cooling;
+    int32_t num_files;
+    double BoxSize;
+    double Omega0;
+    double OmegaLambda;
+    double HubbleParam;
+    int32_t flag_age;
+    int32_t flag_metals;
+    uint32_t npartTotalHW[6];
+    char fill[64];
+} gev_gadget2_header;
+
+/* Write host arrays (e.g. gev_lightcone_fetch output, positions already in the
+ * header's length unit) as one Gadget-2 file. */
+int gev_gadget2_write(const char *path, const gev_gadget2_header *hdr, const float *pos, const float *vel,
+                      const int64_t *ids, int64_t n);
+/* Snapshot of the context's particles (saveGadget2, Particles_gevolution.hpp:
+ * 218-420 without the redshift interpolation): particles whose ID is a
+ * multiple of tracer_factor, pos * hdr->BoxSize, vel = q / a^1.5 in Gadget
+ * velocity units with a = hdr->time. */
+int gev_snapshot_gadget2(gev_ctx *ctx, const char *path, const gev_gadget2_header *hdr, int32_t tracer_factor);
+
+/* ---- Checkpoint and restart ----
+ * Everything a context needs to continue a run: particles (positions,
+ * momenta, IDs, mass), the metric fields phi, chi, B_i, the h_ij / h_ij'
+ * Fourier state (tensor contexts) and the parabolic B_i state, in FP64, plus
+ * the caller's gev_state.  Reading requires a context of the same N, vector
+ * method and tensor flag with enough capacity; the precision may differ.  The
+ * reference's GPU build stops at its hibernation points instead of writing a
+ * checkpoint (main.cu:1288-1303; the CPU build's writer is hibernation.hpp),
+ * so this is the restart path of this build. */
+int gev_checkpoint_write(gev_ctx *ctx, const char *path, const gev_state *st);
+int gev_checkpoint_read(gev_ctx *ctx, const char *path, gev_state *st);
+
 /* ---- Differentiable Newtonian PM run and its adjoint ----
  * A run of nsteps Newtonian particle-mesh steps, main.cu's gr_flag == 0 branch
  * for CDM: scalarProjectionCIC_project (gevolution.hpp:1902), FFT,
