@@ -105,7 +105,7 @@ __host__ __device__ __forceinline__ uint32_t bucket_of_cell(int N, int nt, int x
 // x-pass load modes (fused source preparation)
 enum { FX_COPY = 0, FX_PREP_T00 = 1, FX_PREP_TIJ = 2 };
 // z-pass Fourier-space operators
-enum { OP_POISSON = 0, OP_SCALAR = 1, OP_VECTOR = 2, OP_BIN = 3 };
+enum { OP_POISSON = 0, OP_SCALAR = 1, OP_VECTOR = 2, OP_BIN = 3, OP_ZELD = 4 };
 // optional extras of OP_SCALAR
 enum { EXTRA_TENSOR_PROJECT = 1, EXTRA_TENSOR_EVOLVE = 2, EXTRA_VECTOR_EVOLVE = 4 };
 

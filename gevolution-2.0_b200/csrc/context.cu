@@ -186,6 +186,7 @@ struct CtxBase {
     virtual void lightcone(const gev_lightcone_args &lc, double tau, double dtau, double dtau_old, double a, double dadtau,
                            int64_t cap, float *pos, float *vel, int64_t *ids, int64_t *n_out) = 0;
     virtual void fetch_lightcone(int64_t cap, float *pos, float *vel, int64_t *ids, int64_t *n_out) = 0;
+    virtual void ics_zeldovich(const gev_ics_params &ip) = 0;
     virtual void sync() = 0;
     virtual cudaStream_t stream() = 0;
     virtual int64_t kernel_launches() const = 0;
@@ -412,6 +413,78 @@ template <class R> struct Ctx final : CtxBase {
         cur_is_A = true;
         rebin_from_cells();
         have_particles = true;
+        sync();
+    }
+
+    void ics_zeldovich(const gev_ics_params &ip) override
+    {
+        const int N = g.N;
+        if (cfg.capacity < g.n3) throw ArgError("the context capacity is below N^3 particles");
+        if (ip.boxsize <= 0.0 || ip.a <= 0.0 || ip.fourpiG <= 0.0) throw ArgError("boxsize, a and fourpiG must be positive");
+        if (ip.n_pk < 2 || !ip.pk_k || !ip.pk_p) throw ArgError("the power spectrum table needs at least two points");
+        std::vector<double> tab(2 * (size_t)ip.n_pk);
+        for (int i = 0; i < ip.n_pk; i++) {
+            if (!(ip.pk_k[i] > 0.0) || !(ip.pk_p[i] > 0.0) || (i > 0 && !(ip.pk_k[i] > ip.pk_k[i - 1])))
+                throw ArgError("power spectrum table: k must increase and k, P must be positive");
+            tab[i] = std::log(ip.pk_k[i]);
+            tab[ip.n_pk + i] = std::log(ip.pk_p[i]);
+        }
+        DBuf<double> dtab;
+        dtab.alloc(tab.size(), "P(k) table");
+        ck(cudaMemcpyAsync(dtab.p, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
+        // 1. white noise
+        if (ip.noise) field_set(GEV_FIELD_SOURCE, ip.noise);
+        else {
+            launch_ics_noise<R>(source.p, g.n3, ip.seed, st);
+            launched("ics noise");
+        }
+        if (ip.noise_out) field_get(GEV_FIELD_SOURCE, ip.noise_out);
+        // 2. displacement field into the B_i planes
+        const FftTables<R> tb = tables();
+        fx_forward<R>(N, FX_COPY, source.p, g.n3, 1, 0, nullptr, nullptr, 0, 0, 0, 0, W.p, g.nk, nullptr, tb, st);
+        fy_pass<R>(N, -1, W.p, g.nk, 1, tb, st);
+        FzParams fz{};
+        fz.op = OP_ZELD;
+        fz.p0 = ip.boxsize;
+        fz.p1 = ip.ksphere ? 1.0 : 0.0;
+        fz.tab = dtab.p;
+        fz.ntab = ip.n_pk;
+        fz.err = derr.p;
+        fz_pass<R>(N, fz, W.p, g.nk, nullptr, nullptr, nullptr, tb, st);
+        fy_pass<R>(N, 1, W.p, g.nk, 3, tb, st);
+        fx_inverse<R>(N, W.p, g.nk, Bi.p, g.n3, 3, tb, st);
+        launched("ics displacement", 5);
+        // 3. the displaced lattice (part_simple_info.mass = Omega_m / Np, ic_basic.hpp:2198-2201)
+        np = g.n3;
+        mass = ip.Omega_m / (double)g.n3;
+        cur_is_A = true;
+        launch_ics_lattice<R>(view(true), Bi.p, N, st);
+        launched("ics lattice");
+        rebin_from_cells();
+        have_particles = true;
+        // 4. phi from the CIC density of the particles (ic_basic.hpp:2404-2427)
+        project(GEV_PROJ_CIC, 1.0, 1.0, 0, 0);
+        gev_cosmo cm{ip.Omega_m, ip.Omega_Lambda, ip.Omega_rad, ip.fourpiG, 0.0, 0.0, 0.0, ip.boxsize};
+        const double H = hconf(ip.a, ip.fourpiG, cm);
+        fx_forward<R>(N, FX_COPY, source.p, g.n3, 1, 0, nullptr, nullptr, 0, 0, 0, 0, W.p, g.nk, nullptr, tb, st);
+        fy_pass<R>(N, -1, W.p, g.nk, 1, tb, st);
+        FzParams fp{};
+        fp.op = OP_POISSON;
+        fp.p0 = (ip.fourpiG / ip.a) / -((double)N * (double)N * (double)N);
+        fp.p1 = ip.gr ? 3.0 * (H * H + ip.fourpiG * ip.Omega_m / ip.a) : 0.0;
+        fp.p2 = 1.0;   // remove the k = 0 mode
+        fp.err = derr.p;
+        fz_pass<R>(N, fp, W.p, g.nk, nullptr, nullptr, nullptr, tb, st);
+        fy_pass<R>(N, 1, W.p, g.nk, 1, tb, st);
+        fx_inverse<R>(N, W.p, g.nk, phi.p, g.n3, 1, tb, st);
+        launched("ics phi", 5);
+        // 5. momenta (ic_basic.hpp:2431-2437; Omega_m(a), Omega_rad(a): background.hpp:211-213)
+        const double a = ip.a;
+        const double den = ip.Omega_m + ip.Omega_Lambda * a * a * a + ip.Omega_rad / a;
+        const double om_a = ip.Omega_m / den;
+        const double orad_a = ip.Omega_rad / (ip.Omega_m * a + ip.Omega_Lambda * a * a * a * a + ip.Omega_rad);
+        launch_ics_velocity<R>(cur(), phi.p, N, a / H / (1.5 * om_a + 2.0 * orad_a), st);
+        launched("ics velocity");
         sync();
     }
 
@@ -1035,6 +1108,12 @@ void *gev_stream(gev_ctx *ctx) { return (ctx && ctx->impl) ? (void *)ctx->impl->
 
 int64_t gev_kernel_launches(const gev_ctx *ctx) { return (ctx && ctx->impl) ? ctx->impl->kernel_launches() : -1; }
 
+
+int gev_ics_zeldovich(gev_ctx *ctx, const gev_ics_params *p)
+{
+    if (!p) return fail(ctx, GEV_ERR_ARG, "null argument");
+    return guarded(ctx, [&](gev::CtxBase &c) { c.ics_zeldovich(*p); });
+}
 
 // ---- checkpoint / restart ----
 // File: "GEVCKPT1", int32 {version, N, precision, vector_method, tensor, 0},

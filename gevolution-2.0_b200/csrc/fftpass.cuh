@@ -355,6 +355,8 @@ template <class R> struct FzArgs {
     double *bins;              // OP_BIN: 4*numbins accumulators (k, k^2, P, P^2)
     unsigned long long *occ;   // OP_BIN: mode counts
     int *err;                  // device error word (may be null)
+    const double *tab;         // OP_ZELD: ln k [h/Mpc] (ntab values) then ln P(k) (ntab values)
+    int ntab;
 };
 
 __device__ __forceinline__ double2 zmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
@@ -389,12 +391,13 @@ __device__ __forceinline__ void tt_num(const double *g, const double2 *k, double
 }
 
 template <int OP, int EXTRA> struct OpShape {
-    static constexpr int CIN = (OP == OP_POISSON || OP == OP_BIN) ? 1 : (OP == OP_SCALAR ? 6 : 3);
+    static constexpr int CIN = (OP == OP_POISSON || OP == OP_BIN || OP == OP_ZELD) ? 1 : (OP == OP_SCALAR ? 6 : 3);
     static constexpr int COUT = (OP == OP_BIN) ? 0 : ((OP == OP_POISSON) ? 1 : (OP == OP_SCALAR ? ((EXTRA & EXTRA_VECTOR_EVOLVE) ? 4 : 1) : 3));
+    static constexpr int CMAX = CIN > COUT ? CIN : COUT;   // columns the pass holds at once
     // projectFTscalar alone needs only three kz-independent combinations of the
     // six S_ij (see k_fz), so the z pass transforms three columns instead of six
     static constexpr bool CONTRACT = (OP == OP_SCALAR && EXTRA == 0);
-    static constexpr int CBUF = CONTRACT ? 3 : CIN;
+    static constexpr int CBUF = CONTRACT ? 3 : CMAX;
 };
 
 // Element-wise solver for one (kx, ky, kz): reads CIN values from v, writes
@@ -431,12 +434,42 @@ __device__ __forceinline__ void fz_apply(const FzArgs<R> &a, int N, int kx, int 
             atomicAdd(a.bins + 3 * nb + bin, weight * pw * pw * kk2 * kk2 * kk2 / s / s);
             atomicAdd(a.occ + bin, (unsigned long long)weight);
         }
+    } else if constexpr (OP == OP_ZELD) {
+        // Zel'dovich displacement of a white-noise spectrum (the generator's
+        // counterpart of generateDisplacementField, ic_basic.hpp:1165-1610):
+        // psi_c = i 2 pi n_c / |2 pi n|^2 * sqrt(P(k) N^3 / L^3) * w / N^3 in box
+        // units, n the signed integer wavevector (numpy fftfreq convention),
+        // k = 2 pi |n| / L.  p0 = L [Mpc/h], p1 != 0 cuts |n| > N/2 (k-sphere).
+        const int n0 = kx, n1 = (ky < N / 2) ? ky : ky - N, n2 = (kz < N / 2) ? kz : kz - N;
+        const double kk = (double)n0 * n0 + (double)n1 * n1 + (double)n2 * n2;
+        const double2 w = v[0];
+        v[0] = v[1] = v[2] = make_double2(0.0, 0.0);
+        if (kk == 0.0 || (a.p1 != 0.0 && 4.0 * kk > (double)N * N)) return;
+        const double lk = log(2.0 * 3.14159265358979323846 * sqrt(kk) / a.p0);
+        int lo = 0, hi = a.ntab - 1;
+        double lp;
+        if (lk <= a.tab[0]) lp = a.tab[a.ntab];
+        else if (lk >= a.tab[hi]) lp = a.tab[a.ntab + hi];
+        else {
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (a.tab[mid] <= lk) lo = mid; else hi = mid;
+            }
+            const double t = (lk - a.tab[lo]) / (a.tab[hi] - a.tab[lo]);
+            lp = a.tab[a.ntab + lo] + t * (a.tab[a.ntab + hi] - a.tab[a.ntab + lo]);
+        }
+        const double n3 = (double)N * N * N;
+        const double amp = sqrt(exp(lp) * n3 / (a.p0 * a.p0 * a.p0)) / n3 / (2.0 * 3.14159265358979323846 * kk);
+        const double nc[3] = {(double)n0, (double)n1, (double)n2};
+#pragma unroll
+        for (int c = 0; c < 3; c++) v[c] = make_double2(-nc[c] * amp * w.y, nc[c] * amp * w.x);   // i nc amp w
     } else if constexpr (OP == OP_POISSON) {
-        // solveModifiedPoissonFT: gevolution.hpp:806-852; p0 = coeff / (-N^3), p1 = modif
+        // solveModifiedPoissonFT: gevolution.hpp:806-852; p0 = coeff / (-N^3), p1 = modif;
+        // p2 != 0 removes the k = 0 mode first (ic_basic.hpp:2419-2421)
         double den = k2 + a.p1;
         v[0] = (den != 0.0) ? zsc(v[0], a.p0 / den) : make_double2(0.0, 0.0);
         if (kx == 0 && ky == 0 && kz == 0) {
-            if (a.p1 == 0.0) v[0] = make_double2(0.0, 0.0);
+            if (a.p1 == 0.0 || a.p2 != 0.0) v[0] = make_double2(0.0, 0.0);
             if (a.phi_hom) *a.phi_hom = v[0].x;
         }
     } else if constexpr (OP == OP_VECTOR) {
@@ -591,7 +624,7 @@ __global__ void __launch_bounds__(NT, GEV_FZ_MINB * 256 / NT) k_fz(FzArgs<R> a, 
     __syncthreads();
     // one component at a time keeps the butterfly registers per thread small
 #pragma unroll 1
-    for (int c = 0; c < CBUF; c++) fft_lines<N, -1, T, NT>(buf + c * T, LD, tw);
+    for (int c = 0; c < (CONTRACT ? 3 : CIN); c++) fft_lines<N, -1, T, NT>(buf + c * T, LD, tw);
 
     if constexpr (CONTRACT) {
         for (int idx = threadIdx.x; idx < N * T; idx += NT) {
@@ -657,7 +690,6 @@ __global__ void __launch_bounds__(NT, (FzMinBlocks<OP, EXTRA, NT>::v))
     constexpr int P = N / 2 + 1, PP = N / 2 + 2;
     constexpr int CIN = OpShape<OP, EXTRA>::CIN, COUT = OpShape<OP, EXTRA>::COUT;
     constexpr bool CONTRACT = OpShape<OP, EXTRA>::CONTRACT;
-    constexpr int CBUF = OpShape<OP, EXTRA>::CBUF;
     constexpr int ZB = ZBox<N>::ZB, NZB = ZBox<N>::NZB;
     constexpr int CS = N * T;   // one component: [kz][t], dense
     // bulk tensor copies want 128-byte aligned shared addresses: the launch
@@ -705,7 +737,7 @@ __global__ void __launch_bounds__(NT, (FzMinBlocks<OP, EXTRA, NT>::v))
         __syncthreads();
     }
 #pragma unroll 1
-    for (int c = 0; c < CBUF; c++) fft_lines<N, -1, T, NT>(buf + c * CS, T, tw);
+    for (int c = 0; c < (CONTRACT ? 3 : CIN); c++) fft_lines<N, -1, T, NT>(buf + c * CS, T, tw);
 
     for (int idx = threadIdx.x; idx < CS; idx += NT) {
         const int t = idx % T, n = idx / T, kx = kx0 + t;

@@ -73,11 +73,18 @@ struct FzParams {
     double *bins;
     unsigned long long *occ;
     int *err;   // device error word for the transfer timeout (may be null)
+    const double *tab = nullptr;   // OP_ZELD: ln k then ln P(k), device
+    int ntab = 0;
 };
 template <class R>
 void fz_pass(int N, const FzParams &fp, typename CT<R>::C *data, int64_t stride, typename CT<R>::C *hij,
              typename CT<R>::C *hijp, typename CT<R>::C *bstate, const FftTables<R> &tb, cudaStream_t st);
 int fx_rows_per_block(int N, bool fp64);   // T of the x passes (partial-sum count = N*N/T)
+
+// ---- initial conditions ----
+template <class R> void launch_ics_noise(R *out, int64_t n3, uint64_t seed, cudaStream_t st);
+template <class R> void launch_ics_lattice(PView<R> p, const R *psi, int N, cudaStream_t st);
+template <class R> void launch_ics_velocity(const PView<R> &p, const R *phi, int N, double coeff, cudaStream_t st);
 
 // ---- lightcone ----
 struct LcKernelArgs {

@@ -162,13 +162,13 @@ void fz_n(const FzArgs<R> &a, const FftTables<R> &tb, cudaStream_t st)
     using C = typename CT<R>::C;
     constexpr int T = OpShape<OP, EXTRA>::CONTRACT ? PassCfg<R>::TZC
                       : (OP == OP_POISSON || OP == OP_BIN) ? PassCfg<R>::TZ1
-                      : (OP == OP_VECTOR ? PassCfg<R>::TZ3 : PassCfg<R>::TZ6);
+                      : ((OP == OP_VECTOR || OP == OP_ZELD) ? PassCfg<R>::TZ3 : PassCfg<R>::TZ6);
     constexpr int NT = PassCfg<R>::NTZ;
 #if GEV_FZ_TMA
     static_assert(T % 2 == 0 || sizeof(R) == 8, "TMA boxes need 16-byte rows");
-    constexpr int CIN = OpShape<OP, EXTRA>::CIN;
-    const size_t smem = (size_t)CIN * N * T * sizeof(C) + 128;
-    const CUtensorMap map = fourier_tensor_map<R>(a.data, N, a.stride, CIN, T, 1, ZBox<N>::ZB);
+    constexpr int CMAX = OpShape<OP, EXTRA>::CMAX;
+    const size_t smem = (size_t)CMAX * N * T * sizeof(C) + 128;
+    const CUtensorMap map = fourier_tensor_map<R>(a.data, N, a.stride, CMAX, T, 1, ZBox<N>::ZB);
     auto k = k_fz_tma<R, N, T, NT, OP, EXTRA>;
     set_smem(k, smem);
     k<<<dim3((N / 2 + 1 + T - 1) / T, N), NT, smem, st>>>(a, tb.tw_full, map);
@@ -185,6 +185,7 @@ template <class R, int N>
 void fz_dispatch(const FzParams &fp, const FzArgs<R> &a, const FftTables<R> &tb, cudaStream_t st)
 {
     if (fp.op == OP_POISSON) fz_n<R, N, OP_POISSON, 0>(a, tb, st);
+    else if (fp.op == OP_ZELD) fz_n<R, N, OP_ZELD, 0>(a, tb, st);
     else if (fp.op == OP_BIN) fz_n<R, N, OP_BIN, 0>(a, tb, st);
     else if (fp.op == OP_VECTOR) fz_n<R, N, OP_VECTOR, 0>(a, tb, st);
     else {
@@ -214,6 +215,8 @@ void fz_pass(int N, const FzParams &fp, typename CT<R>::C *data, int64_t stride,
     a.bins = fp.bins;
     a.occ = fp.occ;
     a.err = fp.err;
+    a.tab = fp.tab;
+    a.ntab = fp.ntab;
     GEV_SWITCH_N(N, (fz_dispatch<R, NN>(fp, a, tb, st)))
 }
 

@@ -55,6 +55,12 @@ class State(ctypes.Structure):
                 ("T00hom", _d), ("phi_hom", _d), ("maxvel", _d)]
 
 
+class IcsParams(ctypes.Structure):
+    _fields_ = [("boxsize", _d), ("a", _d), ("fourpiG", _d), ("Omega_m", _d), ("Omega_Lambda", _d),
+                ("Omega_rad", _d), ("seed", ctypes.c_uint64), ("pk_k", _p), ("pk_p", _p), ("n_pk", _i),
+                ("ksphere", _i), ("gr", _i), ("reserved", _i), ("noise", _p), ("noise_out", _p)]
+
+
 class LightconeArgs(ctypes.Structure):
     _fields_ = [("vertex", _d * 3), ("direction", _d * 3), ("opening", _d), ("distance", _d * 2),
                 ("d", _d), ("tracer_factor", _i), ("shell", _i)]
@@ -107,6 +113,7 @@ def version():
 
 
 _poisson_noalloc = _sig("gev_poisson_noalloc", [_i, _i, _p, _p, _d, _d, _p])
+_ics = _sig("gev_ics_zeldovich", [_p, ctypes.POINTER(IcsParams)])
 _ckw = _sig("gev_checkpoint_write", [_p, ctypes.c_char_p, ctypes.POINTER(State)])
 _ckr = _sig("gev_checkpoint_read", [_p, ctypes.c_char_p, ctypes.POINTER(State)])
 
@@ -275,6 +282,20 @@ class Context:
     def step(self, cosmo, state):
         self._ck(_step(self._h, ctypes.byref(cosmo), ctypes.byref(state)))
         return state
+
+    def ics_zeldovich(self, boxsize, a, fourpiG, omega_m, omega_l, pk_k, pk_p, seed=0, omega_rad=0.0,
+                      ksphere=False, gr=True, noise=None, return_noise=False):
+        """Zel'dovich initial conditions (gev_ics_zeldovich): replaces the
+        particles and phi.  pk_k [h/Mpc], pk_p [(Mpc/h)^3] tabulate P(k) at a."""
+        k = np.ascontiguousarray(pk_k, dtype=np.float64)
+        pk = np.ascontiguousarray(pk_p, dtype=np.float64)
+        w = None if noise is None else np.ascontiguousarray(noise, dtype=np.float64).ravel()
+        out = np.empty(self.N ** 3) if return_noise else None
+        prm = IcsParams(float(boxsize), float(a), float(fourpiG), float(omega_m), float(omega_l), float(omega_rad),
+                        int(seed), k.ctypes.data_as(_p), pk.ctypes.data_as(_p), len(k), int(bool(ksphere)),
+                        int(bool(gr)), 0, _ptr(w), _ptr(out))
+        self._ck(_ics(self._h, ctypes.byref(prm)))
+        return out
 
     def checkpoint_write(self, path, state):
         self._ck(_ckw(self._h, str(path).encode(), ctypes.byref(state)))

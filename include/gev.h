@@ -234,6 +234,38 @@ double gev_particle_horizon(double a, double fourpiG, const gev_cosmo *cosmo);
 int gev_poisson_noalloc(int32_t N, int32_t precision, const void *source, void *phi,
                         double poisson_coeff, double modif, void *stream);
 
+/* ---- Zel'dovich initial conditions ----
+ * The path of the reference's IC generator with a tabulated power spectrum
+ * (ic_basic.hpp:1896-1922, 2404-2437, "mPk" branch): a Gaussian white-noise
+ * field (counter-based Philox4x32-10 stream of `seed`, or the caller's
+ * `noise`), shaped into the Zel'dovich displacement psi = grad del^-2 delta
+ * with delta_k = sqrt(P(k) N^3 / L^3) w_k (P interpolated linearly in
+ * ln k / ln P; modes with |n| > N/2 dropped when ksphere != 0), one particle
+ * per cell at the cell centre displaced by psi at its vertex (ID = cell
+ * index, mass = Omega_m / N^3), phi from the CIC density of those particles
+ * by solveModifiedPoissonFT(fourpiG/a, 3 gr (H^2 + fourpiG Omega_m / a)) with
+ * the k = 0 mode removed, and momenta q = -rescale grad phi
+ * (initialize_q_ic_basic, ic_basic.hpp:133-166) with
+ * rescale = a / H_conf / (1.5 Omega_m(a) + 2 Omega_rad(a)).  Replaces the
+ * context's particles and phi. */
+typedef struct {
+    double boxsize;       /* L, Mpc/h */
+    double a;             /* scale factor of the initial conditions */
+    double fourpiG;       /* 4 pi G in the code's units */
+    double Omega_m, Omega_Lambda, Omega_rad;
+    uint64_t seed;
+    const double *pk_k;   /* host: k [h/Mpc], strictly increasing, n_pk values */
+    const double *pk_p;   /* host: P(k) [(Mpc/h)^3] > 0 at a */
+    int32_t n_pk;
+    int32_t ksphere;      /* nonzero: drop modes with |n| > N/2 */
+    int32_t gr;           /* nonzero: GR modification of the Poisson equation */
+    int32_t reserved;
+    const double *noise;  /* optional host N^3 unit white noise used instead of the stream */
+    double *noise_out;    /* optional host N^3: receives the white noise used */
+} gev_ics_params;
+
+int gev_ics_zeldovich(gev_ctx *ctx, const gev_ics_params *p);
+
 /* ---- Gadget-2 files (the lightcone output and snapshots) ----
  * The header mirrors gadget2_header (metadata.hpp:159-178), 256 bytes.  Files
  * hold four blocks with uint32 record lengths before and after each: header,

@@ -684,6 +684,33 @@ double orc_update_q_newton(int N, int64_t np, const double *pos, double *q, cons
     return vmax;
 }
 
+/* initialize_q_ic_basic: ic_basic.hpp:133-166 with one field (nfield = 1):
+ * q = -coeff grad phi / dx, the gradient from the cell's edge differences with
+ * bilinear weights.  Restated from the source; not pinned to a build of the
+ * reference (ic_basic.hpp needs more of LATfield2 than the CPU stand-in has). */
+void orc_initialize_q(int N, int64_t np, const double *pos, double *q, const double *phi, double coeff)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < np; p++) {
+        int c[3]; double d[3];
+        locate(N, pos + 3 * p, c, d);
+        double g[3];
+        g[0] = (1. - d[1]) * (1. - d[2]) * (F(phi, N, c, 1, 0, 0) - F(phi, N, c, 0, 0, 0));
+        g[1] = (1. - d[0]) * (1. - d[2]) * (F(phi, N, c, 0, 1, 0) - F(phi, N, c, 0, 0, 0));
+        g[2] = (1. - d[0]) * (1. - d[1]) * (F(phi, N, c, 0, 0, 1) - F(phi, N, c, 0, 0, 0));
+        g[0] += d[1] * (1. - d[2]) * (F(phi, N, c, 1, 1, 0) - F(phi, N, c, 0, 1, 0));
+        g[1] += d[0] * (1. - d[2]) * (F(phi, N, c, 1, 1, 0) - F(phi, N, c, 1, 0, 0));
+        g[2] += d[0] * (1. - d[1]) * (F(phi, N, c, 1, 0, 1) - F(phi, N, c, 1, 0, 0));
+        g[0] += (1. - d[1]) * d[2] * (F(phi, N, c, 1, 0, 1) - F(phi, N, c, 0, 0, 1));
+        g[1] += (1. - d[0]) * d[2] * (F(phi, N, c, 0, 1, 1) - F(phi, N, c, 0, 0, 1));
+        g[2] += (1. - d[0]) * d[1] * (F(phi, N, c, 0, 1, 1) - F(phi, N, c, 0, 1, 0));
+        g[0] += d[1] * d[2] * (F(phi, N, c, 1, 1, 1) - F(phi, N, c, 0, 1, 1));
+        g[1] += d[0] * d[2] * (F(phi, N, c, 1, 1, 1) - F(phi, N, c, 1, 0, 1));
+        g[2] += d[0] * d[1] * (F(phi, N, c, 1, 1, 1) - F(phi, N, c, 1, 1, 0));
+        for (int k = 0; k < 3; k++) q[3 * p + k] = -g[k] * N * coeff;
+    }
+}
+
 /* update_pos_Newton: gevolution.hpp:1270-1273, pos += dtau q / a (positions
  * left unwrapped: the differentiable run keeps continuous coordinates) */
 void orc_update_pos_newton(int64_t np, double *pos, const double *q, double dtau, double a)

@@ -70,6 +70,9 @@ double orc_update_q_newton(int N, int64_t np, const double *pos, double *q, cons
                            double a);
 void orc_update_pos_newton(int64_t np, double *pos, const double *q, double dtau, double a);
 
+/* ---- initial-condition momenta (ic_basic.hpp:133-166) ---- */
+void orc_initialize_q(int N, int64_t np, const double *pos, double *q, const double *phi, double coeff);
+
 /* ---- background (CDM + Lambda + radiation, no ncdm / fluid) ---- */
 typedef struct {
     double Omega_m, Omega_Lambda, Omega_rad;

@@ -64,6 +64,7 @@ _ORC_EXTRA = {
     "lightcone_select": ([_i, _l, _p, _p, _p, _p, _p, _d, _d, _d, _d, _d, _l, _p, _p, _p, _d], _l),
     "find_intersecting": ([_p, _p, _d, _d, _d, _p, _p], _i),
     "update_pos_newton": ([_l, _p, _p, _d, _d], None),
+    "initialize_q": ([_i, _l, _p, _p, _p, _d], None),
 }
 _REF_EXTRA = {
     "update_pos_newton": ([_i, _l, _p, _p, _d, _d], None),
