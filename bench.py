@@ -170,7 +170,7 @@ def run_gpu(args, rank, world, local_rank):
 
     import gevb200 as gev
     from gevb200 import roofline
-    from gevb200.ics import zeldovich
+    from gevb200.ics import linear_pk
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -178,15 +178,23 @@ def run_gpu(args, rank, world, local_rank):
     box = args.boxsize or 5.0 * N
     np_ = N ** 3
     log("initial conditions %d^3" % N)
-    pos_t, q_t, ids_t, phi_t, mass, a0, fourpiG = zeldovich(N, box, args.z_in, args.seed + 1000 * rank, device=dev)
+    # Zel'dovich ICs generated by the library (gev_ics_zeldovich) in FP64 from the
+    # linear EH no-wiggle P(k) at z_in; every replica has its own seed
+    a0 = 1.0 / (1.0 + args.z_in)
+    fourpiG = 1.5 * box * box / C_LIGHT ** 2
+    mass = OMEGA_M / np_
+    kt = np.logspace(-5, 3, 4096)
+    pt = linear_pk(kt, a0, H_LITTLE, OMEGA_M)
+    with gev.Context(N, precision=gev.FP64, capacity=np_, boxsize=box, device=local_rank) as gen:
+        gen.ics_zeldovich(box, a0, fourpiG, OMEGA_M, OMEGA_L, kt, pt, seed=args.seed + 1000 * rank)
+        p_, q_, i_ = gen.get_particles()
+        phi_h = gen.get_field(gev.FIELD_PHI).ravel()
     log("initial conditions done")
     # host copies in pinned memory: the C ABI takes host buffers
-    pos_h = pos_t.cpu().pin_memory().numpy()
-    q_h = q_t.cpu().pin_memory().numpy()
-    ids_h = ids_t.cpu().pin_memory().numpy()
-    phi_h = phi_t.cpu().numpy()
-    del pos_t, q_t, ids_t, phi_t
-    torch.cuda.empty_cache()
+    pos_h = torch.from_numpy(p_).pin_memory().numpy()
+    q_h = torch.from_numpy(q_).pin_memory().numpy()
+    ids_h = torch.from_numpy(i_).pin_memory().numpy()
+    del p_, q_, i_
 
     z_relax = args.z_in
     cosmo = gev.Cosmo(OMEGA_M, OMEGA_L, 0.0, fourpiG, 48.0, 0.04, z_relax, box)
@@ -364,7 +372,8 @@ def run_gpu(args, rank, world, local_rank):
             "value": value, "unit": "Mpart-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 fields/FFT + f64 particle offsets, background and reductions",
-            "data": "synthetic: seeded Zel'dovich ICs (EH no-wiggle P(k)) at z=%g" % args.z_in,
+            "data": "synthetic: Zel'dovich ICs at z=%g generated on the GPU by gev_ics_zeldovich (Philox4x32-10 white noise, "
+                    "seed %d, linear EH no-wiggle P(k))" % (args.z_in, args.seed),
             "config": workload_config(N, box, world),
             "gpu_launches": launches,
             "stage_ms": stages,
