@@ -114,6 +114,7 @@ constexpr int ERR_NONFINITE = 1;       // a particle coordinate became non-finit
 constexpr int ERR_LC_OVERFLOW = 2;     // lightcone output exceeded its capacity
 constexpr int ERR_BAD_CELL = 4;        // a particle cell index outside the lattice
 constexpr int ERR_TMA_TIMEOUT = 8;     // a bulk tensor copy did not complete within the wait limit
+constexpr int ERR_BAD_ORDER = 16;      // a deposit found a cell's particles not contiguous in their bucket
 
 // kernel launch helper
 inline unsigned int cdiv(int64_t a, int64_t b) { return (unsigned int)((a + b - 1) / b); }

@@ -201,7 +201,7 @@ template <class R> struct Ctx final : CtxBase {
     DBuf<C> tw_full, tw_half;
     DBuf<double> k2;
     DBuf<double2> ks;
-    DBuf<uint32_t> cellA, cellB, bucket, rank, counts, bstart, bsums;
+    DBuf<uint32_t> cellA, cellB, bucket, rank, inv, counts, bstart, bsums;
     DBuf<double> offA, offB;
     DBuf<R> qA, qB;
     DBuf<int64_t> idA, idB;
@@ -258,7 +258,7 @@ template <class R> struct Ctx final : CtxBase {
         offA.alloc(3 * cap, "particles"); offB.alloc(3 * cap, "particles");
         qA.alloc(3 * cap, "particles"); qB.alloc(3 * cap, "particles");
         idA.alloc(cap, "particles"); idB.alloc(cap, "particles");
-        bucket.alloc(cap, "buckets"); rank.alloc(cap, "buckets");
+        bucket.alloc(cap, "buckets"); rank.alloc(cap, "buckets"); inv.alloc(cap, "buckets");
         const int64_t nb = g.ntiles * 8;
         counts.alloc(nb, "bucket counts");
         bstart.alloc(nb + 1, "bucket starts");
@@ -342,10 +342,10 @@ template <class R> struct Ctx final : CtxBase {
         ck(cudaStreamSynchronize(st), "synchronize");
         if (e) {
             ck(cudaMemsetAsync(derr.p, 0, sizeof(int), st), "memset");
-            char buf[160];
-            snprintf(buf, sizeof buf, "device error word 0x%x (%s%s%s%s)", e, (e & ERR_NONFINITE) ? "non-finite particle coordinate " : "",
+            char buf[224];
+            snprintf(buf, sizeof buf, "device error word 0x%x (%s%s%s%s%s)", e, (e & ERR_NONFINITE) ? "non-finite particle coordinate " : "",
                      (e & ERR_LC_OVERFLOW) ? "lightcone buffer overflow " : "", (e & ERR_BAD_CELL) ? "cell index out of range " : "",
-                     (e & ERR_TMA_TIMEOUT) ? "bulk tensor copy timed out" : "");
+                     (e & ERR_TMA_TIMEOUT) ? "bulk tensor copy timed out " : "", (e & ERR_BAD_ORDER) ? "bucket order not sorted by cell" : "");
             throw DeviceError(buf);
         }
     }
@@ -377,8 +377,8 @@ template <class R> struct Ctx final : CtxBase {
         const int64_t nb = g.ntiles * 8;
         launch_scan(counts.p, bstart.p, nb, bsums.p, st);
         launched("scan", 3);
-        launch_scatter<R>(cur(), view(!cur_is_A), bstart.p, bucket.p, rank.p, st);
-        launched("scatter");
+        launch_rebin<R>(cur(), view(!cur_is_A), bstart.p, bucket.p, rank.p, inv.p, g.N, derr.p, st);
+        launched("rebin", 2);
         cur_is_A = !cur_is_A;
     }
 
@@ -598,19 +598,19 @@ template <class R> struct Ctx final : CtxBase {
                 kind = DEP_TIJ;
                 for (int c = 0; c < 6; c++) o.p[c] = Sij.p + c * g.n3;
             }
-            launch_deposit<R>(kind, use_phi != 0, v, bstart.p, g.N, phi.p, o, a, m00, mij, accumulate, st);
+            launch_deposit<R>(kind, use_phi != 0, v, bstart.p, g.N, phi.p, o, a, m00, mij, accumulate, derr.p, st);
             launched("deposit T00/Tij");
         }
         if (which & GEV_PROJ_CIC) {
             DepOut<R> o{};
             o.p[0] = source.p;
-            launch_deposit<R>(DEP_T00, false, v, bstart.p, g.N, phi.p, o, 1.0, mass * coeff * n3, 0.0, accumulate, st);
+            launch_deposit<R>(DEP_T00, false, v, bstart.p, g.N, phi.p, o, 1.0, mass * coeff * n3, 0.0, accumulate, derr.p, st);
             launched("deposit CIC");
         }
         if (which & GEV_PROJ_T0I) {
             DepOut<R> o{};
             for (int c = 0; c < 3; c++) o.p[c] = Bi.p + c * g.n3;
-            launch_deposit<R>(DEP_T0I, use_phi != 0, v, bstart.p, g.N, phi.p, o, 1.0, mass * coeff * n3, 0.0, accumulate, st);
+            launch_deposit<R>(DEP_T0I, use_phi != 0, v, bstart.p, g.N, phi.p, o, 1.0, mass * coeff * n3, 0.0, accumulate, derr.p, st);
             launched("deposit T0i");
         }
     }

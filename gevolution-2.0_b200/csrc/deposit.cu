@@ -4,21 +4,22 @@
 // every particle whose CIC stencil touches them: its own 8 class buckets plus
 // the face-class buckets of the 7 lower neighbour tiles (tile_segments_block).
 //
-// Per chunk of particles the CTA
+// The CTA
 //   1. turns each particle into a short record of per-particle factors (in the
-//      field precision R) and counts it into one of the 9^3 cells of the
-//      tile's reach (relative cell -1..7 per axis);
-//   2. scans the cell counts and sorts record indexes by cell (counting sort);
+//      field precision R) and finds the one of the 9^3 cells of the tile's
+//      reach (relative cell -1..7 per axis) that it lies in;
+//   2. finds the records of each reach cell: when the reach fits one chunk
+//      (the common case) they already form one run, because the re-binning
+//      keeps small buckets in (cell, particle ID) order; denser tiles sort
+//      record indexes by cell (counting sort) chunk by chunk;
 //   3. lets every vertex thread walk the 8 cells whose stencil covers it and
 //      accumulate the contributions in registers -- no shared-memory atomics
 //      on the accumulation path, each output vertex written once with plain
 //      stores, no global atomics and no halo fold (projection_comm1,
 //      gevolution.hpp:1543, is not needed on one GPU).
-// The result does not depend on the order of the particles in memory
+// The result does not depend on the order in which the particles were given
 // (bitwise reproducible, for unique particle IDs):
-//   - when the tile's reach fits one chunk (the common case) the records of
-//     each cell are ordered by particle ID and each vertex sums in R in the
-//     fixed order (source cell, ID);
+//   - single chunk: each vertex sums in R in the fixed order (source cell, ID);
 //   - denser tiles take several chunks and accumulate 64-bit fixed point with
 //     a per-CTA, per-component scale from an upper bound of the contributions
 //     and the particle count, so the sum is exact integer arithmetic.
@@ -38,6 +39,8 @@ constexpr int DEP_NT = 512;   // one thread per tile vertex
 template <class R> struct DepCh;
 template <> struct DepCh<float> { static constexpr int v = 1024; static constexpr int EMAX = 120; };
 template <> struct DepCh<double> { static constexpr int v = 768; static constexpr int EMAX = 1000; };
+static_assert(DepCh<float>::v <= REBIN_SORT_MAX && DepCh<double>::v <= REBIN_SORT_MAX,
+              "a single-chunk deposit must only see buckets that the re-binning keeps sorted");
 
 // record layout: [d0 d1 d2 | T00: E F G | Tij: W00 W11 W22 W01 W02 W12 | T0i: Q0 Q1 Q2]
 template <int KIND> struct DepShape {
@@ -243,7 +246,7 @@ __host__ __device__ constexpr size_t dep_smem_bytes()
 template <class R, int KIND, bool USE_PHI>
 __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt,
                                                        const R *__restrict__ phi, DepOut<R> out, double a, double m00,
-                                                       double mij, int accumulate, FastDiv fN)
+                                                       double mij, int accumulate, int *err, FastDiv fN)
 {
     using S = DepShape<KIND>;
     constexpr int NC = S::NC, NF = S::NF, NFP = S::NFP;
@@ -262,7 +265,6 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
     __shared__ R scl_s[NC];
     __shared__ double iscl_s[NC];
     __shared__ int wsum[DEP_NT / 32];
-    __shared__ int64_t rid[CH];   // particle IDs of the records (single-chunk path)
 
     const int t = threadIdx.x;
     const int tile = blockIdx.x;
@@ -272,7 +274,7 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
     const R ra = (R)a, rm00 = (R)m00, rmij = (R)mij;
     tile_segments_block(bstart, nt, tx, ty, tz, seg_lo, seg_hi, seg_pre);
     if (t < NC) vmax[t] = 0ull;
-    for (int c = t; c < 730; c += DEP_NT) ccount[c] = 0;
+    for (int c = t; c < 730; c += DEP_NT) { cstart[c] = 0; ccount[c] = 0; }
     if (USE_PHI) {
         constexpr int PER = (1000 + DEP_NT - 1) / DEP_NT;
         R pv[PER];
@@ -344,84 +346,61 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
     const int64_t gout = sidx(N, x0 + vx, y0 + vy, z0 + vz);
 
     if (!multi) {
-        // Single chunk (the common case): records are sorted by cell and, inside
-        // each cell, by particle ID; every vertex then sums its contributions in
-        // the field precision in a fixed order (source cell, then ID), so the
-        // result is again independent of the particle order in memory.
+        // Single chunk (the common case).  The re-binning keeps every bucket
+        // this small in (cell, particle ID) order, so in the concatenation of
+        // the candidate buckets the records of each reach cell form one run,
+        // already ordered by ID: records stay at their load position and every
+        // vertex sums its contributions in the field precision in a fixed
+        // order (source cell, then ID) -- independent of the order in which
+        // the particles were given.
         const int n = (int)total;
-        // at most two particles per thread (n <= CH <= 2 DEP_NT); their loads are
-        // issued together and the raw words stay in registers until each
-        // record is written straight to its sorted position
+        // at most two particles per thread (n <= CH <= 2 DEP_NT), loads issued together
         constexpr int PP = (CH + DEP_NT - 1) / DEP_NT;
         RawParticle<R> raw[PP];
-        int64_t pid[PP];
 #pragma unroll
         for (int u = 0; u < PP; u++) {
             const int j = t + u * DEP_NT;
-            if (j < n) {
-                const uint32_t i = seg_index(seg_lo, seg_pre, (uint32_t)j);
-                raw[u] = load_particle(p, i);
-                pid[u] = p.id[i];
-            }
+            if (j < n) raw[u] = load_particle(p, seg_index(seg_lo, seg_pre, (uint32_t)j));
         }
-        // 1. cell of each record inside the tile's reach and its slot in that cell
+        // 1. record j at position j, and the reach cell it came from
 #pragma unroll
         for (int u = 0; u < PP; u++) {
             const int j = t + u * DEP_NT;
             if (j >= n) continue;
-            int cx, cy, cz;
-            decode_cell(raw[u].cell, fN, cx, cy, cz);
-            const int rx = rel_coord(cx, x0, N), ry = rel_coord(cy, y0, N), rz = rel_coord(cz, z0, N);
-            if (rx < -1 || rx > 7 || ry < -1 || ry > 7 || rz < -1 || rz > 7) {
-                rcell[j] = DEP_SKIP;
-            } else {
-                const int lc = (rx + 1) + 9 * ((ry + 1) + 9 * (rz + 1));
-                rid[j] = pid[u];
-                rcell[j] = (uint16_t)lc;
-                rslot[j] = (uint16_t)atomicAdd(&ccount[lc], 1);
-            }
-        }
-        __syncthreads();
-        scan_cells();
-        __syncthreads();
-        const int nvalid = cstart[DEP_NCELL - 1] + ccount[DEP_NCELL - 1];
-        for (int j = t; j < n; j += DEP_NT) {
-            const uint16_t lc = rcell[j];
-            if (lc != DEP_SKIP) order[cstart[lc] + rslot[j]] = (uint16_t)j;
-        }
-        __syncthreads();
-        // 2. insertion sort by ID inside each cell (cells hold a few particles)
-        for (int c = t; c < DEP_NCELL; c += DEP_NT) {
-            const int k0 = cstart[c], m = ccount[c];
-            for (int a1 = 1; a1 < m; a1++) {
-                const uint16_t key = order[k0 + a1];
-                const int64_t kid = rid[key];
-                int b1 = a1 - 1;
-                while (b1 >= 0 && rid[order[k0 + b1]] > kid) {
-                    order[k0 + b1 + 1] = order[k0 + b1];
-                    b1--;
-                }
-                order[k0 + b1 + 1] = key;
-            }
-        }
-        __syncthreads();
-        // 3. sorted position of every record (rslot is free again)
-        uint16_t *pos = rslot;
-        for (int k = t; k < nvalid; k += DEP_NT) pos[order[k]] = (uint16_t)k;
-        __syncthreads();
-        // 4. records written in (cell, ID) order
-#pragma unroll
-        for (int u = 0; u < PP; u++) {
-            const int j = t + u * DEP_NT;
-            if (j >= n || rcell[j] == DEP_SKIP) continue;
             R v[NF], b[NC];
             int lc;
-            make_record<R, KIND, USE_PHI>(raw[u], N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b);
-            R *dst = rec + (size_t)pos[j] * NFP;
+            if (make_record<R, KIND, USE_PHI>(raw[u], N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
+                R *dst = rec + (size_t)j * NFP;
 #pragma unroll
-            for (int k = 0; k < NF; k++) dst[k] = v[k];
+                for (int k = 0; k < NF; k++) dst[k] = v[k];
+                rcell[j] = (uint16_t)lc;
+            } else {
+                rcell[j] = DEP_SKIP;
+            }
         }
         __syncthreads();
+        // 2. cell runs [cstart, cend) from the run boundaries (cend shares ccount's storage)
+        int *cend = ccount;
+        for (int j = t; j < n; j += DEP_NT) {
+            const uint16_t lc = rcell[j];
+            if (lc == DEP_SKIP) continue;
+            if (j == 0 || rcell[j - 1] != lc) cstart[lc] = j;
+            if (j == n - 1 || rcell[j + 1] != lc) cend[lc] = j + 1;
+        }
+        __syncthreads();
+        // 3. every record lies inside its cell's run and is followed by the
+        //    same cell up to the run's end: then each run holds exactly its
+        //    cell's records (otherwise the bucket order was not sorted by cell)
+        {
+            bool bad = false;
+            for (int j = t; j < n; j += DEP_NT) {
+                const uint16_t lc = rcell[j];
+                if (lc == DEP_SKIP) continue;
+                const int e = cend[lc];
+                bad |= j < cstart[lc] || j >= e || (j + 1 < e && rcell[j + 1] != lc);
+            }
+            if (bad) atomicOr(err, ERR_BAD_ORDER);
+        }
         // 5. gather: the 8 source-cell ranges first, then the contiguous records
         int kb0[8], kb1[8];
 #pragma unroll
@@ -429,7 +408,7 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
             const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
             const int lc = (vx - bx + 1) + 9 * ((vy - by + 1) + 9 * (vz - bz + 1));
             kb0[b] = cstart[lc];
-            kb1[b] = kb0[b] + ccount[lc];
+            kb1[b] = cend[lc];
         }
         R acc[NC];
 #pragma unroll
@@ -558,7 +537,7 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
 
 template <class R, int KIND, bool USE_PHI>
 static void launch_k(const PView<R> &p, const uint32_t *bstart, int N, const R *phi, const DepOut<R> &out, double a,
-                     double m00, double mij, int accumulate, cudaStream_t st)
+                     double m00, double mij, int accumulate, int *err, cudaStream_t st)
 {
     constexpr size_t smem = dep_smem_bytes<R, KIND>();
     static bool attr_set = false;
@@ -568,18 +547,18 @@ static void launch_k(const PView<R> &p, const uint32_t *bstart, int N, const R *
     }
     const int nt = N / 8;
     const unsigned grid = (unsigned)nt * nt * nt;
-    k_deposit<R, KIND, USE_PHI><<<grid, DEP_NT, smem, st>>>(p, bstart, N, nt, phi, out, a, m00, mij, accumulate,
+    k_deposit<R, KIND, USE_PHI><<<grid, DEP_NT, smem, st>>>(p, bstart, N, nt, phi, out, a, m00, mij, accumulate, err,
                                                                       FastDiv((uint32_t)N));
 }
 
 template <class R>
 void launch_deposit(int kind, bool use_phi, const PView<R> &p, const uint32_t *bstart, int N, const R *phi,
-                    const DepOut<R> &out, double a, double m00, double mij, int accumulate, cudaStream_t st)
+                    const DepOut<R> &out, double a, double m00, double mij, int accumulate, int *err, cudaStream_t st)
 {
-#define GEV_DEP(K)                                                                          \
-    if (kind == K) {                                                                        \
-        if (use_phi) launch_k<R, K, true>(p, bstart, N, phi, out, a, m00, mij, accumulate, st);  \
-        else launch_k<R, K, false>(p, bstart, N, phi, out, a, m00, mij, accumulate, st);         \
+#define GEV_DEP(K)                                                                                    \
+    if (kind == K) {                                                                                  \
+        if (use_phi) launch_k<R, K, true>(p, bstart, N, phi, out, a, m00, mij, accumulate, err, st);  \
+        else launch_k<R, K, false>(p, bstart, N, phi, out, a, m00, mij, accumulate, err, st);         \
         return;                                                                             \
     }
     GEV_DEP(DEP_T00)
@@ -590,8 +569,8 @@ void launch_deposit(int kind, bool use_phi, const PView<R> &p, const uint32_t *b
 }
 
 template void launch_deposit<float>(int, bool, const PView<float> &, const uint32_t *, int, const float *,
-                                    const DepOut<float> &, double, double, double, int, cudaStream_t);
+                                    const DepOut<float> &, double, double, double, int, int *, cudaStream_t);
 template void launch_deposit<double>(int, bool, const PView<double> &, const uint32_t *, int, const double *,
-                                     const DepOut<double> &, double, double, double, int, cudaStream_t);
+                                     const DepOut<double> &, double, double, double, int, int *, cudaStream_t);
 
 }  // namespace gev

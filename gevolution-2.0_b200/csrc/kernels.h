@@ -16,7 +16,7 @@ template <class R> struct DepOut { R *p[7]; };
 
 template <class R>
 void launch_deposit(int kind, bool use_phi, const PView<R> &p, const uint32_t *bstart, int N, const R *phi,
-                    const DepOut<R> &out, double a, double m00, double mij, int accumulate, cudaStream_t st);
+                    const DepOut<R> &out, double a, double m00, double mij, int accumulate, int *err, cudaStream_t st);
 
 // ---- particles ----
 struct KickDriftParams {
@@ -42,8 +42,8 @@ template <class R>
 void launch_bin_count(const PView<R> &p, int N, uint32_t *counts, uint32_t *bucket, uint32_t *rank, cudaStream_t st);
 void launch_scan(const uint32_t *counts, uint32_t *start, int64_t nb, uint32_t *block_sums, cudaStream_t st);
 template <class R>
-void launch_scatter(const PView<R> &src, PView<R> dst, const uint32_t *bstart, const uint32_t *bucket,
-                    const uint32_t *rank, cudaStream_t st);
+void launch_rebin(const PView<R> &src, PView<R> dst, const uint32_t *bstart, const uint32_t *bucket,
+                  const uint32_t *rank, uint32_t *inv, int N, int *err, cudaStream_t st);
 
 void launch_reduce_sum(const double *partial, int64_t n, double *out, cudaStream_t st);
 

@@ -2,9 +2,11 @@
 // kick/drift and lightcone kernels.
 //
 // Particles are structure-of-arrays, ordered by bucket = 8*tile + class (tiles
-// of 8^3 cells; the class bits mark the tile's upper faces x,y,z == 7).  Order
-// inside a bucket is not significant: every consumer is order-independent
-// (fixed-point deposits, per-particle updates, max reductions).
+// of 8^3 cells; the class bits mark the tile's upper faces x,y,z == 7).  Inside
+// every bucket of at most REBIN_SORT_MAX particles the order is (cell, particle
+// ID), so the records of one cell are contiguous and the deposits sum them in a
+// fixed order; larger buckets keep an arbitrary order and are only ever read by
+// the deposits' fixed-point path, whose sums do not depend on it.
 //   cell  : uint32 linear cell index x + N*(y + N*z)
 //   off   : 3 planes of FP64 offsets inside the cell, in cell units, [0,1)
 //   q     : 3 planes of momenta per unit mass (R = float in mixed mode)
@@ -24,9 +26,26 @@ template <class R> struct PView {
     int64_t n;
 };
 
-struct Buckets {
-    const uint32_t *start;   // nb + 1 entries (exclusive scan of counts)
-};
+// buckets up to this many particles are kept in (cell, ID) order; at least the
+// largest single-chunk deposit (1024 records)
+constexpr int REBIN_SORT_MAX = 1024;
+
+// Rank of the tile-local cell (lx, ly, lz) in class-major order: the cells of
+// class 0 (343 of them), then class 1 (49), ..., class 7 (1), each class in
+// (z, y, x) lexicographic order -- so sorting a tile by this rank sorts it by
+// bucket and, inside every bucket, by cell index.
+__host__ __device__ __forceinline__ int class_ord(int lx, int ly, int lz)
+{
+    const bool fx = lx == 7, fy = ly == 7, fz = lz == 7;
+    const int cls = (fx ? 1 : 0) | (fy ? 2 : 0) | (fz ? 4 : 0);
+    // first rank of each class: 0, 343, 343+49, ... (class sizes 343, 49, 49, 7, 49, 7, 7, 1)
+    const int first = cls == 0 ? 0 : cls == 1 ? 343 : cls == 2 ? 392 : cls == 3 ? 441 : cls == 4 ? 448 : cls == 5 ? 497 : cls == 6 ? 504 : 511;
+    int r = 0, mul = 1;
+    if (!fx) { r += lx * mul; mul *= 7; }
+    if (!fy) { r += ly * mul; mul *= 7; }
+    if (!fz) r += lz * mul;
+    return first + r;
+}
 
 // Particle ranges a tile's deposit needs: its own 8 class buckets and, from
 // each of the 7 lower neighbour tiles, the classes whose cells lie on the

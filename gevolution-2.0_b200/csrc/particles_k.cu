@@ -7,9 +7,10 @@
 // reach ([-1, 10)^3 relative to the tile origin) in shared memory, so every
 // gather is a shared-memory read.  The drift moves the cell index and the FP64
 // in-cell offset and assigns the particle its new bucket; a warp-aggregated
-// counter gives it a slot, and launch_scatter moves it into bucket order after
-// an exclusive scan of the bucket counts (the re-binning that LATfield2's
-// moveParticles does into its row buffers).
+// counter gives it a slot, and launch_rebin moves it into bucket order -- and
+// inside each bucket into (cell, ID) order -- after an exclusive scan of the
+// bucket counts (the re-binning that LATfield2's moveParticles does into its
+// row buffers).
 #include "common.cuh"
 #include "kernels.h"
 #include "particles.cuh"
@@ -423,27 +424,178 @@ void launch_scan(const uint32_t *counts, uint32_t *start, int64_t nb, uint32_t *
     k_scan_add<<<(unsigned)nblk, SCAN_NT, 0, st>>>(start, nb, block_sums);
 }
 
-template <class R>
-__global__ void k_scatter(PView<R> src, PView<R> dst, const uint32_t *bstart, const uint32_t *bucket, const uint32_t *rank)
+// ---- re-binning into bucket order, each bucket in (cell, ID) order ----
+// Step 1: every particle's destination j = start[bucket] + slot; inv[j] = i.
+__global__ void k_scatter_index(const uint32_t *__restrict__ bstart, const uint32_t *__restrict__ bucket,
+                                const uint32_t *__restrict__ rank, int64_t n, uint32_t *inv)
 {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= src.n) return;
-    uint32_t j = bstart[bucket[i]] + rank[i];
-    if ((int64_t)j >= src.n) return;   // inconsistent counts: never write out of range
-    dst.cell[j] = src.cell[i];
+    if (i >= n) return;
+    const uint32_t j = bstart[bucket[i]] + rank[i];
+    if ((int64_t)j < n) inv[j] = (uint32_t)i;   // inconsistent counts: never write out of range
+}
+
+constexpr int RB_NT = 512;   // one thread per tile cell in the counting sort
+
+template <class R> constexpr size_t rb_smem_bytes()
+{
+    // per particle: id, off[3], q[3], cell, source index, cell rank, slot, sorted index
+    return (size_t)REBIN_SORT_MAX * (sizeof(int64_t) + 3 * sizeof(double) + 3 * sizeof(R) + sizeof(uint32_t) + 3 * sizeof(uint16_t));
+}
+
+// Step 2: one CTA per destination tile.  The tile's particles (or, for a tile
+// of more than REBIN_SORT_MAX, each of its buckets that small) are loaded once
+// from their source positions into shared memory, sorted there -- counting
+// sort by class_ord of the cell, then insertion sort by ID inside each cell --
+// and written to the sorted destination positions (coalesced writes).  A
+// bucket larger than REBIN_SORT_MAX is copied in slot order.
+template <class R>
+__global__ void __launch_bounds__(RB_NT) k_rebin_tile(PView<R> src, PView<R> dst, const uint32_t *__restrict__ bstart,
+                                                      const uint32_t *__restrict__ inv, int nt, int *err, FastDiv fN)
+{
+    constexpr int M = REBIN_SORT_MAX;
+    extern __shared__ __align__(16) unsigned char rb_smem[];
+    int64_t *s_id = reinterpret_cast<int64_t *>(rb_smem);
+    double *s_off = reinterpret_cast<double *>(s_id + M);          // 3 planes of M
+    R *s_q = reinterpret_cast<R *>(s_off + 3 * M);                 // 3 planes of M
+    uint32_t *s_cell = reinterpret_cast<uint32_t *>(s_q + 3 * M);
+    uint16_t *s_ord = reinterpret_cast<uint16_t *>(s_cell + M);
+    uint16_t *s_slot = s_ord + M;
+    uint16_t *s_order = s_slot + M;
+    __shared__ int s_cnt[512], s_start[512], s_wsum[RB_NT / 32];
+
+    const int t = threadIdx.x, tile = blockIdx.x;
+    const int x0 = 8 * (tile % nt), y0 = 8 * ((tile / nt) % nt), z0 = 8 * (tile / (nt * nt));
+
+    // source index of destination position pos (never past the particle count)
+    auto source = [&](uint32_t pos) -> uint32_t {
+        uint32_t s = inv[pos];
+        if ((int64_t)s >= src.n) { atomicOr(err, ERR_BAD_CELL); s = 0; }
+        return s;
+    };
+
+    auto sort_range = [&](uint32_t lo, int m) {
+        for (int c = t; c < 512; c += RB_NT) s_cnt[c] = 0;
+        __syncthreads();
+        for (int j = t; j < m; j += RB_NT) {
+            const uint32_t s = source(lo + (uint32_t)j);
+            const uint32_t cell = src.cell[s];
+            const int64_t id = src.id[s];
+            double o[3];
+            R q[3];
 #pragma unroll
-    for (int k = 0; k < 3; k++) {
-        dst.off[k * dst.cap + j] = src.off[k * src.cap + i];
-        dst.q[k * dst.cap + j] = src.q[k * src.cap + i];
+            for (int k = 0; k < 3; k++) {
+                o[k] = src.off[k * src.cap + s];
+                q[k] = src.q[k * src.cap + s];
+            }
+            int cx, cy, cz;
+            decode_cell(cell, fN, cx, cy, cz);
+            int lx = cx - x0, ly = cy - y0, lz = cz - z0;
+            if (lx < 0 || lx > 7 || ly < 0 || ly > 7 || lz < 0 || lz > 7) { atomicOr(err, ERR_BAD_CELL); lx = ly = lz = 0; }
+            const int c = class_ord(lx, ly, lz);
+            s_cell[j] = cell;
+            s_id[j] = id;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                s_off[k * M + j] = o[k];
+                s_q[k * M + j] = q[k];
+            }
+            s_ord[j] = (uint16_t)c;
+            s_slot[j] = (uint16_t)atomicAdd(&s_cnt[c], 1);
+        }
+        __syncthreads();
+        {   // exclusive scan of the 512 cell counts, one per thread
+            const int v = s_cnt[t];
+            int incl = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, incl, o);
+                if ((t & 31) >= o) incl += u;
+            }
+            if ((t & 31) == 31) s_wsum[t >> 5] = incl;
+            __syncthreads();
+            if (t < 32) {
+                const int w = t < RB_NT / 32 ? s_wsum[t] : 0;
+                int wi = w;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int u = __shfl_up_sync(0xffffffffu, wi, o);
+                    if (t >= o) wi += u;
+                }
+                if (t < RB_NT / 32) s_wsum[t] = wi - w;
+            }
+            __syncthreads();
+            s_start[t] = incl - v + s_wsum[t >> 5];
+        }
+        __syncthreads();
+        for (int j = t; j < m; j += RB_NT) s_order[s_start[s_ord[j]] + s_slot[j]] = (uint16_t)j;
+        __syncthreads();
+        {   // insertion sort by ID inside the cell (cells hold a few particles)
+            const int k0 = s_start[t], mc = s_cnt[t];
+            for (int a1 = 1; a1 < mc; a1++) {
+                const uint16_t key = s_order[k0 + a1];
+                const int64_t kid = s_id[key];
+                int b1 = a1 - 1;
+                while (b1 >= 0 && s_id[s_order[k0 + b1]] > kid) {
+                    s_order[k0 + b1 + 1] = s_order[k0 + b1];
+                    b1--;
+                }
+                s_order[k0 + b1 + 1] = key;
+            }
+        }
+        __syncthreads();
+        for (int k = t; k < m; k += RB_NT) {
+            const int j = s_order[k];
+            const uint32_t i = lo + (uint32_t)k;
+            dst.cell[i] = s_cell[j];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                dst.off[c * dst.cap + i] = s_off[c * M + j];
+                dst.q[c * dst.cap + i] = s_q[c * M + j];
+            }
+            dst.id[i] = s_id[j];
+        }
+        __syncthreads();
+    };
+
+    const uint32_t b0 = bstart[8 * tile], b8 = bstart[8 * tile + 8];
+    if (b8 - b0 <= (uint32_t)M) {
+        if (b8 > b0) sort_range(b0, (int)(b8 - b0));
+        return;
     }
-    dst.id[j] = src.id[i];
+    for (int c = 0; c < 8; c++) {
+        const uint32_t lo = bstart[8 * tile + c], hi = bstart[8 * tile + c + 1];
+        if (hi - lo <= (uint32_t)M) {
+            if (hi > lo) sort_range(lo, (int)(hi - lo));
+        } else {
+            for (uint32_t i = lo + (uint32_t)t; i < hi; i += RB_NT) {
+                const uint32_t s = source(i);
+                dst.cell[i] = src.cell[s];
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    dst.off[k * dst.cap + i] = src.off[k * src.cap + s];
+                    dst.q[k * dst.cap + i] = src.q[k * src.cap + s];
+                }
+                dst.id[i] = src.id[s];
+            }
+        }
+    }
 }
 
 template <class R>
-void launch_scatter(const PView<R> &src, PView<R> dst, const uint32_t *bstart, const uint32_t *bucket,
-                    const uint32_t *rank, cudaStream_t st)
+void launch_rebin(const PView<R> &src, PView<R> dst, const uint32_t *bstart, const uint32_t *bucket,
+                  const uint32_t *rank, uint32_t *inv, int N, int *err, cudaStream_t st)
 {
-    if (src.n > 0) k_scatter<R><<<cdiv(src.n, 256), 256, 0, st>>>(src, dst, bstart, bucket, rank);
+    if (src.n <= 0) return;
+    k_scatter_index<<<cdiv(src.n, 256), 256, 0, st>>>(bstart, bucket, rank, src.n, inv);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_rebin_tile<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rb_smem_bytes<R>());
+        attr_set = true;
+    }
+    const int nt = N / 8;
+    k_rebin_tile<R><<<(unsigned)nt * nt * nt, RB_NT, rb_smem_bytes<R>(), st>>>(src, dst, bstart, inv, nt, err,
+                                                                    FastDiv((uint32_t)N));
 }
 
 // deterministic sum of per-block partials (fixed order)
@@ -475,8 +627,8 @@ void launch_reduce_sum(const double *partial, int64_t n, double *out, cudaStream
     template void launch_store_particles<R>(const PView<R> &, double *, double *, int64_t *, int64_t, int,           \
                                             cudaStream_t);                                                            \
     template void launch_bin_count<R>(const PView<R> &, int, uint32_t *, uint32_t *, uint32_t *, cudaStream_t);       \
-    template void launch_scatter<R>(const PView<R> &, PView<R>, const uint32_t *, const uint32_t *, const uint32_t *, \
-                                    cudaStream_t);
+    template void launch_rebin<R>(const PView<R> &, PView<R>, const uint32_t *, const uint32_t *, const uint32_t *,   \
+                                  uint32_t *, int, int *, cudaStream_t);
 GEV_INST(float)
 GEV_INST(double)
 #undef GEV_INST
