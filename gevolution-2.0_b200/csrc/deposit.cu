@@ -272,12 +272,11 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
     const int x0 = tx * 8, y0 = ty * 8, z0 = tz * 8;
 
     const R ra = (R)a, rm00 = (R)m00, rmij = (R)mij;
-    tile_segments_block(bstart, nt, tx, ty, tz, seg_lo, seg_hi, seg_pre);
-    if (t < NC) vmax[t] = 0ull;
-    for (int c = t; c < 730; c += DEP_NT) { cstart[c] = 0; ccount[c] = 0; }
+    // the phi stencil loads go out first and stay in flight while the bucket
+    // ranges are looked up
+    constexpr int PER = (1000 + DEP_NT - 1) / DEP_NT;
+    R pv[PER];
     if (USE_PHI) {
-        constexpr int PER = (1000 + DEP_NT - 1) / DEP_NT;
-        R pv[PER];
 #pragma unroll
         for (int k = 0; k < PER; k++) {
             int s = t + k * DEP_NT;
@@ -286,6 +285,21 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
                 pv[k] = __ldg(phi + sidx(N, wrapi(x0 + vx, N), wrapi(y0 + vy, N), wrapi(z0 + vz, N)));
             }
         }
+    }
+    // the tile's own particles (candidates 0..7: one contiguous range at the
+    // head of the concatenation) are loaded as well, for the single-chunk path
+    constexpr int PP = (CH + DEP_NT - 1) / DEP_NT;   // at most two particles per thread
+    RawParticle<R> raw[PP];
+    const uint32_t own_lo = bstart[8 * tile], own_n = bstart[8 * tile + 8] - own_lo;
+#pragma unroll
+    for (int u = 0; u < PP; u++) {
+        const int j = t + u * DEP_NT;
+        if ((uint32_t)j < own_n) raw[u] = load_particle(p, own_lo + (uint32_t)j);
+    }
+    tile_segments_block(bstart, nt, tx, ty, tz, seg_lo, seg_hi, seg_pre);
+    if (t < NC) vmax[t] = 0ull;
+    for (int c = t; c < 730; c += DEP_NT) { cstart[c] = 0; ccount[c] = 0; }
+    if (USE_PHI) {
 #pragma unroll
         for (int k = 0; k < PER; k++) {
             int s = t + k * DEP_NT;
@@ -354,13 +368,11 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
         // order (source cell, then ID) -- independent of the order in which
         // the particles were given.
         const int n = (int)total;
-        // at most two particles per thread (n <= CH <= 2 DEP_NT), loads issued together
-        constexpr int PP = (CH + DEP_NT - 1) / DEP_NT;
-        RawParticle<R> raw[PP];
+        // the neighbours' particles (the own ones are loaded already)
 #pragma unroll
         for (int u = 0; u < PP; u++) {
             const int j = t + u * DEP_NT;
-            if (j < n) raw[u] = load_particle(p, seg_index(seg_lo, seg_pre, (uint32_t)j));
+            if (j < n && (uint32_t)j >= own_n) raw[u] = load_particle(p, seg_find(seg_lo, seg_pre, (uint32_t)j));
         }
         // 1. record j at position j, and the reach cell it came from
 #pragma unroll
