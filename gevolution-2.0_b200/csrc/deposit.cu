@@ -218,19 +218,47 @@ __device__ __forceinline__ void gather_sum(const R *r, int bx, int by, int bz, R
     }
 }
 
-template <class R, int NFP> __device__ __forceinline__ void load_record(const R *src, R (&dst)[NFP])
+// Records in shared memory: record k is C = NFP / L chunks of 16 bytes (L
+// values of R each), stored whole with 16-byte accesses.  With an even chunk
+// count the two halves of each chunk pair swap places in records 4..7 mod 8,
+// so the same chunk of 8 consecutive records falls in 8 different 4-bank
+// groups (a quarter warp of 16-byte accesses without bank conflicts); an odd
+// count (the 12-value T00+Tij record in FP32) spreads them by itself.
+template <class R, int NFP> struct RecLayout {
+    static constexpr int L = 16 / (int)sizeof(R);
+    static constexpr int C = NFP / L;
+    static_assert(NFP % L == 0, "records are whole 16-byte chunks");
+    __device__ __forceinline__ static int chunk(int k, int m) { return k * C + ((C % 2 == 0) ? (m ^ ((k >> 2) & 1)) : m); }
+};
+
+template <class R, int NFP, int NF>
+__device__ __forceinline__ void store_record(R *rec, int k, const R (&v)[NF])
 {
-    if constexpr (sizeof(R) == 4) {
+    using Lay = RecLayout<R, NFP>;
 #pragma unroll
-        for (int k = 0; k < NFP; k += 4) {
-            float4 t = *reinterpret_cast<const float4 *>(src + k);
-            dst[k] = t.x; dst[k + 1] = t.y; dst[k + 2] = t.z; dst[k + 3] = t.w;
+    for (int m = 0; m < Lay::C; m++) {
+        R *dst = rec + (size_t)Lay::chunk(k, m) * Lay::L;
+        auto val = [&](int f) { return f < NF ? v[f] : (R)0; };
+        if constexpr (sizeof(R) == 4) {
+            *reinterpret_cast<float4 *>(dst) = make_float4(val(4 * m), val(4 * m + 1), val(4 * m + 2), val(4 * m + 3));
+        } else {
+            *reinterpret_cast<double2 *>(dst) = make_double2(val(2 * m), val(2 * m + 1));
         }
-    } else {
+    }
+}
+
+template <class R, int NFP> __device__ __forceinline__ void load_record(const R *rec, int k, R (&dst)[NFP])
+{
+    using Lay = RecLayout<R, NFP>;
 #pragma unroll
-        for (int k = 0; k < NFP; k += 2) {
-            double2 t = *reinterpret_cast<const double2 *>(src + k);
-            dst[k] = t.x; dst[k + 1] = t.y;
+    for (int m = 0; m < Lay::C; m++) {
+        const R *src = rec + (size_t)Lay::chunk(k, m) * Lay::L;
+        if constexpr (sizeof(R) == 4) {
+            const float4 t = *reinterpret_cast<const float4 *>(src);
+            dst[4 * m] = t.x; dst[4 * m + 1] = t.y; dst[4 * m + 2] = t.z; dst[4 * m + 3] = t.w;
+        } else {
+            const double2 t = *reinterpret_cast<const double2 *>(src);
+            dst[2 * m] = t.x; dst[2 * m + 1] = t.y;
         }
     }
 }
@@ -382,9 +410,7 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
             R v[NF], b[NC];
             int lc;
             if (make_record<R, KIND, USE_PHI>(raw[u], N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
-                R *dst = rec + (size_t)j * NFP;
-#pragma unroll
-                for (int k = 0; k < NF; k++) dst[k] = v[k];
+                store_record<R, NFP>(rec, j, v);
                 rcell[j] = (uint16_t)lc;
             } else {
                 rcell[j] = DEP_SKIP;
@@ -430,7 +456,7 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
             const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
             for (int k = kb0[b]; k < kb1[b]; k++) {
                 R r[NFP];
-                load_record<R, NFP>(rec + (size_t)k * NFP, r);
+                load_record<R, NFP>(rec, k, r);
                 gather_sum<R, KIND, USE_PHI>(r, bx, by, bz, phv, phx, phy, phz, acc);
             }
         }
@@ -482,6 +508,7 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
         reduce_bounds(lb);
         __syncthreads();
         set_scales();
+        __syncthreads();   // every record of the first chunk takes the scales
     }
 
     long long acc[NC];
@@ -497,9 +524,8 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
                 R v[NF], b[NC];
                 int lc;
                 if (make_record<R, KIND, USE_PHI>(load_particle(p, i), N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
-                    R *dst = rec + (size_t)j * NFP;
-#pragma unroll
-                    for (int k = 0; k < NF; k++) dst[k] = v[k];
+                    scale_record<R, KIND>(v, scl_s);   // fixed-point scales of the components (weights unscaled)
+                    store_record<R, NFP>(rec, j, v);
                     rcell[j] = (uint16_t)lc;
                     rslot[j] = (uint16_t)atomicAdd(&ccount[lc], 1);
                 } else {
@@ -511,13 +537,10 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
         // 2. exclusive scan of the 729 cell counts
         scan_cells();
         __syncthreads();
-        // 3. counting sort of record indexes by cell; records take their fixed-point scales
+        // 3. counting sort of record indexes by cell
         for (int j = t; j < n; j += DEP_NT) {
             const uint16_t lc = rcell[j];
-            if (lc != DEP_SKIP) {
-                order[cstart[lc] + rslot[j]] = (uint16_t)j;
-                scale_record<R, KIND>(rec + (size_t)j * NFP, scl_s);
-            }
+            if (lc != DEP_SKIP) order[cstart[lc] + rslot[j]] = (uint16_t)j;
         }
         __syncthreads();
         // 4. gather: the vertex receives from the cells v - b, b in {0,1}^3
@@ -528,7 +551,7 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
             const int k0 = cstart[lc], k1 = k0 + ccount[lc];
             for (int k = k0; k < k1; k++) {
                 R r[NFP];
-                load_record<R, NFP>(rec + (size_t)order[k] * NFP, r);
+                load_record<R, NFP>(rec, order[k], r);
                 gather_one<R, KIND, USE_PHI>(r, bx, by, bz, phv, phx, phy, phz, acc);
             }
         }
