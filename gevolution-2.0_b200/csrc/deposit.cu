@@ -35,6 +35,12 @@
 namespace gev {
 
 constexpr int DEP_NT = 512;   // one thread per tile vertex
+#ifndef GEV_DEP_MINB_F
+#define GEV_DEP_MINB_F 3
+#endif
+#ifndef GEV_DEP_MINB_T0I_F
+#define GEV_DEP_MINB_T0I_F 4
+#endif
 
 template <class R> struct DepCh;
 template <> struct DepCh<float> { static constexpr int v = 1024; static constexpr int EMAX = 120; };
@@ -270,9 +276,17 @@ __host__ __device__ constexpr size_t dep_smem_bytes()
            (size_t)3 * DepCh<R>::v * sizeof(uint16_t);
 }
 
+// Resident CTAs per SM the register budget is sized for.  The kernel is bound
+// by the latency of its dependent phases, so FP32 trades a few spilled
+// registers for more resident CTAs: three for the T00/Tij records (40
+// registers; their shared memory fits no fourth), four for the smaller T0i
+// records (32 registers).  FP64 records fill the shared memory of two CTAs.
+template <class R, int KIND> struct DepMinBlocks { static constexpr int v = sizeof(R) == 4 ? GEV_DEP_MINB_F : 2; };
+template <> struct DepMinBlocks<float, DEP_T0I> { static constexpr int v = GEV_DEP_MINB_T0I_F; };
+
 // outputs: component c is written to out[c] (N^3 plane each)
 template <class R, int KIND, bool USE_PHI>
-__global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt,
+__global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v) k_deposit(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt,
                                                        const R *__restrict__ phi, DepOut<R> out, double a, double m00,
                                                        double mij, int accumulate, int *err, FastDiv fN)
 {
@@ -439,22 +453,17 @@ __global__ void __launch_bounds__(DEP_NT, 2) k_deposit(PView<R> p, const uint32_
             }
             if (bad) atomicOr(err, ERR_BAD_ORDER);
         }
-        // 5. gather: the 8 source-cell ranges first, then the contiguous records
-        int kb0[8], kb1[8];
-#pragma unroll
-        for (int b = 0; b < 8; b++) {
-            const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
-            const int lc = (vx - bx + 1) + 9 * ((vy - by + 1) + 9 * (vz - bz + 1));
-            kb0[b] = cstart[lc];
-            kb1[b] = cend[lc];
-        }
+        // 5. gather: the vertex receives from the cells v - b, b in {0,1}^3
         R acc[NC];
 #pragma unroll
         for (int c = 0; c < NC; c++) acc[c] = 0;
+        const int lc0 = (vx + 1) + 9 * ((vy + 1) + 9 * (vz + 1));
 #pragma unroll
         for (int b = 0; b < 8; b++) {
             const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
-            for (int k = kb0[b]; k < kb1[b]; k++) {
+            const int lc = lc0 - bx - 9 * by - 81 * bz;
+            const int k1 = cend[lc];
+            for (int k = cstart[lc]; k < k1; k++) {
                 R r[NFP];
                 load_record<R, NFP>(rec, k, r);
                 gather_sum<R, KIND, USE_PHI>(r, bx, by, bz, phv, phx, phy, phz, acc);
