@@ -141,7 +141,7 @@ constexpr int LC_NT = 256;
 // kept images (margin far above the FP32 rounding of |x - V|^2, |x - V| < 4
 // box lengths) and the exact FP64 test of the reference only near the shell.
 template <class R>
-__global__ void __launch_bounds__(LC_NT) k_lightcone(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt,
+__global__ void __launch_bounds__(LC_NT, 4) k_lightcone(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt,
                                                      const R *__restrict__ phi, const __grid_constant__ LcKernelArgs la,
                                                      float *opos,
                                                      float *ovel, int64_t *oid, unsigned long long *count,

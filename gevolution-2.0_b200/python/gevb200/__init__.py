@@ -154,10 +154,11 @@ class Context:
             raise GevError(rc, _last_error(None).decode())
         self._h = h
         self.cfg = cfg
+        self._destroy = _destroy   # held by the object: module globals may be gone when it is collected at exit
 
     def close(self):
         if getattr(self, "_h", None):
-            _destroy(self._h)
+            self._destroy(self._h)
             self._h = None
 
     def __del__(self):

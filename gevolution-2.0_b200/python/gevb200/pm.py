@@ -63,10 +63,11 @@ class PM:
         if rc != 0:
             raise GevError(rc, _err(None).decode())
         self._h = h
+        self._destroy = _destroy   # held by the object: module globals may be gone when it is collected at exit
 
     def close(self):
         if getattr(self, "_h", None):
-            _destroy(self._h)
+            self._destroy(self._h)
             self._h = None
 
     def __del__(self):
