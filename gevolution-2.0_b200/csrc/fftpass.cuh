@@ -19,10 +19,23 @@ namespace gev {
 
 // occupancy the z pass and the six-component x pass are compiled for
 #ifndef GEV_FZ_MINB
-#define GEV_FZ_MINB 3   // resident CTAs of 256 threads per SM
+#define GEV_FZ_MINB 4   // resident CTAs of 256 threads per SM (FP32)
+#endif
+#ifndef GEV_FZ_MINB_D
+#define GEV_FZ_MINB_D 3   // the same for FP64
 #endif
 #ifndef GEV_TIJ6_MINB
 #define GEV_TIJ6_MINB 3
+#endif
+// resident CTAs per SM of the FP32 x passes (256 threads) and of the FP32 bulk-copy y pass (512 threads)
+#ifndef GEV_FX_MINB
+#define GEV_FX_MINB 4
+#endif
+#ifndef GEV_FXI_MINB
+#define GEV_FXI_MINB 4
+#endif
+#ifndef GEV_FY_MINB
+#define GEV_FY_MINB 2
 #endif
 
 // ---------------------------------------------------------------------------
@@ -125,7 +138,7 @@ __device__ __forceinline__ R prep_tij(const R *T, const R *phi, R coeff, int c, 
 // x pass, forward: real rows -> half spectrum.  grid (N/T, N, ncomp)
 // ---------------------------------------------------------------------------
 template <class R, int N, int T, int NT, int MODE>
-__global__ void __launch_bounds__(NT) k_fx_fwd(FxArgs<R> a, int64_t in_stride, int64_t out_stride,
+__global__ void __launch_bounds__(NT, sizeof(R) == 4 ? GEV_FX_MINB : 1) k_fx_fwd(FxArgs<R> a, int64_t in_stride, int64_t out_stride,
                                                const typename CT<R>::C *__restrict__ tw_half,
                                                const typename CT<R>::C *__restrict__ tw_full)
 {
@@ -296,7 +309,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_fy(typename CT<R>::C *data, i
 // and kx = N/2 entries do not contribute).  grid (N/T, N, ncomp)
 // ---------------------------------------------------------------------------
 template <class R, int N, int T, int NT>
-__global__ void __launch_bounds__(NT) k_fx_inv(const typename CT<R>::C *in, int64_t in_stride, R *out,
+__global__ void __launch_bounds__(NT, sizeof(R) == 4 ? GEV_FXI_MINB : 1) k_fx_inv(const typename CT<R>::C *in, int64_t in_stride, R *out,
                                                int64_t out_stride,
                                                const typename CT<R>::C *__restrict__ tw_half,
                                                const typename CT<R>::C *__restrict__ tw_full)
@@ -678,12 +691,14 @@ template <int N> struct ZBox {
 
 // the tensor extras keep six components in registers through the solve:
 // compiled for one resident CTA instead of GEV_FZ_MINB
-template <int OP, int EXTRA, int NT> struct FzMinBlocks {
-    static constexpr int v = (OpShape<OP, EXTRA>::CIN == 6 && !OpShape<OP, EXTRA>::CONTRACT) ? 1 : GEV_FZ_MINB * 256 / NT;
+template <class R, int OP, int EXTRA, int NT> struct FzMinBlocks {
+    static constexpr int v = (OpShape<OP, EXTRA>::CIN == 6 && !OpShape<OP, EXTRA>::CONTRACT)
+                                 ? 1
+                                 : (sizeof(R) == 4 ? GEV_FZ_MINB : GEV_FZ_MINB_D) * 256 / NT;
 };
 
 template <class R, int N, int T, int NT, int OP, int EXTRA>
-__global__ void __launch_bounds__(NT, (FzMinBlocks<OP, EXTRA, NT>::v))
+__global__ void __launch_bounds__(NT, (FzMinBlocks<R, OP, EXTRA, NT>::v))
     k_fz_tma(FzArgs<R> a, const typename CT<R>::C *__restrict__ tw, const __grid_constant__ CUtensorMap tmap)
 {
     using C = typename CT<R>::C;
@@ -782,7 +797,7 @@ __global__ void __launch_bounds__(NT, (FzMinBlocks<OP, EXTRA, NT>::v))
 // y pass with bulk-tensor-copy staging: T kx-columns over all ky at one kz,
 // in place.  grid (ceil(P/T), N, ncomp)
 template <class R, int N, int T, int NT, int S>
-__global__ void __launch_bounds__(NT, 1024 / NT) k_fy_tma(const typename CT<R>::C *__restrict__ tw,
+__global__ void __launch_bounds__(NT, (sizeof(R) == 4 ? GEV_FY_MINB : 2) * 512 / NT) k_fy_tma(const typename CT<R>::C *__restrict__ tw,
                                                         const __grid_constant__ CUtensorMap tmap)
 {
     using C = typename CT<R>::C;
