@@ -201,21 +201,13 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 4 ? GEV_FX_MINB : 1) k_fx_fwd
 }
 
 // prepareFTsource_Tij for all six components at one point from the ten
-// potential values they share; the arithmetic of each component is that of
-// prep_tij (same expressions, same order), so the results are identical.
+// potential values they share (p0 = phi(x), pxp = phi(x + e_x), ..., pxy =
+// phi(x + e_x + e_y)); the arithmetic of each component is that of prep_tij
+// (same expressions, same order), so the results are identical.
 template <class R>
-__device__ __forceinline__ void prep_tij6(const R *T, int64_t n3, const R *phi, R coeff, int N, int x, int y, int z,
-                                          R o[6])
+__device__ __forceinline__ void tij6_point(R p0, R pxp, R pxm, R pyp, R pym, R pzp, R pzm, R pxy, R pxz, R pyz,
+                                           const R t[6], R coeff, R o[6])
 {
-    const int64_t i = sidx(N, x, y, z);
-    const R p0 = __ldg(phi + i);
-    const R pxp = ldr(phi, N, x + 1, y, z), pxm = ldr(phi, N, x - 1, y, z);
-    const R pyp = ldr(phi, N, x, y + 1, z), pym = ldr(phi, N, x, y - 1, z);
-    const R pzp = ldr(phi, N, x, y, z + 1), pzm = ldr(phi, N, x, y, z - 1);
-    const R pxy = ldr(phi, N, x + 1, y + 1, z), pxz = ldr(phi, N, x + 1, y, z + 1), pyz = ldr(phi, N, x, y + 1, z + 1);
-    R t[6];
-#pragma unroll
-    for (int c = 0; c < 6; c++) t[c] = __ldg(T + c * n3 + i);
     R g;
     g = pxp - pxm; o[0] = (R)0.5 * g * g + coeff * t[0];
     g = pyp - pym; o[3] = (R)0.5 * g * g + coeff * t[3];
@@ -229,6 +221,12 @@ __device__ __forceinline__ void prep_tij6(const R *T, int64_t n3, const R *phi, 
     o[4] = (R)2 * u * v + w * (u + v + (R)0.5 * w) + coeff * t[4];
 }
 
+// two adjacent values (x even: 8- or 16-byte aligned) in one load
+template <class R> __device__ __forceinline__ typename CT<R>::C ld_pair(const R *p)
+{
+    return __ldg(reinterpret_cast<const typename CT<R>::C *>(p));
+}
+
 // x pass, forward, for the six Tij components at once: each potential value
 // is loaded once for all six sources.  grid (N/T, N)
 template <class R, int N, int T, int NT>
@@ -238,18 +236,38 @@ __global__ void __launch_bounds__(NT, GEV_TIJ6_MINB) k_fx_fwd_tij6(const R *__re
                                                     const typename CT<R>::C *__restrict__ tw_full)
 {
     using C = typename CT<R>::C;
-    constexpr int M = N / 2, P = N / 2 + 1, PP = N / 2 + 2, LD = T + 1, CS = M * LD;
+    // the six components' rows side by side: 6T lines of one batched transform,
+    // element n of line c*T + t at buf[n*LD + c*T + t]
+    constexpr int M = N / 2, P = N / 2 + 1, PP = N / 2 + 2, T6 = 6 * T, LD = T6 + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *buf = reinterpret_cast<C *>(smem_raw);   // 6 component buffers of CS
+    C *buf = reinterpret_cast<C *>(smem_raw);
     const int y0 = blockIdx.x * T, z = blockIdx.y;
     const R rc = (R)coeff;
     struct Six { C v[6]; };
     staged_fill<M * T, NT, 2, Six>(
         [&](int idx) {
+            // the points x0 = 2n and x0 + 1 of row (y, z): the potential rows
+            // they touch are read as aligned pairs plus the four values beyond
             const int n = idx % M, t = idx / M, y = y0 + t;
+            const int x0 = 2 * n, xm = x0 == 0 ? N - 1 : x0 - 1, x2 = x0 + 2 == N ? 0 : x0 + 2;
+            const int ym = y == 0 ? N - 1 : y - 1, yp = y == N - 1 ? 0 : y + 1;
+            const int zm = z == 0 ? N - 1 : z - 1, zp = z == N - 1 ? 0 : z + 1;
+            const R *r00 = phi + sidx(N, 0, y, z), *rm0 = phi + sidx(N, 0, ym, z), *rp0 = phi + sidx(N, 0, yp, z);
+            const R *r0p = phi + sidx(N, 0, y, zp), *r0m = phi + sidx(N, 0, y, zm), *rpp = phi + sidx(N, 0, yp, zp);
+            const C c00 = ld_pair(r00 + x0), cm0 = ld_pair(rm0 + x0), cp0 = ld_pair(rp0 + x0);
+            const C c0p = ld_pair(r0p + x0), c0m = ld_pair(r0m + x0), cpp = ld_pair(rpp + x0);
+            const R f00m = __ldg(r00 + xm), f002 = __ldg(r00 + x2), fp02 = __ldg(rp0 + x2), f0p2 = __ldg(r0p + x2);
+            const int64_t i0 = sidx(N, x0, y, z);
+            R t0[6], t1[6];
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                const C tv = ld_pair(Tij + c * n3 + i0);
+                t0[c] = tv.x;
+                t1[c] = tv.y;
+            }
             R a0[6], a1[6];
-            prep_tij6(Tij, n3, phi, rc, N, 2 * n, y, z, a0);
-            prep_tij6(Tij, n3, phi, rc, N, 2 * n + 1, y, z, a1);
+            tij6_point(c00.x, c00.y, f00m, cp0.x, cm0.x, c0p.x, c0m.x, cp0.y, c0p.y, cpp.x, t0, rc, a0);
+            tij6_point(c00.y, f002, c00.x, cp0.y, cm0.y, c0p.y, c0m.y, fp02, f0p2, cpp.y, t1, rc, a1);
             Six s;
 #pragma unroll
             for (int c = 0; c < 6; c++) s.v[c] = mk(a0[c], a1[c]);
@@ -258,14 +276,13 @@ __global__ void __launch_bounds__(NT, GEV_TIJ6_MINB) k_fx_fwd_tij6(const R *__re
         [&](int idx, Six s) {
             const int o = (idx % M) * LD + idx / M;
 #pragma unroll
-            for (int c = 0; c < 6; c++) buf[c * CS + o] = s.v[c];
+            for (int c = 0; c < 6; c++) buf[o + c * T] = s.v[c];
         });
     __syncthreads();
-#pragma unroll 1
-    for (int c = 0; c < 6; c++) fft_lines<M, -1, T, NT>(buf + c * CS, LD, tw_half);
+    fft_lines<M, -1, T6, NT>(buf, LD, tw_half);
     for (int idx = threadIdx.x; idx < 6 * P * T; idx += NT) {
         const int k = idx % P, r = idx / P, t = r % T, c = r / T, y = y0 + t;
-        const C *b = buf + c * CS;
+        const C *b = buf + c * T;
         C zk = b[(k == M ? 0 : k) * LD + t];
         C zm = b[(k == 0 ? 0 : M - k) * LD + t];
         zm.y = -zm.y;

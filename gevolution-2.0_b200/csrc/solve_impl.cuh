@@ -89,7 +89,7 @@ void fx_tij6_n(const FxArgs<R> &a, int64_t in_stride, int64_t out_stride, const 
 {
     using C = typename CT<R>::C;
     constexpr int T = PassCfg<R>::TIJ6, NT = 256;
-    size_t smem = (size_t)6 * (N / 2) * (T + 1) * sizeof(C);
+    size_t smem = (size_t)(N / 2) * (6 * T + 1) * sizeof(C);
     auto k = k_fx_fwd_tij6<R, N, T, NT>;
     set_smem(k, smem);
     k<<<dim3(N / T, N), NT, smem, st>>>(a.in, in_stride, a.phi, a.c, a.out, out_stride, tb.tw_half, tb.tw_full);
