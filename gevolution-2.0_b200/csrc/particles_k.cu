@@ -33,6 +33,15 @@ __device__ __forceinline__ uint32_t lanemask_lt()
     return m;
 }
 
+// 1/x and 1/sqrt(x) in the field precision: the geodesic's divisions by e^2,
+// sqrt(e^2) and the uniform coefficients become multiplications (FP32: the
+// hardware reciprocal square root, within 2 ulp; FP64: correctly rounded
+// division and square root)
+__device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double recip(double x) { return 1.0 / x; }
+__device__ __forceinline__ float rsqrt_r(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double rsqrt_r(double x) { return 1.0 / sqrt(x); }
+
 // slot within bucket b, warp-aggregated (order inside a bucket is not significant)
 __device__ __forceinline__ uint32_t bucket_slot(uint32_t b, uint32_t *counts)
 {
@@ -100,7 +109,10 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
     const R *P_ = sf[0], *X_ = sf[1], *B0 = sf[2], *B1 = sf[3], *B2 = sf[4];
 
     const uint32_t lo = bstart[8 * tile], hi = bstart[8 * tile + 8];
-    double lmax = 0.0;
+    R lmax = 0;   // max of q^2 / a^2 (converted to FP64 once, at the end)
+    const R ib_k = (R)(1.0 / kp.b_k), ib_d = (R)(1.0 / kp.b_d);
+    const R ia2_k = (R)(1.0 / (kp.a_k * kp.a_k));
+    const double dtau_N = kp.dtau_d * (double)N;   // box units -> cell units
     for (uint32_t base = lo; base < hi; base += 2 * KD_NT) {
         // two particles per thread and pass: both loads are issued before either is used
         RawParticle<R> raw[2];
@@ -141,8 +153,9 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
             R phiint = 0;
 #pragma unroll
             for (int k = 0; k < 8; k++) phiint += w8[k] * SF(P_, rx, ry, rz, (k >> 2) & 1, (k >> 1) & 1, k & 1);
-            phiint /= e2;
-            phiint = (R)4 * phiint * v2 + ((R)1 + a * a * phiint) * (v2 + e2) / e2;
+            const R ie2 = recip(e2);
+            phiint *= ie2;
+            phiint = (R)4 * phiint * v2 + ((R)1 + a * a * phiint) * (v2 + e2) * ie2;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 const int ex = c == 0, ey = c == 1, ez = c == 2;
@@ -168,7 +181,8 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
                 gradphi[1] -= d[0] * d[2] * (SF(X_, rx, ry, rz, 1, 1, 1) - SF(X_, rx, ry, rz, 1, 0, 1));
                 gradphi[2] -= d[0] * d[1] * (SF(X_, rx, ry, rz, 1, 1, 1) - SF(X_, rx, ry, rz, 1, 1, 0));
             }
-            e2 = sqrt(e2);
+            const R ie = rsqrt_r(e2);
+            e2 *= ie;   // sqrt(q^2 + a^2)
             if (kp.nfield_k >= 3) {
                 // gevolution.hpp:970-993
                 R pg[3];
@@ -193,7 +207,7 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
                 pg[2] += (1 - d[0]) * d[1] * ((d[2] - 1) * SF(B2, rx, ry, rz, 0, 1, -1) + (1 - 2 * d[2]) * SF(B2, rx, ry, rz, 0, 1, 0) + d[2] * SF(B2, rx, ry, rz, 0, 1, 1)) * v[2];
                 pg[2] += d[0] * d[1] * ((d[2] - 1) * SF(B2, rx, ry, rz, 1, 1, -1) + (1 - 2 * d[2]) * SF(B2, rx, ry, rz, 1, 1, 0) + d[2] * SF(B2, rx, ry, rz, 1, 1, 1)) * v[2];
 #pragma unroll
-                for (int c = 0; c < 3; c++) gradphi[c] += pg[c] / (R)kp.b_k / e2;
+                for (int c = 0; c < 3; c++) gradphi[c] += pg[c] * (ib_k * ie);
             }
             v2 = 0;
 #pragma unroll
@@ -201,16 +215,14 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
                 v[c] -= (R)kp.dtau_k * e2 * gradphi[c] * (R)N;
                 v2 += v[c] * v[c];
             }
-            lmax = fmax(lmax, (double)(v2 / a / a));
+            lmax = fmax(lmax, v2 * ia2_k);
 #pragma unroll
             for (int c = 0; c < 3; c++) p.q[c * p.cap + i] = v[c];
         }
 
         if (kp.do_drift && ok) {
-            // update_pos, gevolution.hpp:1162-1232 (drift uses the kicked momentum,
-            // rounded to the storage precision as the reference stores it first)
-#pragma unroll
-            for (int c = 0; c < 3; c++) v[c] = p.q[c * p.cap + i];
+            // update_pos, gevolution.hpp:1162-1232: the drift uses the kicked
+            // momentum as stored (v holds it: the storage precision is R)
             const R a = (R)kp.a_d;
             R v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
             R e2 = v2 + a * a;
@@ -223,7 +235,7 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
 #pragma unroll
                 for (int k = 0; k < 8; k++) ch += w8[k] * SF(X_, rx, ry, rz, (k >> 2) & 1, (k >> 1) & 1, k & 1);
             }
-            v2 = ((R)1 + ((R)3 - v2 / e2) * ph - ch) / sqrt(e2);
+            v2 = ((R)1 + ((R)3 - v2 * recip(e2)) * ph - ch) * rsqrt_r(e2);
             R dp[3] = {v[0] * v2, v[1] * v2, v[2] * v2};
             if (kp.nfield_d >= 3) {
                 R b0 = SF(B0, rx, ry, rz, 0, 0, 0) * (1 - d[1]) * (1 - d[2]) + SF(B0, rx, ry, rz, 0, 1, 0) * d[1] * (1 - d[2]) +
@@ -232,14 +244,14 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
                             SF(B1, rx, ry, rz, 0, 0, 1) * (1 - d[0]) * d[2] + SF(B1, rx, ry, rz, 1, 0, 1) * d[0] * d[2];
                 R b2 = SF(B2, rx, ry, rz, 0, 0, 0) * (1 - d[0]) * (1 - d[1]) + SF(B2, rx, ry, rz, 1, 0, 0) * d[0] * (1 - d[1]) +
                             SF(B2, rx, ry, rz, 0, 1, 0) * (1 - d[0]) * d[1] + SF(B2, rx, ry, rz, 1, 1, 0) * d[0] * d[1];
-                dp[0] += b0 / (R)kp.b_d;
-                dp[1] += b1 / (R)kp.b_d;
-                dp[2] += b2 / (R)kp.b_d;
+                dp[0] += b0 * ib_d;
+                dp[1] += b1 * ib_d;
+                dp[2] += b2 * ib_d;
             }
             int cc[3] = {cx, cy, cz};
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                double o = dd[c] + kp.dtau_d * (double)dp[c] * (double)N;   // box units -> cell units
+                double o = dd[c] + dtau_N * (double)dp[c];
                 if (!isfinite(o)) { atomicOr(err, ERR_NONFINITE); o = dd[c]; }
                 double s = floor(o);
                 o -= s;
@@ -265,7 +277,7 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
     }
 
     for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = lmax;
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = (double)lmax;
     __syncthreads();
     if (threadIdx.x == 0 && kp.do_kick) {
         double m = 0.0;
