@@ -456,27 +456,35 @@ def adjoint_block(args, dev):
     target = 0.5 * torch.randn(N ** 3, generator=g, dtype=torch.float64).to(dev)
     mass = OMEGA_M / N ** 3
 
-    def run(precision, w, timed=False):
+    def run(precision, w, reps=3):
+        """min device times (ms) of forward and adjoint over reps passes on one
+        PM object; a first, untimed pass allocates the checkpoints"""
         p = gpm.PM(N, N ** 3, mass, precision, checkpoint_every=8)
         x0, q0 = gpm.zeldovich_map(w, N, box, a_in, fourpiG, OMEGA_M, OMEGA_L, H_LITTLE)
         x0, q0 = x0.detach().contiguous(), q0.detach().contiguous()
         delta = torch.empty(N ** 3, dtype=torch.float64, device=dev)
-        st = torch.cuda.ExternalStream(p.stream())
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-        torch.cuda.synchronize()
-        e[0].record(st)
-        p.forward(coef, x0, q0, delta)
-        e[1].record(st)
-        gd = (2.0 * (delta - target)).contiguous()
         gx = torch.empty_like(x0)
         gq = torch.empty_like(q0)
-        torch.cuda.synchronize()
-        e[2].record(st)
-        p.adjoint(gd, gx, gq)
-        e[3].record(st)
-        torch.cuda.synchronize()
-        loss = float(((delta - target) ** 2).sum())
-        return loss, gx, gq, e[0].elapsed_time(e[1]), e[2].elapsed_time(e[3]), p
+        st = torch.cuda.ExternalStream(p.stream())
+        fwd, adj = [], []
+        for r in range(reps + 1):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            torch.cuda.synchronize()
+            e[0].record(st)
+            p.forward(coef, x0, q0, delta)
+            e[1].record(st)
+            torch.cuda.synchronize()
+            gd = (2.0 * (delta - target)).contiguous()
+            torch.cuda.synchronize()
+            e[2].record(st)
+            p.adjoint(gd, gx, gq)
+            e[3].record(st)
+            torch.cuda.synchronize()
+            if r > 0:
+                fwd.append(e[0].elapsed_time(e[1]))
+                adj.append(e[2].elapsed_time(e[3]))
+        p.close()
+        return min(fwd), min(adj)
 
     def grad_modes(precision, w):
         wv = w.clone().requires_grad_(True)
@@ -497,10 +505,7 @@ def adjoint_block(args, dev):
                                   "%d^3 particles, %d steps z = 50 -> 0, loss sum (delta_CIC - target)^2, checkpoints "
                                   "every 8 steps" % (box, N, N, nsteps), "N": N, "steps": nsteps}}
     for name, prec in (("mixed", gev.MIXED), ("fp64", gev.FP64)):
-        run(prec, noise)                       # warm-up
-        times = [run(prec, noise)[3:5] for _ in range(3)]
-        fwd = min(t[0] for t in times)
-        adjm = min(t[1] for t in times)
+        fwd, adjm = run(prec, noise)
         out[name] = {"fwd_ms": fwd, "adjoint_ms": adjm, "grad_fwd_ratio": adjm / fwd,
                      "fwd_mpart_steps_s": N ** 3 * nsteps / (fwd * 1e-3) / 1e6}
     g64 = grad_modes(gev.FP64, noise)
