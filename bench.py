@@ -135,7 +135,7 @@ def lightcone_args(gev, d):
 SINGLE_KERNEL_STAGES = ("deposit_T00_Tij", "deposit_T0i")
 
 # DRAM bytes per launch measured by ncu at 256^3 (mixed precision), per stage kernel
-NCU_TRAFFIC_256 = {"deposit_T00_Tij": 0.881292e9 + 0.444754e9, "deposit_T0i": 0.877812e9 + 0.190918e9}
+NCU_TRAFFIC_256 = {"deposit_T00_Tij": 0.7451e9 + 0.4423e9, "deposit_T0i": 0.7434e9 + 0.1865e9}
 
 
 def ncu_traffic(stage, N):
@@ -380,7 +380,7 @@ def run_gpu(args, rank, world, local_rank):
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": ncu_traffic(dom, N),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same kernel at 256^3 "
-                                           "(profiles/deposit_kick_fz_256_mixed_ncu.md), scaled by the particle count",
+                                           "(profiles/particle_kernels_256_mixed_ncu.md), scaled by the particle count",
                          "algorithmic_bytes_per_launch": dom_bytes,
                          "step_algorithmic_bytes": step_alg, "step_achieved_gbs": step_gbs, "step_frac": step_gbs / peak},
             "clocks": clk,
