@@ -316,6 +316,53 @@ def test_drift_and_rebin(prec, nfield):
         assert abs(rho.sum() / (MASS * len(pos) * N ** 3) - 1) < 1e-6
 
 
+def _bucket_cell(pos, N):
+    """bucket = 8 tile + class and cell index of box-unit positions"""
+    c = np.minimum(np.floor(pos * N).astype(np.int64), N - 1)
+    nt = N // 8
+    t = c // 8
+    cls = (c[:, 0] % 8 == 7) * 1 + (c[:, 1] % 8 == 7) * 2 + (c[:, 2] % 8 == 7) * 4
+    tile = t[:, 0] + nt * (t[:, 1] + nt * t[:, 2])
+    return 8 * tile + cls, c[:, 0] + N * (c[:, 1] + N * c[:, 2])
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_rebin_order(prec):
+    """After loading and after a drift the particles sit in bucket order, every
+    bucket of at most 1024 particles in (cell, ID) order (what the deposit's
+    single-chunk path relies on), with none lost or repeated; a dense clump
+    takes the per-bucket sort (tiles above 1024) and the slot-order copy
+    (buckets above 1024)."""
+    N = 32
+    rng = np.random.default_rng(21)
+    blob = 0.3 + 0.02 * rng.standard_normal((12000, 3))
+    pos = np.concatenate([blob, rng.random((30000, 3))])
+    pos -= np.floor(pos)
+    q = rng.uniform(-0.05, 0.05, pos.shape)
+    ids = rng.permutation(len(pos)).astype(np.int64) * 7 + 3   # unique, not in index order
+    phi, chi = trough_phi(N), smooth_field(N, 70, 1e-6)
+    with make_ctx(N, prec, len(pos)) as c:
+        c.set_particles(pos, q, ids, MASS)
+        c.set_field(gev.FIELD_PHI, phi); c.set_field(gev.FIELD_CHI, chi)
+        for stage in ("load", "drift"):
+            if stage == "drift":
+                c.drift(0.1, 0.4, 0.16 * N, 2)
+            p2, q2, i2 = c.get_particles()
+            assert np.array_equal(np.sort(i2), np.sort(ids)), stage
+            b, cell = _bucket_cell(p2, N)
+            assert np.all(np.diff(b) >= 0), stage
+            starts = np.flatnonzero(np.r_[True, np.diff(b) != 0])
+            ends = np.r_[starts[1:], len(b)]
+            big = 0
+            for s0, e0 in zip(starts, ends):
+                if e0 - s0 > 1024:
+                    big += 1
+                    continue
+                key = cell[s0:e0] * (1 << 40) + i2[s0:e0]
+                assert np.all(np.diff(key) > 0), (stage, s0)
+            assert big >= 1, stage   # the clump exercises the slot-order copy
+
+
 @pytest.mark.parametrize("prec", PRECS)
 def test_power_spectrum(prec):
     N = 32
