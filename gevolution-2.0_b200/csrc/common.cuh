@@ -103,7 +103,7 @@ __host__ __device__ __forceinline__ uint32_t bucket_of_cell(int N, int nt, int x
 }
 
 // x-pass load modes (fused source preparation)
-enum { FX_COPY = 0, FX_PREP_T00 = 1, FX_PREP_TIJ = 2 };
+enum { FX_COPY = 0, FX_PREP_T00 = 1, FX_PREP_TIJ = 2, FX_PREP_T0I = 3 };
 // z-pass Fourier-space operators
 enum { OP_POISSON = 0, OP_SCALAR = 1, OP_VECTOR = 2, OP_BIN = 3, OP_ZELD = 4 };
 // optional extras of OP_SCALAR

@@ -220,6 +220,9 @@ template <class R> struct Ctx final : CtxBase {
     int64_t idset_cap = 0;
     int64_t lc_last = 0;
     bool cur_is_A = true;
+    bool bi_sums = false;       // Bi holds the potential-free T0i sums of project_step
+    bool t0i_pending = false;   // FP64 T0I_SUMS: solve_B deposits T0i first (with t0i_coeff)
+    double t0i_coeff = 1.0;
     int64_t launch_count = 0;
     int64_t np = 0;
     double mass = 0.0;
@@ -459,6 +462,7 @@ template <class R> struct Ctx final : CtxBase {
         mass = ip.Omega_m / (double)g.n3;
         cur_is_A = true;
         launch_ics_lattice<R>(view(true), Bi.p, N, st);
+        bi_sums = false;
         launched("ics lattice");
         rebin_from_cells();
         have_particles = true;
@@ -559,6 +563,7 @@ template <class R> struct Ctx final : CtxBase {
         const int64_t dn = cplx ? 2 * g.nk : g.n3;
         const int w = cplx ? 2 * g.P : (int)g.n3, dw = cplx ? 2 * g.PP : (int)g.n3;
         const int64_t rows = cplx ? (int64_t)g.N * g.N : 1;
+        if (f == GEV_FIELD_BI) bi_sums = t0i_pending = false;
         ensure_stage(n, 0);
         for (int c = 0; c < planes; c++) {
             ck(cudaMemcpyAsync(stage.p, host + (int64_t)c * n, n * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
@@ -576,7 +581,14 @@ template <class R> struct Ctx final : CtxBase {
     void project(uint32_t which, double a, double coeff, int use_phi, int accumulate) override
     {
         need_particles();
-        if (which & ~(GEV_PROJ_T00 | GEV_PROJ_TIJ | GEV_PROJ_T0I | GEV_PROJ_CIC)) throw ArgError("unknown projection");
+        if (which & ~(GEV_PROJ_T00 | GEV_PROJ_TIJ | GEV_PROJ_T0I | GEV_PROJ_CIC | GEV_PROJ_T0I_SUMS))
+            throw ArgError("unknown projection");
+        if (which & GEV_PROJ_T0I_SUMS) {
+            if (which != (GEV_PROJ_T00 | GEV_PROJ_TIJ | GEV_PROJ_T0I_SUMS) || !use_phi || accumulate)
+                throw ArgError("GEV_PROJ_T0I_SUMS goes with T00 | TIJ, use_phi and no accumulate");
+            project_t0i_sums(a, coeff);
+            return;
+        }
         if ((which & GEV_PROJ_CIC) && (which & GEV_PROJ_T00)) throw ArgError("CIC and T00 both target the source field");
         if (use_phi && a <= 0.0 && (which & (GEV_PROJ_T00 | GEV_PROJ_TIJ))) throw ArgError("scale factor must be positive");
         const double n3 = (double)g.n3;   // 1/dx^3
@@ -598,21 +610,53 @@ template <class R> struct Ctx final : CtxBase {
                 kind = DEP_TIJ;
                 for (int c = 0; c < 6; c++) o.p[c] = Sij.p + c * g.n3;
             }
-            launch_deposit<R>(kind, use_phi != 0, v, bstart.p, g.N, phi.p, o, a, m00, mij, accumulate, derr.p, st);
+            launch_deposit<R>(kind, use_phi != 0, v, bstart.p, g.N, phi.p, o, a, m00, mij, 0.0, accumulate, derr.p, st);
             launched("deposit T00/Tij");
         }
         if (which & GEV_PROJ_CIC) {
             DepOut<R> o{};
             o.p[0] = source.p;
-            launch_deposit<R>(DEP_T00, false, v, bstart.p, g.N, phi.p, o, 1.0, mass * coeff * n3, 0.0, accumulate, derr.p, st);
+            launch_deposit<R>(DEP_T00, false, v, bstart.p, g.N, phi.p, o, 1.0, mass * coeff * n3, 0.0, 0.0, accumulate, derr.p, st);
             launched("deposit CIC");
         }
         if (which & GEV_PROJ_T0I) {
             DepOut<R> o{};
             for (int c = 0; c < 3; c++) o.p[c] = Bi.p + c * g.n3;
-            launch_deposit<R>(DEP_T0I, use_phi != 0, v, bstart.p, g.N, phi.p, o, 1.0, mass * coeff * n3, 0.0, accumulate, derr.p, st);
+            launch_deposit<R>(DEP_T0I, use_phi != 0, v, bstart.p, g.N, phi.p, o, 1.0, mass * coeff * n3, 0.0, 0.0, accumulate, derr.p, st);
             launched("deposit T0i");
+            bi_sums = false;
+            t0i_pending = false;
         }
+    }
+
+    // One deposit for the cycle's three projections.  T0i's potential enters
+    // only as the per-vertex factor 1 + phi(x) + phi(x + e_i)
+    // (particle_T0i_project, gevolution.hpp:2031-2201) and the particles do
+    // not move between main.cu's T00/Tij and T0i projections, so the
+    // potential-free sums S_i are deposited here with T00 and Tij (previous
+    // phi), and solve_B's x pass multiplies them by the factor with the phi of
+    // its call (the new phi, as main.cu:836-955 uses).
+    void project_t0i_sums(double a, double coeff)
+    {
+        need_particles();
+        if (a <= 0.0) throw ArgError("scale factor must be positive");
+        if constexpr (sizeof(R) == 8) {
+            // FP64: 16-value records would leave one CTA per SM; the T0i
+            // deposit runs on its own at the start of solve_B instead
+            project(GEV_PROJ_T00 | GEV_PROJ_TIJ, a, coeff, 1, 0);
+            t0i_pending = true;
+            t0i_coeff = coeff;
+            return;
+        }
+        const double n3 = (double)g.n3 * coeff;
+        DepOut<R> o{};
+        o.p[0] = source.p;
+        for (int c = 0; c < 6; c++) o.p[1 + c] = Sij.p + c * g.n3;
+        for (int c = 0; c < 3; c++) o.p[7 + c] = Bi.p + c * g.n3;
+        launch_deposit<R>(DEP_T00_TIJ_S0I, true, cur(), bstart.p, g.N, phi.p, o, a, mass * n3 / a, mass * n3 / a,
+                          mass * n3, 0, derr.p, st);   // gevolution.hpp:1731, :1750, :2584; T0i mass * coeff / dx^3
+        launched("deposit T00/Tij/T0i sums");
+        bi_sums = true;
     }
 
     void solve_phi(int prepare, double bg, double c, double c2, double c3, double pc, double modif, double *sum,
@@ -676,6 +720,7 @@ template <class R> struct Ctx final : CtxBase {
         if (parab) {
             fx_inverse<R>(N, W.p + g.nk, g.nk, Bi.p, g.n3, 3, tb, st);
             launched("fx inverse (B)");
+            bi_sums = false;
         }
     }
 
@@ -683,8 +728,13 @@ template <class R> struct Ctx final : CtxBase {
     {
         const int N = g.N;
         const FftTables<R> tb = tables();
-        fx_forward<R>(N, FX_COPY, Bi.p, g.n3, 3, 0, nullptr, nullptr, 0, 0, 0, 0, W.p, g.nk, nullptr, tb, st);
+        // T0i straight from project(T0I), or completed from project_step's sums with the current phi
+        if (t0i_pending) project(GEV_PROJ_T0I, 1.0, t0i_coeff, 1, 0);
+        t0i_pending = false;
+        fx_forward<R>(N, bi_sums ? FX_PREP_T0I : FX_COPY, Bi.p, g.n3, 3, 0, phi.p, nullptr, 0, 0, 0, 0, W.p, g.nk,
+                      nullptr, tb, st);
         launched("fx forward (T0i)");
+        bi_sums = false;
         fy_pass<R>(N, -1, W.p, g.nk, 3, tb, st);
         launched("fy forward (T0i)");
         FzParams fp{};
@@ -1055,8 +1105,10 @@ int gev_step(gev_ctx *ctx, const gev_cosmo *cosmo, gev_state *s)
         const int N = c.cfg.N;
         const double dx = 1.0 / N;
         double a = s->a;
-        // T00 and Tij with the previous phi (main.cu:623, :756)
-        c.project(GEV_PROJ_T00 | GEV_PROJ_TIJ, a, 1.0, 1, 0);
+        // T00 and Tij with the previous phi (main.cu:623, :756); with elliptic B
+        // also the T0i sums that solve_B completes with the new phi
+        const bool elliptic = c.cfg.vector_method == GEV_VECTOR_ELLIPTIC;
+        c.project(GEV_PROJ_T00 | GEV_PROJ_TIJ | (elliptic ? GEV_PROJ_T0I_SUMS : 0u), a, 1.0, 1, 0);
         // phi (main.cu:719-809)
         if (s->dtau_old > 0.) {
             const double H = gev::hconf(a, cm.fourpiG, cm);
@@ -1069,11 +1121,8 @@ int gev_step(gev_ctx *ctx, const gev_cosmo *cosmo, gev_state *s)
         // chi, h_ij (main.cu:820-966)
         const double H = gev::hconf(a, cm.fourpiG, cm);
         c.solve_chi(2. * cm.fourpiG * dx * dx / a, s->cycle == 0, H, s->dtau, s->dtau_old, a * a * s->dtau_old);
-        // B elliptic with the new phi (main.cu:836-955)
-        if (c.cfg.vector_method == GEV_VECTOR_ELLIPTIC) {
-            c.project(GEV_PROJ_T0I, a, 1.0, 1, 0);
-            c.solve_B(cm.fourpiG * dx * dx, 0.);
-        }
+        // B elliptic with the new phi (main.cu:836-955): T0i completed in solve_B's x pass
+        if (elliptic) c.solve_B(cm.fourpiG * dx * dx, 0.);
         // kick, background half step, drift, background half step (main.cu:1225-1283)
         gev::KickDriftParams kp{};
         kp.do_kick = 1; kp.do_drift = 1; kp.do_bin = 1;

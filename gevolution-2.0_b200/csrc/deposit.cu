@@ -41,25 +41,42 @@ constexpr int DEP_NT = 512;   // one thread per tile vertex
 #ifndef GEV_DEP_MINB_T0I_F
 #define GEV_DEP_MINB_T0I_F 4
 #endif
+// the 16-value T00+Tij+S records: chunks of 768 records keep three CTAs per
+// SM (1024 would leave two; measured over the full cycle at 512^3)
+#ifndef GEV_DEP_MINB_S_F
+#define GEV_DEP_MINB_S_F 3
+#endif
+#ifndef GEV_DEP_CH_S_F
+#define GEV_DEP_CH_S_F 768
+#endif
 
-template <class R> struct DepCh;
-template <> struct DepCh<float> { static constexpr int v = 1024; static constexpr int EMAX = 120; };
-template <> struct DepCh<double> { static constexpr int v = 768; static constexpr int EMAX = 1000; };
-static_assert(DepCh<float>::v <= REBIN_SORT_MAX && DepCh<double>::v <= REBIN_SORT_MAX,
+// records per chunk (shared-memory budget) and the fixed-point exponent limit
+template <class R, int KIND = DEP_T00> struct DepCh;
+template <int KIND> struct DepCh<float, KIND> {
+    static constexpr int v = KIND == DEP_T00_TIJ_S0I ? GEV_DEP_CH_S_F : 1024;
+    static constexpr int EMAX = 120;
+};
+template <int KIND> struct DepCh<double, KIND> { static constexpr int v = 768; static constexpr int EMAX = 1000; };
+static_assert(DepCh<float>::v <= REBIN_SORT_MAX && DepCh<float, DEP_T00_TIJ_S0I>::v <= REBIN_SORT_MAX &&
+                  DepCh<double>::v <= REBIN_SORT_MAX,
               "a single-chunk deposit must only see buckets that the re-binning keeps sorted");
 
-// record layout: [d0 d1 d2 | T00: E F G | Tij: W00 W11 W22 W01 W02 W12 | T0i: Q0 Q1 Q2]
+// record layout: [d0 d1 d2 | T00: E F G | Tij: W00 W11 W22 W01 W02 W12 | T0i: Q0 Q1 Q2 | S: P0 P1 P2]
+// (S: the T0i momenta m q_i without the potential factor, DEP_T00_TIJ_S0I)
 template <int KIND> struct DepShape {
-    static constexpr bool HAS00 = (KIND == DEP_T00 || KIND == DEP_T00_TIJ);
-    static constexpr bool HASIJ = (KIND == DEP_TIJ || KIND == DEP_T00_TIJ);
+    static constexpr bool HAS00 = (KIND == DEP_T00 || KIND == DEP_T00_TIJ || KIND == DEP_T00_TIJ_S0I);
+    static constexpr bool HASIJ = (KIND == DEP_TIJ || KIND == DEP_T00_TIJ || KIND == DEP_T00_TIJ_S0I);
     static constexpr bool HAS0I = (KIND == DEP_T0I);
-    static constexpr int NC = (HAS00 ? 1 : 0) + (HASIJ ? 6 : 0) + (HAS0I ? 3 : 0);
+    static constexpr bool HASS = (KIND == DEP_T00_TIJ_S0I);
+    static constexpr int NC = (HAS00 ? 1 : 0) + (HASIJ ? 6 : 0) + (HAS0I ? 3 : 0) + (HASS ? 3 : 0);
     static constexpr int F00 = 3;
     static constexpr int FIJ = 3 + (HAS00 ? 3 : 0);
     static constexpr int F0I = 3;
-    static constexpr int NF = 3 + (HAS00 ? 3 : 0) + (HASIJ ? 6 : 0) + (HAS0I ? 3 : 0);
+    static constexpr int FS = FIJ + (HASIJ ? 6 : 0);
+    static constexpr int NF = 3 + (HAS00 ? 3 : 0) + (HASIJ ? 6 : 0) + (HAS0I ? 3 : 0) + (HASS ? 3 : 0);
     static constexpr int NFP = (NF + 3) & ~3;   // padded for 16-byte record loads
     static constexpr int CIJ = HAS00 ? 1 : 0;   // first Tij output component
+    static constexpr int CS = CIJ + (HASIJ ? 6 : 0);   // first S output component
 };
 
 constexpr int DEP_NCELL = 729;                  // 9^3 cells of a tile's reach
@@ -79,8 +96,8 @@ __device__ __forceinline__ int phi_slot(int vx, int vy, int vz) { return (vx + 1
 // f2 / (1 + f2/a^2) as f2 a^2 / e^2 (the same quantity).
 template <class R, int KIND, bool USE_PHI>
 __device__ __forceinline__ bool make_record(const RawParticle<R> &pr, int N, const FastDiv &fN, int x0, int y0, int z0,
-                                            const R *phis, R a, R m00, R mij, R (&v)[DepShape<KIND>::NF], int &lc,
-                                            R (&bnd)[DepShape<KIND>::NC])
+                                            const R *phis, R a, R m00, R mij, R m0i, R (&v)[DepShape<KIND>::NF],
+                                            int &lc, R (&bnd)[DepShape<KIND>::NC])
 {
     using S = DepShape<KIND>;
     int cx, cy, cz;
@@ -140,6 +157,13 @@ __device__ __forceinline__ bool make_record(const RawParticle<R> &pr, int N, con
             bnd[k] = fabs(m00 * q[k]) * ((R)1 + (R)2 * pm);
         }
     }
+    if constexpr (S::HASS) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            v[S::FS + k] = m0i * q[k];
+            bnd[S::CS + k] = fabs(m0i * q[k]);
+        }
+    }
     return true;
 }
 
@@ -160,6 +184,10 @@ template <class R, int KIND> __device__ __forceinline__ void scale_record(R *r, 
     if constexpr (S::HAS0I) {
 #pragma unroll
         for (int k = 0; k < 3; k++) r[S::F0I + k] *= scl[k];
+    }
+    if constexpr (S::HASS) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) r[S::FS + k] *= scl[S::CS + k];
     }
 }
 
@@ -193,6 +221,12 @@ __device__ __forceinline__ void gather_one(const R *r, int bx, int by, int bz, R
         if (!by) acc[1] += to_fixed<R>(wx * wz * r[S::F0I + 1] * ((R)1 + phv + phy));
         if (!bz) acc[2] += to_fixed<R>(wx * wy * r[S::F0I + 2] * ((R)1 + phv + phz));
     }
+    if constexpr (S::HASS) {
+        constexpr int C = S::CS;
+        if (!bx) acc[C + 0] += to_fixed<R>(wy * wz * r[S::FS + 0]);
+        if (!by) acc[C + 1] += to_fixed<R>(wx * wz * r[S::FS + 1]);
+        if (!bz) acc[C + 2] += to_fixed<R>(wx * wy * r[S::FS + 2]);
+    }
 }
 
 // add the contributions of one (unscaled) record in the field precision
@@ -221,6 +255,12 @@ __device__ __forceinline__ void gather_sum(const R *r, int bx, int by, int bz, R
         if (!bx) acc[0] += wy * wz * r[S::F0I + 0] * ((R)1 + phv + phx);
         if (!by) acc[1] += wx * wz * r[S::F0I + 1] * ((R)1 + phv + phy);
         if (!bz) acc[2] += wx * wy * r[S::F0I + 2] * ((R)1 + phv + phz);
+    }
+    if constexpr (S::HASS) {
+        constexpr int C = S::CS;
+        if (!bx) acc[C + 0] += wy * wz * r[S::FS + 0];
+        if (!by) acc[C + 1] += wx * wz * r[S::FS + 1];
+        if (!bz) acc[C + 2] += wx * wy * r[S::FS + 2];
     }
 }
 
@@ -272,8 +312,8 @@ template <class R, int NFP> __device__ __forceinline__ void load_record(const R 
 template <class R, int KIND>
 __host__ __device__ constexpr size_t dep_smem_bytes()
 {
-    return (size_t)DepShape<KIND>::NFP * DepCh<R>::v * sizeof(R) + (size_t)(2 * 730) * sizeof(int) +
-           (size_t)3 * DepCh<R>::v * sizeof(uint16_t);
+    return (size_t)DepShape<KIND>::NFP * DepCh<R, KIND>::v * sizeof(R) + (size_t)(2 * 730) * sizeof(int) +
+           (size_t)3 * DepCh<R, KIND>::v * sizeof(uint16_t);
 }
 
 // Resident CTAs per SM the register budget is sized for.  The kernel is bound
@@ -283,16 +323,17 @@ __host__ __device__ constexpr size_t dep_smem_bytes()
 // records (32 registers).  FP64 records fill the shared memory of two CTAs.
 template <class R, int KIND> struct DepMinBlocks { static constexpr int v = sizeof(R) == 4 ? GEV_DEP_MINB_F : 2; };
 template <> struct DepMinBlocks<float, DEP_T0I> { static constexpr int v = GEV_DEP_MINB_T0I_F; };
+template <> struct DepMinBlocks<float, DEP_T00_TIJ_S0I> { static constexpr int v = GEV_DEP_MINB_S_F; };
 
 // outputs: component c is written to out[c] (N^3 plane each)
 template <class R, int KIND, bool USE_PHI>
 __global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v) k_deposit(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt,
                                                        const R *__restrict__ phi, DepOut<R> out, double a, double m00,
-                                                       double mij, int accumulate, int *err, FastDiv fN)
+                                                       double mij, double m0i, int accumulate, int *err, FastDiv fN)
 {
     using S = DepShape<KIND>;
     constexpr int NC = S::NC, NF = S::NF, NFP = S::NFP;
-    constexpr int CH = DepCh<R>::v;
+    constexpr int CH = DepCh<R, KIND>::v;
     extern __shared__ __align__(16) unsigned char dsm[];
     R *rec = reinterpret_cast<R *>(dsm);                      // [CH][NFP]
     int *cstart = reinterpret_cast<int *>(rec + CH * NFP);    // 730
@@ -313,7 +354,7 @@ __global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v) k_deposit(PV
     const int tx = tile % nt, ty = (tile / nt) % nt, tz = tile / (nt * nt);
     const int x0 = tx * 8, y0 = ty * 8, z0 = tz * 8;
 
-    const R ra = (R)a, rm00 = (R)m00, rmij = (R)mij;
+    const R ra = (R)a, rm00 = (R)m00, rmij = (R)mij, rm0i = (R)m0i;
     // the phi stencil loads go out first and stay in flight while the bucket
     // ranges are looked up
     constexpr int PER = (1000 + DEP_NT - 1) / DEP_NT;
@@ -423,7 +464,7 @@ __global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v) k_deposit(PV
             if (j >= n) continue;
             R v[NF], b[NC];
             int lc;
-            if (make_record<R, KIND, USE_PHI>(raw[u], N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
+            if (make_record<R, KIND, USE_PHI>(raw[u], N, fN, x0, y0, z0, phis, ra, rm00, rmij, rm0i, v, lc, b)) {
                 store_record<R, NFP>(rec, j, v);
                 rcell[j] = (uint16_t)lc;
             } else {
@@ -509,7 +550,7 @@ __global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v) k_deposit(PV
             const uint32_t i = seg_index(seg_lo, seg_pre, j);
             R v[NF], b[NC];
             int lc;
-            if (make_record<R, KIND, USE_PHI>(load_particle(p, i), N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
+            if (make_record<R, KIND, USE_PHI>(load_particle(p, i), N, fN, x0, y0, z0, phis, ra, rm00, rmij, rm0i, v, lc, b)) {
 #pragma unroll
                 for (int c = 0; c < NC; c++) lb[c] = fmax(lb[c], b[c]);
             }
@@ -532,7 +573,7 @@ __global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v) k_deposit(PV
                 const uint32_t i = seg_index(seg_lo, seg_pre, base + (uint32_t)j);
                 R v[NF], b[NC];
                 int lc;
-                if (make_record<R, KIND, USE_PHI>(load_particle(p, i), N, fN, x0, y0, z0, phis, ra, rm00, rmij, v, lc, b)) {
+                if (make_record<R, KIND, USE_PHI>(load_particle(p, i), N, fN, x0, y0, z0, phis, ra, rm00, rmij, rm0i, v, lc, b)) {
                     scale_record<R, KIND>(v, scl_s);   // fixed-point scales of the components (weights unscaled)
                     store_record<R, NFP>(rec, j, v);
                     rcell[j] = (uint16_t)lc;
@@ -581,7 +622,7 @@ __global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v) k_deposit(PV
 
 template <class R, int KIND, bool USE_PHI>
 static void launch_k(const PView<R> &p, const uint32_t *bstart, int N, const R *phi, const DepOut<R> &out, double a,
-                     double m00, double mij, int accumulate, int *err, cudaStream_t st)
+                     double m00, double mij, double m0i, int accumulate, int *err, cudaStream_t st)
 {
     constexpr size_t smem = dep_smem_bytes<R, KIND>();
     static bool attr_set = false;
@@ -591,30 +632,32 @@ static void launch_k(const PView<R> &p, const uint32_t *bstart, int N, const R *
     }
     const int nt = N / 8;
     const unsigned grid = (unsigned)nt * nt * nt;
-    k_deposit<R, KIND, USE_PHI><<<grid, DEP_NT, smem, st>>>(p, bstart, N, nt, phi, out, a, m00, mij, accumulate, err,
+    k_deposit<R, KIND, USE_PHI><<<grid, DEP_NT, smem, st>>>(p, bstart, N, nt, phi, out, a, m00, mij, m0i, accumulate, err,
                                                                       FastDiv((uint32_t)N));
 }
 
 template <class R>
 void launch_deposit(int kind, bool use_phi, const PView<R> &p, const uint32_t *bstart, int N, const R *phi,
-                    const DepOut<R> &out, double a, double m00, double mij, int accumulate, int *err, cudaStream_t st)
+                    const DepOut<R> &out, double a, double m00, double mij, double m0i, int accumulate, int *err,
+                    cudaStream_t st)
 {
-#define GEV_DEP(K)                                                                                    \
-    if (kind == K) {                                                                                  \
-        if (use_phi) launch_k<R, K, true>(p, bstart, N, phi, out, a, m00, mij, accumulate, err, st);  \
-        else launch_k<R, K, false>(p, bstart, N, phi, out, a, m00, mij, accumulate, err, st);         \
+#define GEV_DEP(K)                                                                                         \
+    if (kind == K) {                                                                                       \
+        if (use_phi) launch_k<R, K, true>(p, bstart, N, phi, out, a, m00, mij, m0i, accumulate, err, st);  \
+        else launch_k<R, K, false>(p, bstart, N, phi, out, a, m00, mij, m0i, accumulate, err, st);         \
         return;                                                                             \
     }
     GEV_DEP(DEP_T00)
     GEV_DEP(DEP_TIJ)
     GEV_DEP(DEP_T00_TIJ)
     GEV_DEP(DEP_T0I)
+    GEV_DEP(DEP_T00_TIJ_S0I)
 #undef GEV_DEP
 }
 
 template void launch_deposit<float>(int, bool, const PView<float> &, const uint32_t *, int, const float *,
-                                    const DepOut<float> &, double, double, double, int, int *, cudaStream_t);
+                                    const DepOut<float> &, double, double, double, double, int, int *, cudaStream_t);
 template void launch_deposit<double>(int, bool, const PView<double> &, const uint32_t *, int, const double *,
-                                     const DepOut<double> &, double, double, double, int, int *, cudaStream_t);
+                                     const DepOut<double> &, double, double, double, double, int, int *, cudaStream_t);
 
 }  // namespace gev

@@ -134,6 +134,18 @@ __device__ __forceinline__ R prep_tij(const R *T, const R *phi, R coeff, int c, 
     return (R)2 * u * v + w * (u + v + (R)0.5 * w) + coeff * t;
 }
 
+// T0i component c completed from its potential-free sum S_c at vertex x:
+// T0i_c(x) = (1 + phi(x) + phi(x + e_c)) S_c(x) -- the per-vertex factor of
+// particle_T0i_project (gevolution.hpp:2031-2201), which does not depend on
+// the particle, applied once per vertex with the current phi
+template <class R>
+__device__ __forceinline__ R prep_t0i(const R *S, const R *phi, int c, int N, int x, int y, int z)
+{
+    const int64_t i = sidx(N, x, y, z);
+    const R f = (R)1 + __ldg(phi + i) + ldr(phi, N, x + (c == 0), y + (c == 1), z + (c == 2));
+    return f * __ldg(S + i);
+}
+
 // ---------------------------------------------------------------------------
 // x pass, forward: real rows -> half spectrum.  grid (N/T, N, ncomp)
 // ---------------------------------------------------------------------------
@@ -166,6 +178,9 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 4 ? GEV_FX_MINB : 1) k_fx_fwd
                 v0 = (R)prep_t00(a, N, 2 * n, y, z, s0);
                 v1 = (R)prep_t00(a, N, 2 * n + 1, y, z, s1);
                 lsum += s0 + s1;
+            } else if constexpr (MODE == FX_PREP_T0I) {
+                v0 = prep_t0i(in, a.phi, a.comp0 + comp, N, 2 * n, y, z);
+                v1 = prep_t0i(in, a.phi, a.comp0 + comp, N, 2 * n + 1, y, z);
             } else {
                 v0 = prep_tij(in, a.phi, (R)a.c, a.comp0 + comp, N, 2 * n, y, z);
                 v1 = prep_tij(in, a.phi, (R)a.c, a.comp0 + comp, N, 2 * n + 1, y, z);

@@ -10,13 +10,16 @@
 
 namespace gev {
 
-enum { DEP_T00 = 0, DEP_TIJ = 1, DEP_T00_TIJ = 2, DEP_T0I = 3 };
+// DEP_T00_TIJ_S0I: T00 and Tij, plus the three T0i sums without their
+// potential factor (completed by the B solve's x pass with the new phi)
+enum { DEP_T00 = 0, DEP_TIJ = 1, DEP_T00_TIJ = 2, DEP_T0I = 3, DEP_T00_TIJ_S0I = 4 };
 
-template <class R> struct DepOut { R *p[7]; };
+template <class R> struct DepOut { R *p[10]; };
 
 template <class R>
 void launch_deposit(int kind, bool use_phi, const PView<R> &p, const uint32_t *bstart, int N, const R *phi,
-                    const DepOut<R> &out, double a, double m00, double mij, int accumulate, int *err, cudaStream_t st);
+                    const DepOut<R> &out, double a, double m00, double mij, double m0i, int accumulate, int *err,
+                    cudaStream_t st);
 
 // ---- particles ----
 struct KickDriftParams {

@@ -106,6 +106,7 @@ void fx_forward(int N, int mode, const R *in, int64_t in_stride, int ncomp, int 
     a.comp0 = comp0; a.out = out; a.partial = partial;
     if (mode == FX_COPY) { GEV_SWITCH_N(N, (fx_fwd_n<R, NN, FX_COPY>(a, ncomp, in_stride, out_stride, tb, st))) }
     else if (mode == FX_PREP_T00) { GEV_SWITCH_N(N, (fx_fwd_n<R, NN, FX_PREP_T00>(a, ncomp, in_stride, out_stride, tb, st))) }
+    else if (mode == FX_PREP_T0I) { GEV_SWITCH_N(N, (fx_fwd_n<R, NN, FX_PREP_T0I>(a, ncomp, in_stride, out_stride, tb, st))) }
     else if (ncomp == 6 && comp0 == 0) { GEV_SWITCH_N(N, (fx_tij6_n<R, NN>(a, in_stride, out_stride, tb, st))) }
     else { GEV_SWITCH_N(N, (fx_fwd_n<R, NN, FX_PREP_TIJ>(a, ncomp, in_stride, out_stride, tb, st))) }
 }

@@ -35,7 +35,7 @@ GEV_ERR_SIZE = 7
 FP64, MIXED = 0, 1
 VECTOR_PARABOLIC, VECTOR_ELLIPTIC = 0, 1
 FIELD_PHI, FIELD_CHI, FIELD_SOURCE, FIELD_SIJ, FIELD_BI, FIELD_HIJ_FT, FIELD_HIJP_FT, FIELD_BI_FT = range(8)
-PROJ_T00, PROJ_TIJ, PROJ_T0I, PROJ_CIC = 1, 2, 4, 8
+PROJ_T00, PROJ_TIJ, PROJ_T0I, PROJ_CIC, PROJ_T0I_SUMS = 1, 2, 4, 8, 16
 
 _d, _i, _u, _l, _p = ctypes.c_double, ctypes.c_int32, ctypes.c_uint32, ctypes.c_int64, ctypes.c_void_p
 

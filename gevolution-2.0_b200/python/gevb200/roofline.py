@@ -23,20 +23,28 @@ def stage_bytes(stage, N, precision="mixed", np_=None):
         "deposit_T00_Tij": np_ * P + n3 * F * (1 + 7),
         # read particles, read phi, write 3 T0i
         "deposit_T0i": np_ * P + n3 * F * (1 + 3),
+        # one deposit for the cycle (GEV_PROJ_T0I_SUMS): read particles, read phi,
+        # write T00 + 6 Tij + 3 potential-free T0i sums
+        "deposit_T00_Tij_T0i": np_ * P + n3 * F * (1 + 7 + 3),
         # read T00, phi, chi; write spectrum; read spectrum; write phi
         "solve_phi": n3 * F * (3 + 1 + 1 + 1),
         # read 6 Tij + phi, write 6 spectra; read 6 spectra (as the fused solve needs them), write chi
         "solve_chi": n3 * F * (7 + 6 + 6 + 1),
         # read 3 T0i, write 3 spectra; read 3, write 3 B
         "solve_B": n3 * F * (3 + 3 + 3 + 3),
+        # the same from the T0i sums, which the x pass completes with phi (one more read)
+        "solve_B_sums": n3 * F * (3 + 1 + 3 + 3 + 3),
         # read + write particles, read phi, chi, 3 B
         "kick_drift": 2 * np_ * P + n3 * F * 5,
     }
     return table[stage]
 
 
-STAGES = ("deposit_T00_Tij", "solve_phi", "solve_chi", "deposit_T0i", "solve_B", "kick_drift")
+# the cycle's stages: in mixed precision one deposit completes T0i through the
+# B solve (GEV_PROJ_T0I_SUMS); FP64 keeps the separate T0i deposit
+STAGES = {"mixed": ("deposit_T00_Tij_T0i", "solve_phi", "solve_chi", "solve_B_sums", "kick_drift"),
+          "fp64": ("deposit_T00_Tij", "solve_phi", "solve_chi", "deposit_T0i", "solve_B", "kick_drift")}
 
 
 def step_bytes(N, precision="mixed", np_=None):
-    return sum(stage_bytes(s, N, precision, np_) for s in STAGES)
+    return sum(stage_bytes(s, N, precision, np_) for s in STAGES[precision])

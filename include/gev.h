@@ -65,6 +65,7 @@ typedef struct gev_ctx gev_ctx;
 #define GEV_PROJ_TIJ 2u
 #define GEV_PROJ_T0I 4u
 #define GEV_PROJ_CIC 8u
+#define GEV_PROJ_T0I_SUMS 16u
 
 typedef struct {
     int32_t N;              /* grid points per side: multiple of 8, N/8 a power of two or 3x one, 16..1024 */
@@ -111,7 +112,15 @@ int gev_field_components(int32_t field);
  * use_phi != 0 applies the Bardeen-potential corrections with GEV_FIELD_PHI
  * (the reference's phi != nullptr).  accumulate == 0 overwrites the targets
  * (the reference zeroes them first, main.cu:616, :681, :840); accumulate != 0
- * adds to them. */
+ * adds to them.
+ *   T0I_SUMS (only as T00 | TIJ | T0I_SUMS, use_phi != 0, accumulate == 0):
+ *        the same deposit also leaves in GEV_FIELD_BI the T0i sums without
+ *        their potential factor; the next gev_solve_B multiplies them by
+ *        1 + phi(x) + phi(x + e_i) with the phi of that call, which gives
+ *        projection_T0i_project with that phi (the potential enters T0i only
+ *        through that per-vertex factor, and main.cu projects T0i after the
+ *        phi update with the particles unmoved).  params {a, coeff}; one
+ *        deposit instead of two per cycle (gev_step uses it with elliptic B). */
 int gev_project(gev_ctx *ctx, uint32_t which, double a, double coeff, int32_t use_phi,
                 int32_t accumulate);
 

@@ -109,6 +109,50 @@ def test_deposit_is_order_independent_and_bitwise_reproducible(prec, n):
 
 
 @pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("n", [30000, 60000])
+def test_t0i_sums_completed_by_solve_B(prec, n):
+    """GEV_PROJ_T0I_SUMS: T00 and Tij as without it, and T0i -- completed by
+    the next solve_B with the phi of that call -- as a separate T0i deposit
+    with that phi (the potential changes in between, as in the cycle)."""
+    N = 32
+    pos, q, ids = particles(N, n=n, seed=31)
+    phi_old, phi_new = trough_phi(N), trough_phi(N, 2e-5)
+    coeff = 0.7
+    outs = []
+    for fused in (False, True):
+        with make_ctx(N, prec, len(pos)) as c:
+            c.set_particles(pos, q, ids, MASS)
+            c.set_field(gev.FIELD_PHI, phi_old)
+            if fused:
+                c.project(gev.PROJ_T00 | gev.PROJ_TIJ | gev.PROJ_T0I_SUMS, 0.5, coeff, True)
+            else:
+                c.project(gev.PROJ_T00 | gev.PROJ_TIJ, 0.5, coeff, True)
+            src, sij = c.get_field(gev.FIELD_SOURCE), c.get_field(gev.FIELD_SIJ)
+            c.set_field(gev.FIELD_PHI, phi_new)
+            if not fused:
+                c.project(gev.PROJ_T0I, 0.5, coeff, True)
+            c.solve_B(1e-3)
+            outs.append((src, sij, c.get_field(gev.FIELD_BI)))
+    tol = 1e-12 if prec == gev.FP64 else 1e-5
+    for x, y in zip(outs[0], outs[1]):
+        assert rel_err(y, x) < tol
+
+
+def test_t0i_sums_arguments():
+    N = 16
+    pos, q, ids = particles(N, n=2000, seed=32)
+    with make_ctx(N, gev.MIXED, len(pos)) as c:
+        c.set_particles(pos, q, ids, MASS)
+        for which, use_phi, acc in ((gev.PROJ_T0I_SUMS, True, False),
+                                    (gev.PROJ_T00 | gev.PROJ_T0I_SUMS, True, False),
+                                    (gev.PROJ_T00 | gev.PROJ_TIJ | gev.PROJ_T0I | gev.PROJ_T0I_SUMS, True, False),
+                                    (gev.PROJ_T00 | gev.PROJ_TIJ | gev.PROJ_T0I_SUMS, False, False),
+                                    (gev.PROJ_T00 | gev.PROJ_TIJ | gev.PROJ_T0I_SUMS, True, True)):
+            with pytest.raises(gev.GevError):
+                c.project(which, 0.5, 1.0, use_phi, acc)
+
+
+@pytest.mark.parametrize("prec", PRECS)
 def test_deposit_clustered_particles(prec):
     """A dense clump (thousands of particles in a few tiles, several chunks per
     tile) next to a sparse background, against the oracle."""
@@ -490,6 +534,8 @@ def test_step_matches_oracle(prec):
         assert abs(gst.T00hom / ost.T00hom - 1) < (1e-10 if prec == gev.FP64 else 1e-6)
         assert rel_err(c.get_field(gev.FIELD_PHI), phi) < (1e-8 if prec == gev.FP64 else 1e-3)
         assert rel_err(c.get_field(gev.FIELD_CHI), chi) < (1e-6 if prec == gev.FP64 else 2e-2)
+        # B_i from the T0i sums of the cycle's single deposit, completed with the new phi
+        assert rel_err(c.get_field(gev.FIELD_BI), Bi) < (1e-12 if prec == gev.FP64 else 1e-5)
         p2, q2, i2 = c.get_particles()
         order = np.argsort(i2)
         d = p2[order] - p_ref
