@@ -265,16 +265,24 @@ __device__ __forceinline__ void gather_sum(const R *r, int bx, int by, int bz, R
 }
 
 // Records in shared memory: record k is C = NFP / L chunks of 16 bytes (L
-// values of R each), stored whole with 16-byte accesses.  With an even chunk
-// count the two halves of each chunk pair swap places in records 4..7 mod 8,
-// so the same chunk of 8 consecutive records falls in 8 different 4-bank
-// groups (a quarter warp of 16-byte accesses without bank conflicts); an odd
-// count (the 12-value T00+Tij record in FP32) spreads them by itself.
+// values of R each), stored whole with 16-byte accesses.  Chunk m of record k
+// sits in 4-bank group (C k + m') mod 8; the chunk order m' is permuted by
+// k so that the same chunk of any 8 consecutive records falls in 8 different
+// groups (a quarter warp of 16-byte accesses without bank conflicts): an odd
+// C spreads them by itself, C = 2 mod 4 swaps chunk pairs in records 4..7 mod
+// 8, C = 4 mod 8 XORs the chunk index with (k / 2) mod 4, C = 0 mod 8 with
+// k mod 8.
 template <class R, int NFP> struct RecLayout {
     static constexpr int L = 16 / (int)sizeof(R);
     static constexpr int C = NFP / L;
     static_assert(NFP % L == 0, "records are whole 16-byte chunks");
-    __device__ __forceinline__ static int chunk(int k, int m) { return k * C + ((C % 2 == 0) ? (m ^ ((k >> 2) & 1)) : m); }
+    __device__ __forceinline__ static int chunk(int k, int m)
+    {
+        if constexpr (C % 8 == 0) return k * C + (m ^ (k & 7));
+        else if constexpr (C % 4 == 0) return k * C + (m ^ ((k >> 1) & 3));
+        else if constexpr (C % 2 == 0) return k * C + (m ^ ((k >> 2) & 1));
+        else return k * C + m;
+    }
 };
 
 template <class R, int NFP, int NF>
