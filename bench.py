@@ -214,10 +214,7 @@ def run_gpu(args, rank, world, local_rank):
 
     def cycle(c, st):
         """One cycle of main.cu's loop with the lightcone between the solves and the kick."""
-        a = st.a
-        Hc = gev.hconf(a, fourpiG, ctypes.byref(cosmo))
-        c.lightcone(lc, st.tau, st.dtau, st.dtau_old, a, a * Hc, lc_cap, fetch=False)
-        c.step(cosmo, st)
+        c.step_lightcone(cosmo, st, lc, lc_cap)
 
     def barrier():
         if world > 1:

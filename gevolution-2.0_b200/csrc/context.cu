@@ -1096,11 +1096,17 @@ void gev_rungekutta4bg(double *a, double fourpiG, const gev_cosmo *cosmo, double
 
 double gev_particle_horizon(double a, double fourpiG, const gev_cosmo *cosmo) { return gev::particle_horizon(a, fourpiG, *cosmo); }
 
-// One cycle of main.cu:608-1317 (GR, CDM, elliptic or parabolic B), no outputs.
-int gev_step(gev_ctx *ctx, const gev_cosmo *cosmo, gev_state *s)
+namespace {
+
+// One cycle of main.cu:608-1317 (GR, CDM, elliptic or parabolic B); with lc,
+// the lightcone shell between the solves and the kick.  A lightcone capacity
+// overflow lets the cycle finish and is reported at the end.
+int step_cycle(gev_ctx *ctx, const gev_cosmo *cosmo, gev_state *s, const gev_lightcone_args *lc, int64_t lc_cap,
+               int64_t *lc_n)
 {
-    if (!cosmo || !s) return fail(ctx, GEV_ERR_ARG, "null argument");
-    return guarded(ctx, [&](gev::CtxBase &c) {
+    if (!cosmo || !s || (lc && (!lc_n || lc_cap < 0))) return fail(ctx, GEV_ERR_ARG, "null argument");
+    bool lc_overflow = false;
+    const int rc = guarded(ctx, [&](gev::CtxBase &c) {
         const gev_cosmo &cm = *cosmo;
         const int N = c.cfg.N;
         const double dx = 1.0 / N;
@@ -1123,6 +1129,14 @@ int gev_step(gev_ctx *ctx, const gev_cosmo *cosmo, gev_state *s)
         c.solve_chi(2. * cm.fourpiG * dx * dx / a, s->cycle == 0, H, s->dtau, s->dtau_old, a * a * s->dtau_old);
         // B elliptic with the new phi (main.cu:836-955): T0i completed in solve_B's x pass
         if (elliptic) c.solve_B(cm.fourpiG * dx * dx, 0.);
+        // lightcone shell with this cycle's phi (main.cu:1040-1100)
+        if (lc) {
+            try {
+                c.lightcone(*lc, s->tau, s->dtau, s->dtau_old, a, a * H, lc_cap, nullptr, nullptr, nullptr, lc_n);
+            } catch (const gev::CapacityError &) {
+                lc_overflow = true;
+            }
+        }
         // kick, background half step, drift, background half step (main.cu:1225-1283)
         gev::KickDriftParams kp{};
         kp.do_kick = 1; kp.do_drift = 1; kp.do_bin = 1;
@@ -1146,6 +1160,20 @@ int gev_step(gev_ctx *ctx, const gev_cosmo *cosmo, gev_state *s)
         s->a = a;
         s->cycle++;
     });
+    if (rc == GEV_OK && lc_overflow)
+        return fail(ctx, GEV_ERR_CAPACITY, "lightcone output exceeds the buffer capacity (n_out holds the required size)");
+    return rc;
+}
+
+}  // namespace
+
+int gev_step(gev_ctx *ctx, const gev_cosmo *cosmo, gev_state *s) { return step_cycle(ctx, cosmo, s, nullptr, 0, nullptr); }
+
+int gev_step_lightcone(gev_ctx *ctx, const gev_cosmo *cosmo, gev_state *s, const gev_lightcone_args *lc,
+                       int64_t capacity, int64_t *n_out)
+{
+    if (!lc) return fail(ctx, GEV_ERR_ARG, "null argument");
+    return step_cycle(ctx, cosmo, s, lc, capacity, n_out);
 }
 
 int gev_synchronize(gev_ctx *ctx)

@@ -94,6 +94,8 @@ _pk = _sig("gev_power_spectrum", [_p, _i, _d, _p, _p, _p, _p, _p])
 _lc = _sig("gev_lightcone", [_p, ctypes.POINTER(LightconeArgs), _d, _d, _d, _d, _d, _l, _p, _p, _p, ctypes.POINTER(_l)])
 _lcf = _sig("gev_lightcone_fetch", [_p, _l, _p, _p, _p, ctypes.POINTER(_l)])
 _step = _sig("gev_step", [_p, ctypes.POINTER(Cosmo), ctypes.POINTER(State)])
+_step_lc = _sig("gev_step_lightcone", [_p, ctypes.POINTER(Cosmo), ctypes.POINTER(State), ctypes.POINTER(LightconeArgs),
+                                      _l, ctypes.POINTER(_l)])
 _sync = _sig("gev_synchronize", [_p])
 _stream = _sig("gev_stream", [_p], _p)
 _launches = _sig("gev_kernel_launches", [_p], _l)
@@ -283,6 +285,14 @@ class Context:
     def step(self, cosmo, state):
         self._ck(_step(self._h, ctypes.byref(cosmo), ctypes.byref(state)))
         return state
+
+    def step_lightcone(self, cosmo, state, args, capacity):
+        """gev_step with the lightcone shell between the solves and the kick;
+        returns the number of selected particles (left on the device)."""
+        n = _l()
+        self._ck(_step_lc(self._h, ctypes.byref(cosmo), ctypes.byref(state), ctypes.byref(args), int(capacity),
+                          ctypes.byref(n)))
+        return n.value
 
     def ics_zeldovich(self, boxsize, a, fourpiG, omega_m, omega_l, pk_k, pk_p, seed=0, omega_rad=0.0,
                       ksphere=False, gr=True, noise=None, return_noise=False):

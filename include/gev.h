@@ -198,9 +198,10 @@ int gev_lightcone_fetch(gev_ctx *ctx, int64_t capacity, float *pos, float *vel, 
                         int64_t *n_out);
 
 /* One full cycle of main.cu:608-1317 for CDM in the weak-field GR gauge:
- * T00 and Tij projections, Phi, chi (and h_ij), T0i projection and B_i,
- * lightcone shells, kick, background half steps, drift, step control.  The
- * caller's state struct is advanced in place. */
+ * T00 and Tij projections, Phi, chi (and h_ij), T0i projection and B_i, kick,
+ * background half steps, drift, step control (gev_step_lightcone adds the
+ * lightcone shell between the solves and the kick).  The caller's state
+ * struct is advanced in place. */
 typedef struct {
     double Omega_m, Omega_Lambda, Omega_rad;
     double fourpiG;        /* 1.5 L^2 / c^2 (main.cu:418) */
@@ -216,6 +217,15 @@ typedef struct {
 } gev_state;
 
 int gev_step(gev_ctx *ctx, const gev_cosmo *cosmo, gev_state *st);
+/* gev_step with one lightcone shell written where main.cu writes it: after
+ * the field solves and before the kick (writeLightcones, main.cu:1040-1100),
+ * with this cycle's phi, a, tau, dtau, dtau_old and dadtau = a Hconf(a).  The
+ * selected particles stay in the context's device buffer of `capacity` slots
+ * (gev_lightcone_fetch); n_out receives their number.  If they do not fit, the
+ * cycle still completes and the call returns GEV_ERR_CAPACITY with n_out the
+ * size needed. */
+int gev_step_lightcone(gev_ctx *ctx, const gev_cosmo *cosmo, gev_state *st, const gev_lightcone_args *lc,
+                       int64_t capacity, int64_t *n_out);
 
 /* Background (background.hpp:200-207, :235-244, :268-291). */
 double gev_hconf(double a, double fourpiG, const gev_cosmo *cosmo);

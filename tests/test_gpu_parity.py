@@ -489,6 +489,51 @@ def test_lightcone_selection_and_backlog(prec):
 
 
 @pytest.mark.parametrize("prec", PRECS)
+def test_step_lightcone_between_solves_and_kick(prec):
+    """gev_step_lightcone: the same cycle as gev_step (bitwise), and a shell
+    equal to gev_lightcone on the pre-step particles with the post-solve phi
+    (the kick does not change phi, the projections do not move particles)."""
+    import ctypes
+    N = 32
+    pos, q, ids = particles(N, n=40000, seed=41, qscale=2e-3)
+    fourpiG = 1.5 * 320.0 ** 2 / 2997.92458 ** 2
+    cosmo = gev.Cosmo(0.32, 0.68, 0.0, fourpiG, 48.0, 0.04, 30.0, 320.0)
+    a0 = 1.0 / 11
+    H = gev.hconf(a0, fourpiG, ctypes.byref(cosmo))
+    dtau0 = min(48.0 / N, 0.04 / H)
+    tau0 = gev.particle_horizon(a0, fourpiG, ctypes.byref(cosmo))
+    lc = gev.LightconeArgs((0.5, 0.5, 0.5), (0.0, 0.0, 1.0), -1.0, (0.5, 0.2), tau0 + 0.3, 1, 0)
+    phi0 = trough_phi(N, 1e-6)
+    cap = len(pos)
+
+    def fresh():
+        c = make_ctx(N, prec, len(pos))
+        c.set_particles(pos, q, ids, MASS)
+        c.set_field(gev.FIELD_PHI, phi0)
+        return c, gev.State(a0, tau0, dtau0, 0.5 * dtau0, 1, 0, 0, 0)
+
+    ca, sa = fresh()
+    n = ca.step_lightcone(cosmo, sa, lc, cap)
+    assert n > 100
+    lp, lv, li = ca.lightcone_fetch(cap)
+    cb, sb = fresh()
+    cb.step(cosmo, sb)
+    for x, y in zip(ca.get_particles(), cb.get_particles()):
+        assert np.array_equal(x, y)
+    assert np.array_equal(ca.get_field(gev.FIELD_PHI), cb.get_field(gev.FIELD_PHI))
+    assert (sa.a, sa.tau, sa.dtau, sa.maxvel) == (sb.a, sb.tau, sb.dtau, sb.maxvel)
+    phi1 = cb.get_field(gev.FIELD_PHI)
+    cb.close()
+    cc, sc = fresh()
+    cc.set_field(gev.FIELD_PHI, phi1)
+    p2, v2, i2 = cc.lightcone(lc, tau0, dtau0, 0.5 * dtau0, a0, a0 * H, cap)
+    o1, o2 = np.argsort(li), np.argsort(i2)
+    assert np.array_equal(li[o1], i2[o2])
+    assert np.array_equal(lp[o1], p2[o2]) and np.array_equal(lv[o1], v2[o2])
+    ca.close(); cc.close()
+
+
+@pytest.mark.parametrize("prec", PRECS)
 def test_step_matches_oracle(prec):
     """Three full cycles of main.cu's loop against the oracle's orc_step."""
     import ctypes
