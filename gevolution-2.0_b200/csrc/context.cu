@@ -818,21 +818,22 @@ template <class R> struct Ctx final : CtxBase {
         }
     }
 
-    void lightcone(const gev_lightcone_args &lc, double tau, double dtau, double dtau_old, double a, double dadtau,
-                   int64_t cap, float *pos, float *vel, int64_t *ids, int64_t *n_out) override
+    // The shell's kernel arguments and output buffers for this cycle; false when
+    // the shell writes nothing this cycle (output.hpp:2093), with the backlog
+    // cleared as the reference does (output.hpp:2172).
+    bool lightcone_setup(const gev_lightcone_args &lc, double tau, double dtau, double dtau_old, double a,
+                         double dadtau, int64_t cap, LcKernelArgs &la, LcOut &lo)
     {
         need_particles();
         if (lc.shell < 0 || lc.shell >= 8) throw ArgError("lightcone shell slot must be 0..7");
         const int s = lc.shell;
         const double dist = lc.d - tau;
-        *n_out = 0;
-        // output condition, output.hpp:2093
         if (!(lc.distance[0] > dist + 0.5 * dtau_old && lc.distance[1] <= dist + 0.5 * dtau_old && dist + 0.5 * dtau_old > 0.)) {
-            backlog_valid[s] = false;   // the reference clears the backlog every cycle (output.hpp:2172)
+            backlog_valid[s] = false;
             lc_last = 0;
-            return;
+            return false;
         }
-        LcKernelArgs la{};
+        la = LcKernelArgs{};
         const int N = g.N;
         double domain[6];
         for (int i = 0; i < 3; i++) { domain[i] = -0.5 / N; domain[i + 3] = (N + 0.5) / N; }   // output.hpp:1174-1186
@@ -864,17 +865,35 @@ template <class R> struct Ctx final : CtxBase {
         la.capacity = lcap;
         if ((int64_t)lc_id.n < lcap) { lc_pos.alloc(3 * lcap, "lightcone"); lc_vel.alloc(3 * lcap, "lightcone"); lc_id.alloc(lcap, "lightcone"); }
         ck(cudaMemsetAsync(u64.p + 1, 0, sizeof(unsigned long long), st), "memset");
-        launch_lightcone<R>(cur(), bstart.p, N, phi.p, la, lc_pos.p, lc_vel.p, lc_id.p, u64.p + 1, newer, idset_cap, derr.p, st);
-        launched("lightcone");
-        // the IDs logged near the inner edge become the next cycle's backlog
-        idset_cur[s] = 1 - idset_cur[s];
-        backlog_valid[s] = true;
+        lo = LcOut{lc_pos.p, lc_vel.p, lc_id.p, u64.p + 1, newer, idset_cap};
+        return true;
+    }
+
+    // after the shell's kernel: the IDs logged near the inner edge become the
+    // next cycle's backlog; returns the number selected (synchronises)
+    int64_t lightcone_count(int shell)
+    {
+        idset_cur[shell] = 1 - idset_cur[shell];
+        backlog_valid[shell] = true;
         unsigned long long cnt = 0;
         ck(cudaMemcpyAsync(&cnt, u64.p + 1, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st), "D2H");
         sync();
-        *n_out = (int64_t)cnt;
         lc_last = (int64_t)cnt;
-        if ((int64_t)cnt > lcap) throw CapacityError("lightcone output exceeds the buffer capacity (n_out holds the required size)");
+        return (int64_t)cnt;
+    }
+
+    void lightcone(const gev_lightcone_args &lc, double tau, double dtau, double dtau_old, double a, double dadtau,
+                   int64_t cap, float *pos, float *vel, int64_t *ids, int64_t *n_out) override
+    {
+        *n_out = 0;
+        LcKernelArgs la;
+        LcOut lo;
+        if (!lightcone_setup(lc, tau, dtau, dtau_old, a, dadtau, cap, la, lo)) return;
+        launch_lightcone<R>(cur(), bstart.p, g.N, phi.p, la, lo.pos, lo.vel, lo.ids, lo.count, lo.newlog,
+                            lo.newlog_cap, derr.p, st);
+        launched("lightcone");
+        *n_out = lightcone_count(lc.shell);
+        if (*n_out > la.capacity) throw CapacityError("lightcone output exceeds the buffer capacity (n_out holds the required size)");
         if (pos || vel || ids) fetch_lightcone(cap, pos, vel, ids, n_out);
     }
 

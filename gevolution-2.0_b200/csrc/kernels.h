@@ -103,6 +103,13 @@ struct LcKernelArgs {
     int64_t backlog_cap;                 // power of two (0: empty)
     int64_t capacity;                    // output slots
 };
+// a shell's output buffers and ID log for one cycle
+struct LcOut {
+    float *pos, *vel;
+    int64_t *ids;
+    unsigned long long *count, *newlog;
+    int64_t newlog_cap;
+};
 constexpr unsigned long long LC_EMPTY = ~0ull;   // free slot of an ID set (tables are filled with 0xff bytes)
 constexpr int64_t LC_MAX_PROBES = 4096;          // bound on linear probing (load factor stays below 1/4)
 template <class R>
