@@ -102,6 +102,23 @@ __host__ __device__ __forceinline__ uint32_t bucket_of_cell(int N, int nt, int x
     return tile * 8u + cls;
 }
 
+// Raises a kernel's dynamic shared-memory limit once per device: the attribute
+// belongs to the current device, so a process with contexts on several GPUs
+// sets it on each.  done: the call site's flags, one per device ordinal.
+constexpr int SMEM_ATTR_DEVICES = 64;
+template <class K> inline void raise_smem_limit(K kernel, size_t bytes, bool (&done)[SMEM_ATTR_DEVICES])
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= SMEM_ATTR_DEVICES) {
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        return;
+    }
+    if (!done[dev]) {
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        done[dev] = true;
+    }
+}
+
 // x-pass load modes (fused source preparation)
 enum { FX_COPY = 0, FX_PREP_T00 = 1, FX_PREP_TIJ = 2, FX_PREP_T0I = 3 };
 // z-pass Fourier-space operators

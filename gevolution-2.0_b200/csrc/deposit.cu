@@ -633,11 +633,8 @@ static void launch_k(const PView<R> &p, const uint32_t *bstart, int N, const R *
                      double m00, double mij, double m0i, int accumulate, int *err, cudaStream_t st)
 {
     constexpr size_t smem = dep_smem_bytes<R, KIND>();
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_deposit<R, KIND, USE_PHI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_set = true;
-    }
+    static bool attr_set[SMEM_ATTR_DEVICES] = {};
+    raise_smem_limit(k_deposit<R, KIND, USE_PHI>, smem, attr_set);
     const int nt = N / 8;
     const unsigned grid = (unsigned)nt * nt * nt;
     k_deposit<R, KIND, USE_PHI><<<grid, DEP_NT, smem, st>>>(p, bstart, N, nt, phi, out, a, m00, mij, m0i, accumulate, err,

@@ -293,11 +293,8 @@ void launch_kick_drift(const PView<R> &p, const uint32_t *bstart, int N, const R
 {
     int nt = N / 8;
     const size_t smem = 5 * KD_W * KD_W * KD_W * sizeof(R);
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_kick_drift<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_set = true;
-    }
+    static bool attr_set[SMEM_ATTR_DEVICES] = {};
+    raise_smem_limit(k_kick_drift<R>, smem, attr_set);
     k_kick_drift<R><<<(unsigned)nt * nt * nt, KD_NT, smem, st>>>(p, bstart, N, nt, phi, chi, Bi, n3, kp, counts,
                                                                 bucket, rank, vmax_bits, err, FastDiv((uint32_t)N));
 }
@@ -600,11 +597,8 @@ void launch_rebin(const PView<R> &src, PView<R> dst, const uint32_t *bstart, con
 {
     if (src.n <= 0) return;
     k_scatter_index<<<cdiv(src.n, 256), 256, 0, st>>>(bstart, bucket, rank, src.n, inv);
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_rebin_tile<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rb_smem_bytes<R>());
-        attr_set = true;
-    }
+    static bool attr_set[SMEM_ATTR_DEVICES] = {};
+    raise_smem_limit(k_rebin_tile<R>, rb_smem_bytes<R>(), attr_set);
     const int nt = N / 8;
     k_rebin_tile<R><<<(unsigned)nt * nt * nt, RB_NT, rb_smem_bytes<R>(), st>>>(src, dst, bstart, inv, nt, err,
                                                                     FastDiv((uint32_t)N));
