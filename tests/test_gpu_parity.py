@@ -408,6 +408,40 @@ def test_rebin_order(prec):
 
 
 @pytest.mark.parametrize("prec", PRECS)
+def test_empty_and_invalid_particle_input(prec):
+    """No particles: every projection is zero and the cycle runs; a context
+    without particles refuses to project; a non-finite coordinate surfaces as
+    a device error at the next synchronising call (the load kernel checks it
+    and substitutes 0); more particles than the capacity are refused."""
+    import ctypes
+    N = 16
+    with make_ctx(N, prec, 1000) as c:
+        with pytest.raises(gev.GevError):
+            c.project(gev.PROJ_T00, 0.5, 1.0, False)
+        e = np.zeros((0, 3))
+        c.set_particles(e, e, np.zeros(0, dtype=np.int64), MASS)
+        c.set_field(gev.FIELD_PHI, trough_phi(N))
+        c.project(gev.PROJ_T00 | gev.PROJ_TIJ | gev.PROJ_T0I_SUMS, 0.5, 1.0, True)
+        assert not c.get_field(gev.FIELD_SOURCE).any() and not c.get_field(gev.FIELD_SIJ).any()
+        fourpiG = 1.5 * 160.0 ** 2 / 2997.92458 ** 2
+        cosmo = gev.Cosmo(0.32, 0.68, 0.0, fourpiG, 48.0, 0.04, 30.0, 160.0)
+        st = gev.State(0.1, 1.0, 0.05, 0.05, 1, 0, 0, 0)
+        c.step(cosmo, st)
+        assert c.get_particles()[0].shape == (0, 3)
+        pos, q, ids = particles(N, n=200, seed=51)
+        bad = pos.copy()
+        bad[17, 1] = np.nan
+        with pytest.raises(gev.GevError, match="non-finite"):
+            c.set_particles(bad, q, ids, MASS)
+        big = np.zeros((1001, 3))
+        with pytest.raises(gev.GevError):
+            c.set_particles(big, big, np.arange(1001, dtype=np.int64), MASS)
+        c.set_particles(pos, q, ids, MASS)   # the context stays usable
+        c.project(gev.PROJ_CIC, 1.0, 1.0, False)
+        assert abs(c.get_field(gev.FIELD_SOURCE).sum() / (MASS * 200 * N ** 3) - 1) < 1e-6
+
+
+@pytest.mark.parametrize("prec", PRECS)
 def test_power_spectrum(prec):
     N = 32
     pos, q, ids = particles(N, seed=11, lattice=True, disp=0.4)
