@@ -12,7 +12,7 @@ Phi, chi, T0i projection, B, lightcone, kick, drift, background, step control.
 
 Metric: Mpart-steps/s = particles x cycles / second (whole job: all ranks).
 Multi-GPU (torchrun): every rank evolves its own independent box (replicas;
-the single-box cycle has no data-parallel split in this build) -> weak scaling.
+the single-box cycle is not split across GPUs) -> weak scaling.
 
 --impl reference times the CPU restatement of the reference cycle (the oracle,
 OpenMP over all host cores) on a bounded sample of the same physics.

@@ -330,7 +330,7 @@ int gev_snapshot_gadget2(gev_ctx *ctx, const char *path, const gev_gadget2_heade
  * method and tensor flag with enough capacity; the precision may differ.  The
  * reference's GPU build stops at its hibernation points instead of writing a
  * checkpoint (main.cu:1288-1303; the CPU build's writer is hibernation.hpp),
- * so this is the restart path of this build. */
+ * so this is the restart path of this library. */
 int gev_checkpoint_write(gev_ctx *ctx, const char *path, const gev_state *st);
 int gev_checkpoint_read(gev_ctx *ctx, const char *path, gev_state *st);
 
