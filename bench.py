@@ -70,15 +70,18 @@ class Clocks:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
+    # started before the warm-up so that the sampler is running when the timed
+    # region begins; samples are kept by their arrival time within the region
     def __init__(self, gpu_index):
         self.idx = gpu_index
         self.proc = None
         self.lines = []
+        self.t0 = self.t1 = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                                          "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except (OSError, ValueError):
@@ -86,19 +89,30 @@ class Clocks:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def begin(self):
+        self.t0 = time.time()
+
+    def end(self):
+        self.t1 = time.time()
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.1)   # let the sample taken at the end of the region arrive
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
+        t0 = self.t0 if self.t0 is not None else 0.0
+        t1 = (self.t1 if self.t1 is not None else time.time()) + 0.06
         sm, mx, reasons = [], None, set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for ln in self.lines:
+        for ts, ln in list(self.lines):
+            if ts < t0 or ts > t1:
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -225,22 +239,24 @@ def run_gpu(args, rank, world, local_rank):
         c = make(precision)
         st = gev.State(a0, tau0, dtau0, 0.0, 0, 0.0, 0.0, 0.0)
         stream = torch.cuda.ExternalStream(c.stream())
+        clocks = Clocks(local_rank)
+        clocks.start()
         log("warm-up")
         for _ in range(warmup):
             cycle(c, st)
         c.synchronize()
         log("timed cycles")
-        clocks = Clocks(local_rank)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
         torch.cuda.synchronize()
-        clocks.start()
+        clocks.begin()
         l0 = c.kernel_launches()
         e0.record(stream)
         for _ in range(steps):
             cycle(c, st)
         e1.record(stream)
         e1.synchronize()
+        clocks.end()
         launches = c.kernel_launches() - l0
         clk = clocks.stop()
         torch.cuda.synchronize()
