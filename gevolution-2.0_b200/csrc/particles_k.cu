@@ -184,28 +184,37 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
             const R ie = rsqrt_r(e2);
             e2 *= ie;   // sqrt(q^2 + a^2)
             if (kp.nfield_k >= 3) {
-                // gevolution.hpp:970-993
+                // gevolution.hpp:970-993.  The (d-1) B(-1) + (1-2d) B(0) + d B(1)
+                // terms, weighted over the other two axes, are evaluated as that
+                // combination of the bilinear interpolations I(-1), I(0), I(1)
+                // of the three planes (the same quantity, fewer operations).
+                const R wyz[4] = {(1 - d[1]) * (1 - d[2]), d[1] * (1 - d[2]), (1 - d[1]) * d[2], d[1] * d[2]};
+                const R wxz[4] = {(1 - d[0]) * (1 - d[2]), d[0] * (1 - d[2]), (1 - d[0]) * d[2], d[0] * d[2]};
+                const R wxy[4] = {(1 - d[0]) * (1 - d[1]), d[0] * (1 - d[1]), (1 - d[0]) * d[1], d[0] * d[1]};
+                auto I0 = [&](int x) {
+                    return wyz[0] * SF(B0, rx, ry, rz, x, 0, 0) + wyz[1] * SF(B0, rx, ry, rz, x, 1, 0) +
+                           wyz[2] * SF(B0, rx, ry, rz, x, 0, 1) + wyz[3] * SF(B0, rx, ry, rz, x, 1, 1);
+                };
+                auto I1 = [&](int y) {
+                    return wxz[0] * SF(B1, rx, ry, rz, 0, y, 0) + wxz[1] * SF(B1, rx, ry, rz, 1, y, 0) +
+                           wxz[2] * SF(B1, rx, ry, rz, 0, y, 1) + wxz[3] * SF(B1, rx, ry, rz, 1, y, 1);
+                };
+                auto I2 = [&](int z) {
+                    return wxy[0] * SF(B2, rx, ry, rz, 0, 0, z) + wxy[1] * SF(B2, rx, ry, rz, 1, 0, z) +
+                           wxy[2] * SF(B2, rx, ry, rz, 0, 1, z) + wxy[3] * SF(B2, rx, ry, rz, 1, 1, z);
+                };
                 R pg[3];
                 pg[0] = ((1 - d[2]) * (SF(B1, rx, ry, rz, 1, 0, 0) - SF(B1, rx, ry, rz, 0, 0, 0)) + d[2] * (SF(B1, rx, ry, rz, 1, 0, 1) - SF(B1, rx, ry, rz, 0, 0, 1))) * v[1];
                 pg[0] += ((1 - d[1]) * (SF(B2, rx, ry, rz, 1, 0, 0) - SF(B2, rx, ry, rz, 0, 0, 0)) + d[1] * (SF(B2, rx, ry, rz, 1, 1, 0) - SF(B2, rx, ry, rz, 0, 1, 0))) * v[2];
-                pg[0] += (1 - d[1]) * (1 - d[2]) * ((d[0] - 1) * SF(B0, rx, ry, rz, -1, 0, 0) + (1 - 2 * d[0]) * SF(B0, rx, ry, rz, 0, 0, 0) + d[0] * SF(B0, rx, ry, rz, 1, 0, 0)) * v[0];
-                pg[0] += d[1] * (1 - d[2]) * ((d[0] - 1) * SF(B0, rx, ry, rz, -1, 1, 0) + (1 - 2 * d[0]) * SF(B0, rx, ry, rz, 0, 1, 0) + d[0] * SF(B0, rx, ry, rz, 1, 1, 0)) * v[0];
-                pg[0] += (1 - d[1]) * d[2] * ((d[0] - 1) * SF(B0, rx, ry, rz, -1, 0, 1) + (1 - 2 * d[0]) * SF(B0, rx, ry, rz, 0, 0, 1) + d[0] * SF(B0, rx, ry, rz, 1, 0, 1)) * v[0];
-                pg[0] += d[1] * d[2] * ((d[0] - 1) * SF(B0, rx, ry, rz, -1, 1, 1) + (1 - 2 * d[0]) * SF(B0, rx, ry, rz, 0, 1, 1) + d[0] * SF(B0, rx, ry, rz, 1, 1, 1)) * v[0];
+                pg[0] += ((d[0] - 1) * I0(-1) + (1 - 2 * d[0]) * I0(0) + d[0] * I0(1)) * v[0];
 
                 pg[1] = ((1 - d[0]) * (SF(B2, rx, ry, rz, 0, 1, 0) - SF(B2, rx, ry, rz, 0, 0, 0)) + d[0] * (SF(B2, rx, ry, rz, 1, 1, 0) - SF(B2, rx, ry, rz, 1, 0, 0))) * v[2];
                 pg[1] += ((1 - d[2]) * (SF(B0, rx, ry, rz, 0, 1, 0) - SF(B0, rx, ry, rz, 0, 0, 0)) + d[2] * (SF(B0, rx, ry, rz, 0, 1, 1) - SF(B0, rx, ry, rz, 0, 0, 1))) * v[0];
-                pg[1] += (1 - d[0]) * (1 - d[2]) * ((d[1] - 1) * SF(B1, rx, ry, rz, 0, -1, 0) + (1 - 2 * d[1]) * SF(B1, rx, ry, rz, 0, 0, 0) + d[1] * SF(B1, rx, ry, rz, 0, 1, 0)) * v[1];
-                pg[1] += d[0] * (1 - d[2]) * ((d[1] - 1) * SF(B1, rx, ry, rz, 1, -1, 0) + (1 - 2 * d[1]) * SF(B1, rx, ry, rz, 1, 0, 0) + d[1] * SF(B1, rx, ry, rz, 1, 1, 0)) * v[1];
-                pg[1] += (1 - d[0]) * d[2] * ((d[1] - 1) * SF(B1, rx, ry, rz, 0, -1, 1) + (1 - 2 * d[1]) * SF(B1, rx, ry, rz, 0, 0, 1) + d[1] * SF(B1, rx, ry, rz, 0, 1, 1)) * v[1];
-                pg[1] += d[0] * d[2] * ((d[1] - 1) * SF(B1, rx, ry, rz, 1, -1, 1) + (1 - 2 * d[1]) * SF(B1, rx, ry, rz, 1, 0, 1) + d[1] * SF(B1, rx, ry, rz, 1, 1, 1)) * v[1];
+                pg[1] += ((d[1] - 1) * I1(-1) + (1 - 2 * d[1]) * I1(0) + d[1] * I1(1)) * v[1];
 
                 pg[2] = ((1 - d[1]) * (SF(B0, rx, ry, rz, 0, 0, 1) - SF(B0, rx, ry, rz, 0, 0, 0)) + d[1] * (SF(B0, rx, ry, rz, 0, 1, 1) - SF(B0, rx, ry, rz, 0, 1, 0))) * v[0];
                 pg[2] += ((1 - d[0]) * (SF(B1, rx, ry, rz, 0, 0, 1) - SF(B1, rx, ry, rz, 0, 0, 0)) + d[0] * (SF(B1, rx, ry, rz, 1, 0, 1) - SF(B1, rx, ry, rz, 1, 0, 0))) * v[1];
-                pg[2] += (1 - d[0]) * (1 - d[1]) * ((d[2] - 1) * SF(B2, rx, ry, rz, 0, 0, -1) + (1 - 2 * d[2]) * SF(B2, rx, ry, rz, 0, 0, 0) + d[2] * SF(B2, rx, ry, rz, 0, 0, 1)) * v[2];
-                pg[2] += d[0] * (1 - d[1]) * ((d[2] - 1) * SF(B2, rx, ry, rz, 1, 0, -1) + (1 - 2 * d[2]) * SF(B2, rx, ry, rz, 1, 0, 0) + d[2] * SF(B2, rx, ry, rz, 1, 0, 1)) * v[2];
-                pg[2] += (1 - d[0]) * d[1] * ((d[2] - 1) * SF(B2, rx, ry, rz, 0, 1, -1) + (1 - 2 * d[2]) * SF(B2, rx, ry, rz, 0, 1, 0) + d[2] * SF(B2, rx, ry, rz, 0, 1, 1)) * v[2];
-                pg[2] += d[0] * d[1] * ((d[2] - 1) * SF(B2, rx, ry, rz, 1, 1, -1) + (1 - 2 * d[2]) * SF(B2, rx, ry, rz, 1, 1, 0) + d[2] * SF(B2, rx, ry, rz, 1, 1, 1)) * v[2];
+                pg[2] += ((d[2] - 1) * I2(-1) + (1 - 2 * d[2]) * I2(0) + d[2] * I2(1)) * v[2];
 #pragma unroll
                 for (int c = 0; c < 3; c++) gradphi[c] += pg[c] * (ib_k * ie);
             }
