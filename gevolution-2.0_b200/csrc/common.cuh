@@ -74,14 +74,19 @@ struct FastDiv {
         while ((1ull << l) < div) l++;
         m = (uint32_t)((((1ull << l) - div) << 32) / div + 1);
     }
-    __device__ __forceinline__ uint32_t div(uint32_t n) const
+    __host__ __device__ __forceinline__ uint32_t div(uint32_t n) const
     {
-        return (uint32_t)(((uint64_t)__umulhi(m, n) + n) >> l);
+#ifdef __CUDA_ARCH__
+        const uint32_t hi = __umulhi(m, n);
+#else
+        const uint32_t hi = (uint32_t)(((uint64_t)m * n) >> 32);
+#endif
+        return (uint32_t)(((uint64_t)hi + n) >> l);
     }
 };
 
 // cell index x + N*(y + N*z) -> (x, y, z)
-__device__ __forceinline__ void decode_cell(uint32_t cell, const FastDiv &fN, int &x, int &y, int &z)
+__host__ __device__ __forceinline__ void decode_cell(uint32_t cell, const FastDiv &fN, int &x, int &y, int &z)
 {
     const uint32_t q = fN.div(cell);
     x = (int)(cell - q * fN.d);

@@ -1,9 +1,12 @@
-// Host-only check of the tile ordering the re-bin and the deposit rely on
-// (csrc/particles.cuh, csrc/common.cuh): class_ord is a bijection of the 512
-// tile-local cells onto 0..511, class-major in bucket order (the bucket of a
-// cell is 8 tile + class), and inside each class it follows the cell's
-// (z, y, x) order, i.e. its linear cell index.  Prints "ok" or the first
-// violation.
+// Host-only checks of index arithmetic the particle kernels rely on
+// (csrc/particles.cuh, csrc/common.cuh):
+//   * class_ord is a bijection of the 512 tile-local cells onto 0..511,
+//     class-major in bucket order (the bucket of a cell is 8 tile + class),
+//     and inside each class it follows the cell's linear index;
+//   * the multiply-shift division FastDiv and decode_cell give exact
+//     quotients for every cell index of every supported grid size, and
+//     FastDiv for 32-bit dividends across the whole range.
+// Prints "ok" or the first violation.
 #include <cstdio>
 
 #include "common.cuh"
@@ -32,6 +35,23 @@ int main()
             const bool key_less = ba < bb || (ba == bb && a < b);
             if (rank_less != key_less) { printf("order differs for cells %d and %d\n", a, b); return 1; }
         }
+    const int sizes[] = {16, 32, 64, 128, 256, 384, 512, 768};
+    for (int n : sizes) {
+        const FastDiv f((uint32_t)n);
+        const uint32_t n3 = (uint32_t)n * n * n;
+        for (uint32_t c = 0; c < n3; c++) {
+            int x, y, z;
+            decode_cell(c, f, x, y, z);
+            if ((uint32_t)x != c % n || (uint32_t)y != (c / n) % n || (uint32_t)z != c / ((uint32_t)n * n)) {
+                printf("decode_cell(%u) wrong for N = %d\n", c, n);
+                return 1;
+            }
+        }
+        for (uint64_t v = 0; v <= 0xffffffffull; v += 65521) {   // a prime stride over the 32-bit range
+            if (f.div((uint32_t)v) != (uint32_t)v / (uint32_t)n) { printf("div(%llu) wrong for N = %d\n", (unsigned long long)v, n); return 1; }
+        }
+        if (f.div(0xffffffffu) != 0xffffffffu / (uint32_t)n) { printf("div(max) wrong for N = %d\n", n); return 1; }
+    }
     printf("ok\n");
     return 0;
 }
