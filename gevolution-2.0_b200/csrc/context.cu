@@ -445,7 +445,7 @@ template <class R> struct Ctx final : CtxBase {
         // 2. displacement field into the B_i planes
         const FftTables<R> tb = tables();
         fx_forward<R>(N, FX_COPY, source.p, g.n3, 1, 0, nullptr, nullptr, 0, 0, 0, 0, W.p, g.nk, nullptr, tb, st);
-        fy_pass<R>(N, -1, W.p, g.nk, 1, tb, st);
+        fy_pass<R>(N, -1, W.p, g.nk, 1, derr.p, tb, st);
         FzParams fz{};
         fz.op = OP_ZELD;
         fz.p0 = ip.boxsize;
@@ -454,7 +454,7 @@ template <class R> struct Ctx final : CtxBase {
         fz.ntab = ip.n_pk;
         fz.err = derr.p;
         fz_pass<R>(N, fz, W.p, g.nk, nullptr, nullptr, nullptr, tb, st);
-        fy_pass<R>(N, 1, W.p, g.nk, 3, tb, st);
+        fy_pass<R>(N, 1, W.p, g.nk, 3, derr.p, tb, st);
         fx_inverse<R>(N, W.p, g.nk, Bi.p, g.n3, 3, tb, st);
         launched("ics displacement", 5);
         // 3. the displaced lattice (part_simple_info.mass = Omega_m / Np, ic_basic.hpp:2198-2201)
@@ -471,7 +471,7 @@ template <class R> struct Ctx final : CtxBase {
         gev_cosmo cm{ip.Omega_m, ip.Omega_Lambda, ip.Omega_rad, ip.fourpiG, 0.0, 0.0, 0.0, ip.boxsize};
         const double H = hconf(ip.a, ip.fourpiG, cm);
         fx_forward<R>(N, FX_COPY, source.p, g.n3, 1, 0, nullptr, nullptr, 0, 0, 0, 0, W.p, g.nk, nullptr, tb, st);
-        fy_pass<R>(N, -1, W.p, g.nk, 1, tb, st);
+        fy_pass<R>(N, -1, W.p, g.nk, 1, derr.p, tb, st);
         FzParams fp{};
         fp.op = OP_POISSON;
         fp.p0 = (ip.fourpiG / ip.a) / -((double)N * (double)N * (double)N);
@@ -479,7 +479,7 @@ template <class R> struct Ctx final : CtxBase {
         fp.p2 = 1.0;   // remove the k = 0 mode
         fp.err = derr.p;
         fz_pass<R>(N, fp, W.p, g.nk, nullptr, nullptr, nullptr, tb, st);
-        fy_pass<R>(N, 1, W.p, g.nk, 1, tb, st);
+        fy_pass<R>(N, 1, W.p, g.nk, 1, derr.p, tb, st);
         fx_inverse<R>(N, W.p, g.nk, phi.p, g.n3, 1, tb, st);
         launched("ics phi", 5);
         // 5. momenta (ic_basic.hpp:2431-2437; Omega_m(a), Omega_rad(a): background.hpp:211-213)
@@ -671,7 +671,7 @@ template <class R> struct Ctx final : CtxBase {
             launch_reduce_sum(partial.p, (int64_t)(N / fx_rows_per_block(N, sizeof(R) == 8)) * N, scal.p, st);
             launched("reduce");
         }
-        fy_pass<R>(N, -1, W.p, g.nk, 1, tb, st);
+        fy_pass<R>(N, -1, W.p, g.nk, 1, derr.p, tb, st);
         launched("fy forward (phi)");
         FzParams fp{};
         fp.err = derr.p;
@@ -681,7 +681,7 @@ template <class R> struct Ctx final : CtxBase {
         fp.phi_hom = scal.p + 1;
         fz_pass<R>(N, fp, W.p, g.nk, nullptr, nullptr, nullptr, tb, st);
         launched("fz Poisson");
-        fy_pass<R>(N, 1, W.p, g.nk, 1, tb, st);
+        fy_pass<R>(N, 1, W.p, g.nk, 1, derr.p, tb, st);
         launched("fy inverse (phi)");
         fx_inverse<R>(N, W.p, g.nk, phi.p, g.n3, 1, tb, st);
         launched("fx inverse (phi)");
@@ -700,7 +700,7 @@ template <class R> struct Ctx final : CtxBase {
         const FftTables<R> tb = tables();
         fx_forward<R>(N, FX_PREP_TIJ, Sij.p, g.n3, 6, 0, phi.p, chi.p, 0, coeff, 0, 0, W.p, g.nk, nullptr, tb, st);
         launched("fx forward (Sij)");
-        fy_pass<R>(N, -1, W.p, g.nk, 6, tb, st);
+        fy_pass<R>(N, -1, W.p, g.nk, 6, derr.p, tb, st);
         launched("fy forward (Sij)");
         FzParams fp{};
         fp.err = derr.p;
@@ -713,7 +713,7 @@ template <class R> struct Ctx final : CtxBase {
         fz_pass<R>(N, fp, W.p, g.nk, hij.p, hijp.p, bstate.p, tb, st);
         launched("fz scalar projection");
         const int nout = parab ? 4 : 1;
-        fy_pass<R>(N, 1, W.p, g.nk, nout, tb, st);
+        fy_pass<R>(N, 1, W.p, g.nk, nout, derr.p, tb, st);
         launched("fy inverse (chi)");
         fx_inverse<R>(N, W.p, g.nk, chi.p, g.n3, 1, tb, st);
         launched("fx inverse (chi)");
@@ -735,7 +735,7 @@ template <class R> struct Ctx final : CtxBase {
                       nullptr, tb, st);
         launched("fx forward (T0i)");
         bi_sums = false;
-        fy_pass<R>(N, -1, W.p, g.nk, 3, tb, st);
+        fy_pass<R>(N, -1, W.p, g.nk, 3, derr.p, tb, st);
         launched("fy forward (T0i)");
         FzParams fp{};
         fp.err = derr.p;
@@ -744,7 +744,7 @@ template <class R> struct Ctx final : CtxBase {
         fp.p1 = modif;
         fz_pass<R>(N, fp, W.p, g.nk, nullptr, nullptr, nullptr, tb, st);
         launched("fz vector projection");
-        fy_pass<R>(N, 1, W.p, g.nk, 3, tb, st);
+        fy_pass<R>(N, 1, W.p, g.nk, 3, derr.p, tb, st);
         launched("fy inverse (B)");
         fx_inverse<R>(N, W.p, g.nk, Bi.p, g.n3, 3, tb, st);
         launched("fx inverse (B)");
@@ -781,7 +781,7 @@ template <class R> struct Ctx final : CtxBase {
         const FftTables<R> tb = tables();
         fx_forward<R>(N, FX_COPY, source.p, g.n3, 1, 0, nullptr, nullptr, 0, 0, 0, 0, W.p, g.nk, nullptr, tb, st);
         launched("fx forward (CIC)");
-        fy_pass<R>(N, -1, W.p, g.nk, 1, tb, st);
+        fy_pass<R>(N, -1, W.p, g.nk, 1, derr.p, tb, st);
         launched("fy forward (CIC)");
         if ((int)occ.n < nb) { bins.alloc(4 * nb, "bins"); occ.alloc(nb, "bins"); }
         ck(cudaMemsetAsync(bins.p, 0, 4 * nb * sizeof(double), st), "memset");

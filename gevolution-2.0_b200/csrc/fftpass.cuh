@@ -830,7 +830,7 @@ __global__ void __launch_bounds__(NT, (FzMinBlocks<R, OP, EXTRA, NT>::v))
 // in place.  grid (ceil(P/T), N, ncomp)
 template <class R, int N, int T, int NT, int S>
 __global__ void __launch_bounds__(NT, (sizeof(R) == 4 ? GEV_FY_MINB : 2) * 512 / NT) k_fy_tma(const typename CT<R>::C *__restrict__ tw,
-                                                        const __grid_constant__ CUtensorMap tmap)
+                                                        int *err, const __grid_constant__ CUtensorMap tmap)
 {
     using C = typename CT<R>::C;
     constexpr int YB = ZBox<N>::ZB, NYB = ZBox<N>::NZB;
@@ -846,7 +846,10 @@ __global__ void __launch_bounds__(NT, (sizeof(R) == 4 ? GEV_FY_MINB : 2) * 512 /
         for (int yc = 0; yc < NYB; yc++) tma_load_4d(buf + yc * YB * T, &tmap, 2 * kx0, yc * YB, z, comp, &bar);
     }
     const bool ok = mbar_wait(&bar, 0);
-    if (__syncthreads_or(!ok)) return;   // the data never arrived: leave the array untouched
+    if (__syncthreads_or(!ok)) {   // the data never arrived: leave the array untouched and say so
+        if (threadIdx.x == 0 && err) atomicOr(err, ERR_TMA_TIMEOUT);
+        return;
+    }
     fft_lines<N, S, T, NT>(buf, T, tw);
     fence_async_smem();
     __syncthreads();

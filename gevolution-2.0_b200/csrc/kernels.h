@@ -63,8 +63,8 @@ void fx_forward(int N, int mode, const R *in, int64_t in_stride, int ncomp, int 
                 double bg, double c, double c2, double c3, typename CT<R>::C *out, int64_t out_stride,
                 double *partial, const FftTables<R> &tb, cudaStream_t st);
 template <class R>
-void fy_pass(int N, int sign, typename CT<R>::C *data, int64_t stride, int ncomp, const FftTables<R> &tb,
-             cudaStream_t st);
+void fy_pass(int N, int sign, typename CT<R>::C *data, int64_t stride, int ncomp, int *err, const FftTables<R> &tb,
+             cudaStream_t st);   // err: device error word for the transfer timeout (may be null)
 template <class R>
 void fx_inverse(int N, const typename CT<R>::C *in, int64_t in_stride, R *out, int64_t out_stride, int ncomp,
                 const FftTables<R> &tb, cudaStream_t st);

@@ -269,6 +269,7 @@ template <class R> struct Pm final : PmBase {
     PBuf<double> k2;
     PBuf<double2> ks;
     PBuf<double> x, q, lx, lq;
+    PBuf<int> derr;                                        // device error word of the Fourier passes
     std::vector<std::unique_ptr<PBuf<double>>> ckx, ckq;   // checkpoints (x, q) before steps 0, k, 2k, ...
     std::vector<std::unique_ptr<PBuf<double>>> segx;       // x_n within the segment being reversed
     std::vector<std::unique_ptr<PBuf<R>>> segpsi;          // psi_n within the segment
@@ -289,6 +290,8 @@ template <class R> struct Pm final : PmBase {
         q.alloc(3 * np, "particles");
         lx.alloc(3 * np, "adjoint");
         lq.alloc(3 * np, "adjoint");
+        derr.alloc(1, "error word");
+        pck(cudaMemset(derr.p, 0, sizeof(int)), "memset");
         std::vector<C> tf(N), th(N / 2);
         for (int k = 0; k < N; k++) {
             const double ang = -2.0 * M_PI * (double)k / N;
@@ -322,6 +325,18 @@ template <class R> struct Pm final : PmBase {
     }
     cudaStream_t stream() override { return st; }
 
+    // after a synchronisation: a bulk tensor copy of a Fourier pass that timed
+    // out leaves its pencils untransformed and sets the error word
+    void check_device(const char *what)
+    {
+        int e = 0;
+        pck(cudaMemcpy(&e, derr.p, sizeof(int), cudaMemcpyDeviceToHost), "error word");
+        if (e) {
+            pck(cudaMemset(derr.p, 0, sizeof(int)), "memset");
+            throw PmError(GEV_ERR_DEVICE, std::string(what) + ": device error word (bulk tensor copy timed out)");
+        }
+    }
+
     unsigned pgrid() const { return (unsigned)std::min<int64_t>((np + PM_NT - 1) / PM_NT, 148 * 16); }
     unsigned fgrid() const { return (unsigned)std::min<int64_t>((n3 + PM_NT - 1) / PM_NT, 148 * 16); }
     FftTables<R> tables() const { return FftTables<R>{twf.p, twh.p, k2.p, ks.p}; }
@@ -331,13 +346,14 @@ template <class R> struct Pm final : PmBase {
     {
         const FftTables<R> tb = tables();
         fx_forward<R>(N, FX_COPY, f, n3, 1, 0, nullptr, nullptr, 0.0, 0.0, 0.0, 0.0, W.p, nk, nullptr, tb, st);
-        fy_pass<R>(N, -1, W.p, nk, 1, tb, st);
+        fy_pass<R>(N, -1, W.p, nk, 1, derr.p, tb, st);
         FzParams fp{};
         fp.op = OP_POISSON;
         fp.p0 = pc / -((double)N * (double)N * (double)N);
         fp.p1 = 0.0;
+        fp.err = derr.p;
         fz_pass<R>(N, fp, W.p, nk, nullptr, nullptr, nullptr, tb, st);
-        fy_pass<R>(N, 1, W.p, nk, 1, tb, st);
+        fy_pass<R>(N, 1, W.p, nk, 1, derr.p, tb, st);
         fx_inverse<R>(N, W.p, nk, f, n3, 1, tb, st);
     }
 
@@ -386,6 +402,7 @@ template <class R> struct Pm final : PmBase {
         if (qo) pck(cudaMemcpyAsync(qo, q.p, 3 * np * sizeof(double), cudaMemcpyDeviceToDevice, st), "copy q");
         pck(cudaGetLastError(), "forward launch");
         pck(cudaStreamSynchronize(st), "forward");
+        check_device("forward");
         have_forward = true;
     }
 
@@ -436,6 +453,7 @@ template <class R> struct Pm final : PmBase {
         pck(cudaMemcpyAsync(gq0, lq.p, 3 * np * sizeof(double), cudaMemcpyDeviceToDevice, st), "copy gq");
         pck(cudaGetLastError(), "adjoint launch");
         pck(cudaStreamSynchronize(st), "adjoint");
+        check_device("adjoint");
     }
 };
 

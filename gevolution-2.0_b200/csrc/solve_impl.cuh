@@ -112,7 +112,7 @@ void fx_forward(int N, int mode, const R *in, int64_t in_stride, int ncomp, int 
 }
 
 template <class R, int N, int S>
-void fy_n(typename CT<R>::C *data, int64_t stride, int ncomp, const FftTables<R> &tb, cudaStream_t st)
+void fy_n(typename CT<R>::C *data, int64_t stride, int ncomp, int *err, const FftTables<R> &tb, cudaStream_t st)
 {
     using C = typename CT<R>::C;
     constexpr int T = PassCfg<R>::TY, NT = PassCfg<R>::NTY;
@@ -121,7 +121,7 @@ void fy_n(typename CT<R>::C *data, int64_t stride, int ncomp, const FftTables<R>
     const CUtensorMap map = fourier_tensor_map<R>(data, N, stride, ncomp, T, ZBox<N>::ZB, 1);
     auto k = k_fy_tma<R, N, T, NT, S>;
     set_smem(k, smem);
-    k<<<dim3((N / 2 + 1 + T - 1) / T, N, ncomp), NT, smem, st>>>(tb.tw_full, map);
+    k<<<dim3((N / 2 + 1 + T - 1) / T, N, ncomp), NT, smem, st>>>(tb.tw_full, err, map);
 #else
     size_t smem = (size_t)N * (T + 1) * sizeof(C);
     auto k = k_fy<R, N, T, NT, S>;
@@ -131,11 +131,11 @@ void fy_n(typename CT<R>::C *data, int64_t stride, int ncomp, const FftTables<R>
 }
 
 template <class R>
-void fy_pass(int N, int sign, typename CT<R>::C *data, int64_t stride, int ncomp, const FftTables<R> &tb,
+void fy_pass(int N, int sign, typename CT<R>::C *data, int64_t stride, int ncomp, int *err, const FftTables<R> &tb,
              cudaStream_t st)
 {
-    if (sign < 0) { GEV_SWITCH_N(N, (fy_n<R, NN, -1>(data, stride, ncomp, tb, st))) }
-    else { GEV_SWITCH_N(N, (fy_n<R, NN, 1>(data, stride, ncomp, tb, st))) }
+    if (sign < 0) { GEV_SWITCH_N(N, (fy_n<R, NN, -1>(data, stride, ncomp, err, tb, st))) }
+    else { GEV_SWITCH_N(N, (fy_n<R, NN, 1>(data, stride, ncomp, err, tb, st))) }
 }
 
 template <class R, int N>
@@ -224,7 +224,7 @@ void fz_pass(int N, const FzParams &fp, typename CT<R>::C *data, int64_t stride,
 #define GEV_SOLVE_INST(R)                                                                                            \
     template void fx_forward<R>(int, int, const R *, int64_t, int, int, const R *, const R *, double, double, double, \
                                 double, CT<R>::C *, int64_t, double *, const FftTables<R> &, cudaStream_t);          \
-    template void fy_pass<R>(int, int, CT<R>::C *, int64_t, int, const FftTables<R> &, cudaStream_t);                \
+    template void fy_pass<R>(int, int, CT<R>::C *, int64_t, int, int *, const FftTables<R> &, cudaStream_t);                \
     template void fx_inverse<R>(int, const CT<R>::C *, int64_t, R *, int64_t, int, const FftTables<R> &,             \
                                 cudaStream_t);                                                                       \
     template void fz_pass<R>(int, const FzParams &, CT<R>::C *, int64_t, CT<R>::C *, CT<R>::C *, CT<R>::C *,          \

@@ -248,8 +248,14 @@ double gev_particle_horizon(double a, double fourpiG, const gev_cosmo *cosmo);
  *   - No part of the scratch has to start at zero.
  *   - All callers on one device share that scratch: calls whose work overlaps
  *     in time (unordered streams) race.  Order them on one stream.
- *   - The first call on each device looks up the scratch address (and may
- *     load the library's device code); make it before any stream capture. */
+ *   - The host needs the scratch's device address: the first call on each
+ *     device, and the first call after that device's context was destroyed
+ *     and re-created (cudaDeviceReset), looks it up (cudaGetSymbolAddress,
+ *     which may also load the library's device code); make that call before
+ *     any stream capture begins.
+ *   - A Fourier pass whose bulk tensor copy does not complete within its wait
+ *     limit leaves phi filled with NaN: the failure shows in the output, not
+ *     in the return code, which reports argument and launch errors only. */
 int gev_poisson_noalloc(int32_t N, int32_t precision, const void *source, void *phi,
                         double poisson_coeff, double modif, void *stream);
 

@@ -45,8 +45,28 @@ def smooth_field(N, seed, amp=1e-3, kmax=4):
     return np.ascontiguousarray((amp * f).ravel())
 
 
+def rfft3(f, N):
+    """Unnormalised forward R2C of a flat N^3 field (index x + N(y + Nz)) into
+    the half spectrum [kz][ky][kx] with kx <= N/2 -- the library's and the
+    oracle's convention, exp(-2 pi i k.x/N).  pocketfft through scipy.fft with
+    all host threads."""
+    import scipy.fft
+    return scipy.fft.rfftn(np.asarray(f, dtype=np.float64).reshape(N, N, N), workers=-1)
+
+
+def irfft3(F, N):
+    """Unnormalised C2R of a half spectrum [kz][ky][kx] into a flat N^3 field."""
+    import scipy.fft
+    return scipy.fft.irfftn(F, s=(N, N, N), norm="forward", workers=-1).ravel()
+
+
 def rel_err(a, b):
-    a = np.asarray(a, dtype=np.float64).ravel()
-    b = np.asarray(b, dtype=np.float64).ravel()
+    """max |a - b| / max |b|; complex arrays are compared by the modulus of
+    the complex difference (real and imaginary parts both count)."""
+    a = np.asarray(a).ravel()
+    b = np.asarray(b).ravel()
+    dt = np.complex128 if (np.iscomplexobj(a) or np.iscomplexobj(b)) else np.float64
+    a = a.astype(dt, copy=False)
+    b = b.astype(dt, copy=False)
     scale = max(np.abs(b).max(), 1e-300)
     return np.abs(a - b).max() / scale

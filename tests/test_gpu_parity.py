@@ -5,6 +5,8 @@ Tolerances: FP64 mode 1e-10 relative to the largest magnitude of the compared
 array (the oracle sums in a different order and uses its own FFT); mixed mode
 (FP32 fields and FFTs) 2e-5 for deposits and particle updates and 1e-4 for the
 FFT-based solves."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -567,57 +569,79 @@ def test_step_lightcone_between_solves_and_kick(prec):
     ca.close(); cc.close()
 
 
-@pytest.mark.parametrize("prec", PRECS)
-def test_step_matches_oracle(prec):
-    """Three full cycles of main.cu's loop against the oracle's orc_step."""
-    import ctypes
-    from _libs import _d, _i, _l  # noqa: F401
-    N = 32
+class _OSim(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int), ("boxsize", ctypes.c_double), ("fourpiG", ctypes.c_double),
+                ("mass", ctypes.c_double), ("Om", ctypes.c_double), ("OL", ctypes.c_double),
+                ("Orad", ctypes.c_double), ("z_relax", ctypes.c_double), ("Cf", ctypes.c_double),
+                ("steplimit", ctypes.c_double), ("with_B", ctypes.c_int)]
+
+
+class _OState(ctypes.Structure):
+    _fields_ = [("a", ctypes.c_double), ("tau", ctypes.c_double), ("dtau", ctypes.c_double),
+                ("dtau_old", ctypes.c_double), ("cycle", ctypes.c_int), ("T00hom", ctypes.c_double),
+                ("phi_hom", ctypes.c_double), ("maxvel", ctypes.c_double)]
+
+
+def _oracle_cycles(N, box, cycles, a0):
+    """orc_step (main.cu:608-1317 restated) from the perturbed-lattice fixture:
+    returns the inputs and the oracle's state, fields and particles after
+    `cycles` cycles."""
     pos, q, ids = particles(N, seed=12, lattice=True, disp=0.2, qscale=2e-4)
     mass = 0.32 / len(pos)
-    fourpiG = 1.5 * 320.0 ** 2 / 2997.92458 ** 2
-    phi = trough_phi(N, 1e-6)
-    chi = np.zeros(N ** 3)
-    Bi = np.zeros(3 * N ** 3)
+    fourpiG = 1.5 * box ** 2 / 2997.92458 ** 2
+    phi0 = trough_phi(N, 1e-6)
+    phi, chi, Bi = phi0.copy(), np.zeros(N ** 3), np.zeros(3 * N ** 3)
     o = oracle()
-
-    class OSim(ctypes.Structure):
-        _fields_ = [("N", ctypes.c_int), ("boxsize", ctypes.c_double), ("fourpiG", ctypes.c_double),
-                    ("mass", ctypes.c_double), ("Om", ctypes.c_double), ("OL", ctypes.c_double),
-                    ("Orad", ctypes.c_double), ("z_relax", ctypes.c_double), ("Cf", ctypes.c_double),
-                    ("steplimit", ctypes.c_double), ("with_B", ctypes.c_int)]
-
-    class OState(ctypes.Structure):
-        _fields_ = [("a", ctypes.c_double), ("tau", ctypes.c_double), ("dtau", ctypes.c_double),
-                    ("dtau_old", ctypes.c_double), ("cycle", ctypes.c_int), ("T00hom", ctypes.c_double),
-                    ("phi_hom", ctypes.c_double), ("maxvel", ctypes.c_double)]
-
-    o.lib.orc_step.argtypes = [ctypes.POINTER(OSim), ctypes.POINTER(OState), ctypes.c_int64] + [ctypes.c_void_p] * 5
+    o.lib.orc_step.argtypes = [ctypes.POINTER(_OSim), ctypes.POINTER(_OState), ctypes.c_int64] + [ctypes.c_void_p] * 5
     o.lib.orc_step.restype = None
-    sim = OSim(N, 320.0, fourpiG, mass, 0.32, 0.68, 0.0, 30.0, 48.0, 0.04, 1)
-    a0 = 1.0 / 51
-    cosmo = gev.Cosmo(0.32, 0.68, 0.0, fourpiG, 48.0, 0.04, 30.0, 320.0)
+    sim = _OSim(N, box, fourpiG, mass, 0.32, 0.68, 0.0, 30.0, 48.0, 0.04, 1)
+    cosmo = gev.Cosmo(0.32, 0.68, 0.0, fourpiG, 48.0, 0.04, 30.0, box)
     H = gev.hconf(a0, fourpiG, ctypes.byref(cosmo))
     dtau0 = min(48.0 / N, 0.04 / H)
-    ost = OState(a0, 0.1, dtau0, 0.0, 0, 0, 0, 0)
-    gst = gev.State(a0, 0.1, dtau0, 0.0, 0, 0, 0, 0)
+    ost = _OState(a0, 0.1, dtau0, 0.0, 0, 0, 0, 0)
     p_ref, q_ref = pos.copy(), q.copy()
-    with make_ctx(N, prec, len(pos)) as c:
-        c.set_particles(pos, q, ids, mass)
-        c.set_field(gev.FIELD_PHI, phi)
-        for _ in range(3):
-            o.lib.orc_step(ctypes.byref(sim), ctypes.byref(ost), len(pos), ptr(p_ref), ptr(q_ref), ptr(phi), ptr(chi), ptr(Bi))
-            c.step(cosmo, gst)
+    for _ in range(cycles):
+        o.lib.orc_step(ctypes.byref(sim), ctypes.byref(ost), len(pos), ptr(p_ref), ptr(q_ref), ptr(phi), ptr(chi), ptr(Bi))
+    return dict(pos=pos, q=q, ids=ids, mass=mass, phi0=phi0, cosmo=cosmo, a0=a0, dtau0=dtau0, ost=ost,
+                phi=phi, chi=chi, Bi=Bi, p_ref=p_ref, q_ref=q_ref)
+
+
+def _check_cycles(N, r, prec, cycles):
+    gst = gev.State(r["a0"], 0.1, r["dtau0"], 0.0, 0, 0, 0, 0)
+    ost = r["ost"]
+    with make_ctx(N, prec, len(r["pos"])) as c:
+        c.set_particles(r["pos"], r["q"], r["ids"], r["mass"])
+        c.set_field(gev.FIELD_PHI, r["phi0"])
+        for _ in range(cycles):
+            c.step(r["cosmo"], gst)
         assert abs(gst.a / ost.a - 1) < 1e-14
         assert abs(gst.maxvel / ost.maxvel - 1) < (1e-8 if prec == gev.FP64 else 1e-4)
         assert abs(gst.T00hom / ost.T00hom - 1) < (1e-10 if prec == gev.FP64 else 1e-6)
-        assert rel_err(c.get_field(gev.FIELD_PHI), phi) < (1e-8 if prec == gev.FP64 else 1e-3)
-        assert rel_err(c.get_field(gev.FIELD_CHI), chi) < (1e-6 if prec == gev.FP64 else 2e-2)
+        assert rel_err(c.get_field(gev.FIELD_PHI), r["phi"]) < (1e-8 if prec == gev.FP64 else 1e-3)
+        assert rel_err(c.get_field(gev.FIELD_CHI), r["chi"]) < (1e-6 if prec == gev.FP64 else 2e-2)
         # B_i from the T0i sums of the cycle's single deposit, completed with the new phi
-        assert rel_err(c.get_field(gev.FIELD_BI), Bi) < (1e-12 if prec == gev.FP64 else 1e-5)
+        assert rel_err(c.get_field(gev.FIELD_BI), r["Bi"]) < (1e-12 if prec == gev.FP64 else 1e-5)
         p2, q2, i2 = c.get_particles()
         order = np.argsort(i2)
-        d = p2[order] - p_ref
+        d = p2[order] - r["p_ref"]
         d -= np.round(d)
         assert np.abs(d).max() * N < (1e-8 if prec == gev.FP64 else 1e-4)
-        assert rel_err(q2[order], q_ref) < (1e-7 if prec == gev.FP64 else 1e-3)
+        assert rel_err(q2[order], r["q_ref"]) < (1e-7 if prec == gev.FP64 else 1e-3)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_step_matches_oracle(prec):
+    """Three full cycles of main.cu's loop against the oracle's orc_step."""
+    N = 32
+    _check_cycles(N, _oracle_cycles(N, 320.0, 3, 1.0 / 51), prec, 3)
+
+
+def test_step_matches_oracle_128():
+    """Two full cycles at 128^3 (2,097,152 particles, box 640 Mpc/h) against
+    orc_step, FP64 and mixed: the cycle's kernels at a size where every
+    deposit tile, re-bin bucket and Fourier pencil shape of the production
+    grids is exercised."""
+    N = 128
+    r = _oracle_cycles(N, 640.0, 2, 1.0 / 51)
+    for prec in PRECS:
+        _check_cycles(N, r, prec, 2)

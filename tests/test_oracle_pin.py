@@ -232,3 +232,24 @@ def test_find_intersecting_matches_reference(libs, opening):
         assert na == nb
         sa = sorted(map(tuple, va[:3 * na].reshape(-1, 3))); sb = sorted(map(tuple, vb[:3 * nb].reshape(-1, 3)))
         assert sa == sb
+
+
+def test_scipy_transforms_match_oracle_fft():
+    """rfft3 / irfft3 (pocketfft with threads, the large-N reference of the GPU
+    solver tests) agree with the oracle's own FFT in both directions."""
+    from _fixtures import irfft3, rfft3
+    o = oracle()
+    for N in (16, 24, 48):
+        f = np.random.default_rng(N).standard_normal(N ** 3)
+        FT = np.zeros(kshape(N), dtype=np.complex128)
+        o.r2c(N, ptr(f), ptr(FT))
+        assert rel_err(rfft3(f, N), FT) < 1e-13
+        back = np.zeros(N ** 3)
+        o.c2r(N, ptr(FT), ptr(back))
+        assert rel_err(irfft3(FT, N), back) < 1e-13
+
+
+def test_rel_err_sees_imaginary_parts():
+    a = np.array([1 + 1j, 2 - 1j])
+    assert rel_err(a, a) == 0
+    assert rel_err(a + 0.1j, a) > 0.04
