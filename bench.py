@@ -14,8 +14,11 @@ Metric: Mpart-steps/s = particles x cycles / second (whole job: all ranks).
 Multi-GPU (torchrun): every rank evolves its own independent box (replicas;
 the single-box cycle is not split across GPUs) -> weak scaling.
 
---impl reference times the CPU restatement of the reference cycle (the oracle,
-OpenMP over all host cores) on a bounded sample of the same physics.
+--impl reference times the reference's own cycle functions (ref_step in
+oracle/_ref: gevolution.hpp's projections, source preparation and Fourier
+solvers, update_q / update_pos and background.hpp's integrator, compiled for
+the host with a single-rank LATfield2 stand-in, OpenMP over all host cores) on
+a 128^3 sample box of the same physics and cell size.
 """
 import argparse
 import ctypes
@@ -58,7 +61,7 @@ def parse():
     p.add_argument("--adj-steps", type=int, default=32)
     p.add_argument("--adj-modes", type=int, default=64)
     p.add_argument("--cpu-sample-N", type=int, default=128)
-    p.add_argument("--cpu-sample-steps", type=int, default=2)
+    p.add_argument("--cpu-sample-steps", type=int, default=4)
     return p.parse_args()
 
 
@@ -216,7 +219,11 @@ def run_gpu(args, rank, world, local_rank):
     H = gev.hconf(a0, fourpiG, ctypes.byref(cosmo))
     dtau0 = min(48.0 / N, 0.04 / H)
     tau0 = gev.particle_horizon(a0, fourpiG, ctypes.byref(cosmo))
-    d_lc = tau0 + 0.75   # the shell's crossing surface sits at 0.75 box lengths during the timed cycles
+    # the crossing surface d - tau starts just inside the shell's outer limit (1.0
+    # box lengths) and moves inward by the conformal time of each cycle: over the
+    # warm-up and timed cycles from z = 100 (tau grows by about 2 % per cycle) it
+    # stays inside [0.5, 1.0], so every cycle writes a populated shell
+    d_lc = tau0 + 0.98
     lc = lightcone_args(gev, d_lc)
     lc_cap = int(0.2 * np_)
 
@@ -227,8 +234,9 @@ def run_gpu(args, rank, world, local_rank):
         return c
 
     def cycle(c, st):
-        """One cycle of main.cu's loop with the lightcone between the solves and the kick."""
-        c.step_lightcone(cosmo, st, lc, lc_cap)
+        """One cycle of main.cu's loop with the lightcone between the solves and
+        the kick; returns the number of particles the shell selected."""
+        return c.step_lightcone(cosmo, st, lc, lc_cap)
 
     def barrier():
         if world > 1:
@@ -251,9 +259,11 @@ def run_gpu(args, rank, world, local_rank):
         torch.cuda.synchronize()
         clocks.begin()
         l0 = c.kernel_launches()
+        counts = []
+        taus = [st.tau]
         e0.record(stream)
         for _ in range(steps):
-            cycle(c, st)
+            counts.append(cycle(c, st))
         e1.record(stream)
         e1.synchronize()
         clocks.end()
@@ -262,10 +272,11 @@ def run_gpu(args, rank, world, local_rank):
         torch.cuda.synchronize()
         barrier()
         ms = e0.elapsed_time(e1)
-        return c, st, ms, launches, clk, stream
+        taus.append(st.tau)
+        return c, st, ms, launches, clk, stream, (counts, taus)
 
     # ---- mixed precision: the headline ----
-    c, st, ms, launches, clk, stream = timed_run(gev.MIXED, args.steps, args.warmup)
+    c, st, ms, launches, clk, stream, (lc_counts, lc_taus) = timed_run(gev.MIXED, args.steps, args.warmup)
     ms_max = max_over_ranks(ms, world, dev)
     value = job_rate(world, np_, args.steps, ms_max)
 
@@ -316,7 +327,7 @@ def run_gpu(args, rank, world, local_rank):
     del c
     fp64 = None
     if not args.no_fp64:
-        c64, st64, ms64, _, _, _ = timed_run(gev.FP64, args.steps, args.warmup)
+        c64, st64, ms64, _, _, _, _ = timed_run(gev.FP64, args.steps, args.warmup)
         pk64 = c64.power_spectrum(1024)
         occ = pk64[4] > 0
         kb = pk64[0][occ]
@@ -394,6 +405,8 @@ def run_gpu(args, rank, world, local_rank):
             "config": workload_config(N, box, world),
             "gpu_launches": launches,
             "stage_ms": stages,
+            "lightcone_counts": lc_counts,
+            "lightcone_distance_box": [d_lc - lc_taus[0], d_lc - lc_taus[1]],
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": ncu_traffic(dom, N),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same kernel at 256^3 "
@@ -410,46 +423,104 @@ def run_gpu(args, rank, world, local_rank):
 
 
 # ---------------------------------------------------------------------------
-# CPU: the oracle cycle (OpenMP, all host cores) on a bounded sample
+# CPU: the reference's own cycle (oracle/_ref) on the host cores
 # ---------------------------------------------------------------------------
-def oracle_cycle_rate(Ns, steps, seed):
+def _load_ics_module():
+    """gevb200/ics.py by file path: the reference arm uses its numpy/torch IC
+    synthesis without importing the package (which loads the CUDA library)."""
+    import importlib.util
+    path = os.path.join(ROOT, "gevolution-2.0_b200", "python", "gevb200", "ics.py")
+    spec = importlib.util.spec_from_file_location("gev_ics_host", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def reference_cycle_rate(Ns, steps, warmup, seed, z_in=100.0):
+    """Time ref_step -- one cycle of main.cu:608-1317 composed from the
+    reference's own functors, Fourier solvers and background integrator,
+    compiled for the host by oracle/Makefile with the single-rank LATfield2
+    stand-in (OpenMP) -- on an Ns^3 box with 5 Mpc/h cells and Zel'dovich
+    initial conditions at z_in (synthesised on the host).  LATfield2's FFT is
+    stood in for by pocketfft (scipy.fft, all host threads).  Returns
+    (Mpart-steps/s, seconds of the timed cycles, threads) or None when the
+    reference build is absent."""
     import numpy as np
+    import scipy.fft
+    import torch
 
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from _libs import oracle, ptr
-    from _fixtures import particles, trough_phi
+    from _libs import ptr, ref
 
-    o = oracle()
+    r = ref()
+    if r is None:
+        return None
 
-    class OSim(ctypes.Structure):
+    class Sim(ctypes.Structure):   # orc_sim
         _fields_ = [("N", ctypes.c_int), ("boxsize", ctypes.c_double), ("fourpiG", ctypes.c_double),
                     ("mass", ctypes.c_double), ("Om", ctypes.c_double), ("OL", ctypes.c_double),
                     ("Orad", ctypes.c_double), ("z_relax", ctypes.c_double), ("Cf", ctypes.c_double),
                     ("steplimit", ctypes.c_double), ("with_B", ctypes.c_int)]
 
-    class OState(ctypes.Structure):
+    class State(ctypes.Structure):   # orc_state
         _fields_ = [("a", ctypes.c_double), ("tau", ctypes.c_double), ("dtau", ctypes.c_double),
                     ("dtau_old", ctypes.c_double), ("cycle", ctypes.c_int), ("T00hom", ctypes.c_double),
                     ("phi_hom", ctypes.c_double), ("maxvel", ctypes.c_double)]
 
-    o.lib.orc_step.argtypes = [ctypes.POINTER(OSim), ctypes.POINTER(OState), ctypes.c_int64] + [ctypes.c_void_p] * 5
-    o.lib.orc_step.restype = None
+    fft_t = ctypes.CFUNCTYPE(None, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p)
+    dptr = ctypes.POINTER(ctypes.c_double)
+
+    def r2c(N, pin, pout):
+        f = np.ctypeslib.as_array(ctypes.cast(pin, dptr), shape=(N, N, N))
+        o = np.ctypeslib.as_array(ctypes.cast(pout, dptr), shape=(N, N, N + 2)).view(np.complex128)
+        o[...] = scipy.fft.rfftn(f, workers=-1)
+
+    def c2r(N, pin, pout):
+        F = np.ctypeslib.as_array(ctypes.cast(pin, dptr), shape=(N, N, N + 2)).view(np.complex128)
+        o = np.ctypeslib.as_array(ctypes.cast(pout, dptr), shape=(N, N, N))
+        o[...] = scipy.fft.irfftn(F, s=(N, N, N), norm="forward", workers=-1)
+
+    cb = (fft_t(r2c), fft_t(c2r))
+    r.lib.ref_set_fft.argtypes = [fft_t, fft_t]
+    r.lib.ref_set_fft.restype = None
+    r.lib.ref_step.argtypes = [ctypes.POINTER(Sim), ctypes.POINTER(State), ctypes.c_int64] + [ctypes.c_void_p] * 5
+    r.lib.ref_step.restype = None
+    r.lib.ref_set_fft(*cb)
+
     box = 5.0 * Ns
-    fourpiG = 1.5 * box * box / C_LIGHT ** 2
-    pos, q, ids = particles(Ns, seed=seed, lattice=True, disp=0.2, qscale=2e-4)
-    phi = trough_phi(Ns, 1e-6)
+    ics = _load_ics_module()
+    pos, q, _, phi, mass, a0, fourpiG = ics.zeldovich(Ns, box, z_in, seed, device="cpu", omega_m=OMEGA_M,
+                                                      omega_l=OMEGA_L, h=H_LITTLE)
+    pos, q = np.ascontiguousarray(pos.numpy()), np.ascontiguousarray(q.numpy())
+    phi = np.ascontiguousarray(phi.numpy())
+    del torch
     chi = np.zeros(Ns ** 3)
     Bi = np.zeros(3 * Ns ** 3)
-    sim = OSim(Ns, box, fourpiG, OMEGA_M / Ns ** 3, OMEGA_M, OMEGA_L, 0.0, 100.0, 48.0, 0.04, 1)
-    a0 = 1.0 / 101
+    sim = Sim(Ns, box, fourpiG, mass, OMEGA_M, OMEGA_L, 0.0, z_in, 48.0, 0.04, 1)
     H = math.sqrt((2 * fourpiG / 3) * (OMEGA_M / a0 + OMEGA_L * a0 * a0))
-    st = OState(a0, 0.1, min(48.0 / Ns, 0.04 / H), 0.0, 0, 0, 0, 0)
-    o.lib.orc_step(ctypes.byref(sim), ctypes.byref(st), len(pos), ptr(pos), ptr(q), ptr(phi), ptr(chi), ptr(Bi))   # warm-up
+    st = State(a0, 0.0, min(48.0 / Ns, 0.04 / H), 0.0, 0, 0, 0, 0)
+
+    def cycle():
+        r.lib.ref_step(ctypes.byref(sim), ctypes.byref(st), len(pos), ptr(pos), ptr(q), ptr(phi), ptr(chi), ptr(Bi))
+
+    for _ in range(max(1, warmup)):
+        cycle()
     t0 = time.perf_counter()
     for _ in range(steps):
-        o.lib.orc_step(ctypes.byref(sim), ctypes.byref(st), len(pos), ptr(pos), ptr(q), ptr(phi), ptr(chi), ptr(Bi))
+        cycle()
     dt = time.perf_counter() - t0
-    return Ns ** 3 * steps / dt / 1e6, dt
+    r.lib.ref_set_fft(fft_t(0), fft_t(0))
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return Ns ** 3 * steps / dt / 1e6, dt, threads
+
+
+def reference_sample_config(Ns, N):
+    box = 5.0 * Ns
+    return {"workload": "PM cycle of the reference's own functions on the host cores (FP64): box %g Mpc/h, grid %d^3, "
+                        "%d^3 particles, GR, elliptic B; a bounded sample of the %d^3 workload with the same physics and "
+                        "5 Mpc/h cells" % (box, Ns, Ns, N),
+            "N": Ns, "particles": Ns ** 3, "boxsize_mpc_h": box, "sample_of": "grid %d^3, %d^3 particles" % (N, N),
+            "parallelism": "host cores (OpenMP)"}
 
 
 def adjoint_block(args, dev):
@@ -547,11 +618,14 @@ def adjoint_block(args, dev):
 def cpu_sample(args):
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    rate, dt = oracle_cycle_rate(args.cpu_sample_N, args.cpu_sample_steps, args.seed)
-    return {"value": rate, "unit": "Mpart-steps/s", "cores": int(os.environ.get("OMP_NUM_THREADS", cores)),
-            "kind": "port",
-            "sample": "%d cycles of the FP64 oracle cycle (orc_step) on a %d^3 box with %d^3 particles, %.1f s"
-                      % (args.cpu_sample_steps, args.cpu_sample_N, args.cpu_sample_N, dt)}
+    res = reference_cycle_rate(args.cpu_sample_N, args.cpu_sample_steps, 1, args.seed)
+    if res is None:
+        return None
+    rate, dt, threads = res
+    return {"value": rate, "unit": "Mpart-steps/s", "cores": threads, "kind": "reference",
+            "sample": "%d cycles of the reference's own cycle functions (ref_step, oracle/_ref) on a %d^3 box with %d^3 "
+                      "Zel'dovich particles from z = 100, %.1f s, FFT by pocketfft" % (args.cpu_sample_steps, args.cpu_sample_N,
+                                                                                     args.cpu_sample_N, dt)}
 
 
 def run_reference(args, rank):
@@ -560,16 +634,23 @@ def run_reference(args, rank):
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
     Ns = args.cpu_sample_N
-    rate, dt = oracle_cycle_rate(Ns, max(1, min(args.steps, 3)), args.seed)
+    res = reference_cycle_rate(Ns, args.steps, args.warmup, args.seed)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's cycle functions were not built here "
+                                                              "(oracle/_ref/libgevref.so is missing)"}), flush=True)
+        return
+    rate, dt, threads = res
     line = {"impl": "reference", "metric": "Mpart-steps/s at 512^3 (mixed vs FP64 GPU, P(k) err<1e-4); grad/fwd ratio",
-            "value": rate, "unit": "Mpart-steps/s", "n_gpus": args.gpus, "steps": max(1, min(args.steps, 3)),
-            "warmup": 1, "ms_per_step": dt / max(1, min(args.steps, 3)) * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic: seeded perturbed lattice",
-            "config": workload_config(args.N, args.boxsize or 5.0 * args.N, args.gpus),
-            "cpu_baseline": {"value": rate, "unit": "Mpart-steps/s", "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
-                             "sample": "FP64 oracle cycle (orc_step) on a %d^3 box with %d^3 particles, the same physics and "
-                                       "cell size as the workload, %d cycles in %.1f s" % (Ns, Ns, max(1, min(args.steps, 3)), dt)},
+            "value": rate, "unit": "Mpart-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": max(1, args.warmup), "ms_per_step": dt / args.steps * 1e3, "ms_per_step_grid": "%d^3" % Ns,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: Zel'dovich ICs at z=100 (EH no-wiggle P(k)), synthesised on the host, seed %d" % args.seed,
+            "config": reference_sample_config(Ns, args.N),
+            "cpu_baseline": {"value": rate, "unit": "Mpart-steps/s", "cores": threads, "kind": "reference",
+                             "sample": "the reference's own cycle functions (ref_step: gevolution.hpp projections, "
+                                       "prepareFTsource, Fourier solvers, update_q/update_pos, background.hpp) on a %d^3 "
+                                       "box, %d cycles after %d warm-up, %.1f s; FFT by pocketfft" % (Ns, args.steps,
+                                                                                                     max(1, args.warmup), dt)},
             "e2e": {"value": rate, "unit": "Mpart-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

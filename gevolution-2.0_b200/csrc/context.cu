@@ -1290,17 +1290,23 @@ int gev_checkpoint_read(gev_ctx *ctx, const char *path, gev_state *st)
         if (hdr[1] != c.cfg.N || hdr[3] != c.cfg.vector_method || (hdr[4] != 0) != (c.cfg.tensor != 0))
             throw gev::ArgError("checkpoint grid or metric configuration differs from the context");
         if (np < 0 || np > c.cfg.capacity) throw gev::ArgError("checkpoint holds more particles than the context capacity");
+        if (!(md[1] == c.cfg.boxsize)) throw gev::ArgError("checkpoint box size differs from the context");
+        // the whole file is read before the context changes: a truncated or
+        // mismatched file leaves the context's particles and fields as they were
         std::vector<double> pos(3 * (size_t)np), q(3 * (size_t)np);
         std::vector<int64_t> id((size_t)np);
         if (np > 0 && (fread(pos.data(), 8, pos.size(), fc.f) != pos.size() || fread(q.data(), 8, q.size(), fc.f) != q.size() ||
                        fread(id.data(), 8, id.size(), fc.f) != id.size()))
             throw gev::ArgError("truncated checkpoint particles");
-        c.particles_set(pos.data(), q.data(), id.data(), np, md[0]);
-        for (int f : ckpt_fields(c.cfg)) {
-            std::vector<double> buf((size_t)field_doubles(c.cfg, f));
+        const std::vector<int> fields = ckpt_fields(c.cfg);
+        std::vector<std::vector<double>> bufs;
+        for (int f : fields) {
+            bufs.emplace_back((size_t)field_doubles(c.cfg, f));
+            std::vector<double> &buf = bufs.back();
             if (fread(buf.data(), 8, buf.size(), fc.f) != buf.size()) throw gev::ArgError("truncated checkpoint fields");
-            c.field_set(f, buf.data());
         }
+        c.particles_set(pos.data(), q.data(), id.data(), np, md[0]);
+        for (size_t i = 0; i < fields.size(); i++) c.field_set(fields[i], bufs[i].data());
         *st = s;
     });
 }

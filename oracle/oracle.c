@@ -34,35 +34,39 @@ static int smallest_factor(int n)
     return n;
 }
 
-static void dft_rec(int n, const cplx *in, long is, cplx *out, int sign)
+/* exp(sign 2 pi i j / n) for j < n, from the exact angle of each j */
+static cplx *twiddles(int n, int sign)
+{
+    cplx *w = malloc(sizeof(cplx) * n);
+    for (int j = 0; j < n; j++) {
+        double ang = sign * 2.0 * M_PI * (double)j / n;
+        w[j] = cos(ang) + I * sin(ang);
+    }
+    return w;
+}
+
+/* DFT of length n of in[0], in[is], ...; w holds the twiddles of a length
+ * n0 = n * ws transform, so exp(sign 2 pi i j / n) = w[j * ws] */
+static void dft_rec(int n, const cplx *in, long is, cplx *out, const cplx *w, long ws)
 {
     if (n == 1) { out[0] = in[0]; return; }
     int p = smallest_factor(n);
     if (p == n) {                       /* prime length: direct sum */
         for (int k = 0; k < n; k++) {
             cplx s = 0;
-            for (int j = 0; j < n; j++) {
-                double ang = sign * 2.0 * M_PI * (double)((long)j * k % n) / n;
-                s += in[j * is] * (cos(ang) + I * sin(ang));
-            }
+            for (int j = 0; j < n; j++) s += in[j * is] * w[((long)j * k % n) * ws];
             out[k] = s;
         }
         return;
     }
     int m = n / p;
-    for (int r = 0; r < p; r++) dft_rec(m, in + r * is, is * p, out + r * m, sign);
+    for (int r = 0; r < p; r++) dft_rec(m, in + r * is, is * p, out + r * m, w, ws * p);
     cplx tmp[p];
     for (int k = 0; k < m; k++) {
-        for (int r = 0; r < p; r++) {
-            double ang = sign * 2.0 * M_PI * (double)(r * k) / n;
-            tmp[r] = out[r * m + k] * (cos(ang) + I * sin(ang));
-        }
+        for (int r = 0; r < p; r++) tmp[r] = out[r * m + k] * w[(long)r * k * ws];
         for (int q = 0; q < p; q++) {
             cplx s = 0;
-            for (int r = 0; r < p; r++) {
-                double ang = sign * 2.0 * M_PI * (double)((r * q) % p) / p;
-                s += tmp[r] * (cos(ang) + I * sin(ang));
-            }
+            for (int r = 0; r < p; r++) s += tmp[r] * w[(long)((r * q) % p) * m * ws];
             out[k + q * m] = s;
         }
     }
@@ -72,15 +76,18 @@ void orc_fft1d(int n, double *re_im, int sign)
 {
     cplx *a = (cplx *)re_im;
     cplx *in = malloc(sizeof(cplx) * n);
+    cplx *w = twiddles(n, sign);
     memcpy(in, a, sizeof(cplx) * n);
-    dft_rec(n, in, 1, a, sign);
+    dft_rec(n, in, 1, a, w, 1);
     free(in);
+    free(w);
 }
 
 /* transform along y (axis 1) and z (axis 2) of a (N/2+1) x N x N complex block */
 static void fft_yz(int N, cplx *c, int sign, int axis_first_z)
 {
     const int P = N / 2 + 1;
+    cplx *w = twiddles(N, sign);
     for (int pass = 0; pass < 2; pass++) {
         int along_z = axis_first_z ? (pass == 0) : (pass == 1);
 #pragma omp parallel
@@ -93,7 +100,7 @@ static void fft_yz(int N, cplx *c, int sign, int axis_first_z)
                         long idx = along_z ? kx + (long)P * (o + (long)N * t) : kx + (long)P * (t + (long)N * o);
                         col[t] = c[idx];
                     }
-                    dft_rec(N, col, 1, res, sign);
+                    dft_rec(N, col, 1, res, w, 1);
                     for (int t = 0; t < N; t++) {
                         long idx = along_z ? kx + (long)P * (o + (long)N * t) : kx + (long)P * (t + (long)N * o);
                         c[idx] = res[t];
@@ -102,12 +109,14 @@ static void fft_yz(int N, cplx *c, int sign, int axis_first_z)
             free(col); free(res);
         }
     }
+    free(w);
 }
 
 void orc_r2c(int N, const double *in, double *out_)
 {
     const int P = N / 2 + 1;
     cplx *out = (cplx *)out_;
+    cplx *w = twiddles(N, -1);
 #pragma omp parallel
     {
         cplx *row = malloc(sizeof(cplx) * N), *res = malloc(sizeof(cplx) * N);
@@ -115,11 +124,12 @@ void orc_r2c(int N, const double *in, double *out_)
         for (int z = 0; z < N; z++)
             for (int y = 0; y < N; y++) {
                 for (int x = 0; x < N; x++) row[x] = in[IDX(N, x, y, z)];
-                dft_rec(N, row, 1, res, -1);
+                dft_rec(N, row, 1, res, w, 1);
                 for (int kx = 0; kx < P; kx++) out[kx + (long)P * (y + (long)N * z)] = res[kx];
             }
         free(row); free(res);
     }
+    free(w);
     fft_yz(N, out, -1, 0);
 }
 
@@ -131,6 +141,7 @@ void orc_c2r(int N, const double *in_, double *out)
     cplx *c = malloc(sizeof(cplx) * (size_t)P * N * N);
     memcpy(c, in_, sizeof(cplx) * (size_t)P * N * N);
     fft_yz(N, c, +1, 1);
+    cplx *w = twiddles(N, +1);
 #pragma omp parallel
     {
         cplx *row = malloc(sizeof(cplx) * N), *res = malloc(sizeof(cplx) * N);
@@ -141,11 +152,12 @@ void orc_c2r(int N, const double *in_, double *out)
                 for (int k = 0; k < N; k++) row[k] = (k < P) ? r[k] : conj(r[N - k]);
                 row[0] = creal(row[0]);
                 if (N % 2 == 0) row[N / 2] = creal(row[N / 2]);
-                dft_rec(N, row, 1, res, +1);
+                dft_rec(N, row, 1, res, w, 1);
                 for (int x = 0; x < N; x++) out[IDX(N, x, y, z)] = creal(res[x]);
             }
         free(row); free(res);
     }
+    free(w);
     free(c);
 }
 

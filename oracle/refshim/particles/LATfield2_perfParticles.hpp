@@ -6,11 +6,20 @@
 // (gevolution.hpp:1339, :1358).  updateVel returns the square root of the largest
 // functor return value (ic_basic.hpp:2433 divides it by a to obtain a velocity
 // from a functor that returns q^2); moveParticles wraps positions into [0,1).
+//
+// Threads (OpenMP): updateVel and moveParticles touch one particle per functor
+// call and run over particles in parallel.  A projection functor adds into the
+// cells of its particle's stencil, which never reaches beyond one cell on
+// either side along z (gevolution.hpp:1729-1854, :2031-2201, :2582-2965), so
+// projections run by z-planes of cells in four rounds (cz mod 4): planes of one
+// round are at least 4 apart and their particles write disjoint field planes.
+// Within a plane particles keep their order.
 #ifndef GEV_REFSHIM_PERFPARTICLES_HPP
 #define GEV_REFSHIM_PERFPARTICLES_HPP
 
 #include <cmath>
 #include <vector>
+#include <omp.h>
 
 struct part_simple
 {
@@ -59,6 +68,7 @@ public:
 	Real updateVel(F f, double dtau, Field<Real> ** fields, int nfield, double * params)
 	{
 		Real vmax = 0;
+#pragma omp parallel for reduction(max : vmax) schedule(static)
 		for (long p = 0; p < count_; p++)
 		{
 			double ref_dist[3];
@@ -72,15 +82,21 @@ public:
 	template <class F>
 	void moveParticles(F f, double dtau, Field<Real> ** fields, int nfield, double * params)
 	{
-		for_each_particle(f, dtau, fields, nfield, params);
+#pragma omp parallel for schedule(static)
 		for (long p = 0; p < count_; p++)
+		{
+			double ref_dist[3];
+			Site sites[4];
+			locate(p, fields, nfield, ref_dist, sites);
+			f(dtau, 1.0 / lat_->N(), parts_ + p, ref_dist, info_, fields, sites, nfield, params, nullptr, 0);
 			for (int i = 0; i < 3; i++) parts_[p].pos[i] -= std::floor(parts_[p].pos[i]);
+		}
 	}
 	void meshprojection_project(Field<Real> * field)
 	{
 		const double dx = 1.0 / lat_->N();
 		const double mass = info_.mass / (dx * dx * dx);
-		for (long p = 0; p < count_; p++)
+		by_z_planes([&](long p)
 		{
 			double d[3];
 			Site sites[4];
@@ -93,7 +109,7 @@ public:
 				if (k & 1) s = s + 2;
 				(*field)(s) += mass * ((k & 4) ? d[0] : 1. - d[0]) * ((k & 2) ? d[1] : 1. - d[1]) * ((k & 1) ? d[2] : 1. - d[2]);
 			}
-		}
+		});
 	}
 
 private:
@@ -111,16 +127,43 @@ private:
 		for (int i = 0; i < nfield && i < 4; i++)
 			sites[i] = Site(fields[i] ? fields[i]->lattice() : *lat_, c[0], c[1], c[2]);
 	}
+	// body(p) for every particle, by z-planes of cells in four rounds (see the top)
+	template <class B>
+	void by_z_planes(B && body)
+	{
+		const int N = lat_->N();
+		std::vector<long> start(N + 1, 0), order(count_);
+		std::vector<int> cz(count_);
+		for (long p = 0; p < count_; p++)
+		{
+			cz[p] = ((int) std::floor((double) parts_[p].pos[2] * N) % N + N) % N;
+			start[cz[p] + 1]++;
+		}
+		for (int z = 0; z < N; z++) start[z + 1] += start[z];
+		std::vector<long> fill(start.begin(), start.end() - 1);
+		for (long p = 0; p < count_; p++) order[fill[cz[p]]++] = p;
+		if (N % 4 != 0)   // the rounds need N a multiple of 4 (planes N-4+r and r are 4 apart)
+		{
+			for (long i = 0; i < count_; i++) body(order[i]);
+			return;
+		}
+		for (int round = 0; round < 4; round++)
+		{
+#pragma omp parallel for schedule(dynamic, 1)
+			for (int z = round; z < N; z += 4)
+				for (long i = start[z]; i < start[z + 1]; i++) body(order[i]);
+		}
+	}
 	template <class F>
 	void for_each_particle(F f, double dtau, Field<Real> ** fields, int nfield, double * params)
 	{
-		for (long p = 0; p < count_; p++)
+		by_z_planes([&](long p)
 		{
 			double ref_dist[3];
 			Site sites[4];
 			locate(p, fields, nfield, ref_dist, sites);
 			f(dtau, 1.0 / lat_->N(), parts_ + p, ref_dist, info_, fields, sites, nfield, params, nullptr, 0);
-		}
+		});
 	}
 	const Lattice * lat_;
 	part * parts_ = nullptr;

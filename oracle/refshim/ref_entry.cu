@@ -8,6 +8,10 @@
 // reference CPU arm of bench.py.  Nothing here is part of the product path.
 //
 // Every entry point takes the same arguments as its orc_* twin in oracle.h.
+// ref_step composes them into one cycle of main.cu's loop; LATfield2's FFT
+// (PlanFFT, cuFFT/FFTW inside, not part of the reference tree) is stood in for
+// by the oracle's FFT (orc_r2c / orc_c2r, linked from ../liboracle.so) or by
+// the pair of transforms given to ref_set_fft.
 #include <cstdint>
 #include <omp.h>
 #include <nvtx3/nvToolsExt.h>
@@ -21,6 +25,8 @@
 #include <cstdint>
 #include <functional>
 #include <vector>
+
+#include "../oracle.h"
 
 using namespace LATfield2;
 
@@ -288,5 +294,143 @@ int ref_find_intersecting(const double * lc_vertex, const double * lc_direction,
 }
 
 int ref_max_intersects(void) { return MAX_INTERSECTS; }
+
+// One cycle of main.cu's loop (main.cu:608-1317) for CDM in the weak-field GR
+// gauge with the elliptic vector method, no radiation, ncdm, baryons or
+// output, composed from the reference's own functors and functions:
+//   T00, Tij projections with the previous phi   main.cu:616-623, :750-756
+//   prepareFTsource (T00) + FFT + solveModifiedPoissonFT + FFT^-1
+//                                                 main.cu:719-809
+//   prepareFTsource (Tij) + 6 FFTs + projectFTscalar + FFT^-1
+//                                                 main.cu:811-903
+//   T0i projection with the new phi + 3 FFTs + projectFTvector + 3 FFT^-1
+//                                                 main.cu:836-955
+//   updateVel(update_q), rungekutta4bg, moveParticles(update_pos),
+//   rungekutta4bg, maxvel, step control          main.cu:1225-1310
+// sim and st have the layouts of orc_sim and orc_state (oracle.h); pos and q
+// are advanced in place (particle p has ID p), phi, chi and Bi are the
+// persistent fields.
+typedef void (*ref_fft_fn)(int N, const double * in, double * out);
+static ref_fft_fn g_r2c = orc_r2c, g_c2r = orc_c2r;
+
+// transforms used by ref_step, with the conventions of orc_r2c / orc_c2r
+// (unnormalised, half spectrum kx + (N/2+1)(ky + N kz)); null restores those
+void ref_set_fft(ref_fft_fn r2c, ref_fft_fn c2r)
+{
+	g_r2c = r2c ? r2c : orc_r2c;
+	g_c2r = c2r ? c2r : orc_c2r;
+}
+
+void ref_step(const orc_sim * sim, orc_state * st, int64_t np, double * pos, double * q, double * phi, double * chi, double * Bi)
+{
+	const int N = sim->N;
+	const int64_t n3 = (int64_t) N * N * N, nk = (int64_t) (N / 2 + 1) * N * N;
+	const double dx = 1. / N;
+	const double fourpiG = sim->fourpiG;
+	const cosmology cosmo = make_cosmo(sim->cosmo.Omega_m, sim->cosmo.Omega_Lambda, sim->cosmo.Omega_rad);
+	double a = st->a;
+
+	ParticleSet ps(N, np, pos, q, sim->mass);
+	Lattice klat(N, true);
+	std::vector<double> source(n3, 0.), Sij(6 * n3, 0.);
+	std::vector<Imag> FT(6 * nk);
+	Field<Real> fsource(ps.lat, source.data(), 1), fphi(ps.lat, phi, 1), fchi(ps.lat, chi, 1);
+	Field<Real> fSij(ps.lat, Sij.data(), 6, symmetric), fBi(ps.lat, Bi, 3);
+	Field<Imag> fscalar(klat, FT.data(), 1), fSijFT(klat, FT.data(), 6, symmetric), fBiFT(klat, FT.data(), 3);
+	double * ft = reinterpret_cast<double *>(FT.data());
+
+	// stress-energy: projection_T00_project(&pcls_cdm, &source, a, &phi) and
+	// projection_Tij_project_Async with f_params {a, 1}
+	{
+		Field<Real> * f[2] = {&fsource, &fphi};
+		double params[2] = {a, 1.};
+		ps.pcls.projectParticles(particle_T00_project_functor(), f, 2, params);
+	}
+	{
+		Field<Real> * f[2] = {&fSij, &fphi};
+		double params[7] = {a, 1., 0., 0., 0., 0., 0.};
+		ps.pcls.projectParticles(particle_Tij_project_functor(), f, 2, params);
+	}
+
+	// phi update
+	if (st->dtau_old > 0.)
+	{
+		const double H = Hconf(a, fourpiG, cosmo);
+		Field<Real> * f[4] = {&fsource, &fsource, &fphi, &fchi};
+		double params[4] = {cosmo.Omega_cdm + cosmo.Omega_b, 3. * H * dx * dx / st->dtau_old, fourpiG * dx * dx / a, 3. * H * H * dx * dx};
+		double sum = 0.;
+#pragma omp parallel for collapse(2) reduction(+ : sum) schedule(static)
+		for (int z = 0; z < N; z++)
+			for (int y = 0; y < N; y++)
+				for (int x = 0; x < N; x++)
+				{
+					Site s(ps.lat, x, y, z);
+					Site sites[4] = {s, s, s, s};
+					double out[1];
+					prepareFTsource_T00(f, sites, 4, params, out);
+					sum += out[0];
+				}
+		st->T00hom = sum / (double) n3;
+		g_r2c(N, source.data(), ft);
+		solveModifiedPoissonFT(fscalar, fscalar, 1. / (dx * dx), 3. * H / st->dtau_old);
+		st->phi_hom = ft[0];
+		g_c2r(N, ft, phi);
+	}
+
+	// chi: prepareFTsource(phi, Sij, Sij, 2 fourpiG dx^2 / a), projectFTscalar
+	{
+		Field<Real> * f[3] = {&fSij, &fSij, &fphi};
+		double coeff = 2. * fourpiG * dx * dx / a;
+		site_loop(N, [&](int x, int y, int z) {
+			Site s(ps.lat, x, y, z);
+			Site sites[3] = {s, s, s};
+			prepareFTsource_Tij(f, sites, 3, &coeff, nullptr);
+		});
+		for (int c = 0; c < 6; c++) g_r2c(N, Sij.data() + c * n3, ft + 2 * c * nk);
+		std::vector<Imag> chiFT(nk);
+		Field<Imag> fchiFT(klat, chiFT.data(), 1);
+		projectFTscalar(fSijFT, fchiFT);
+		g_c2r(N, reinterpret_cast<double *>(chiFT.data()), chi);
+	}
+
+	// B_i, elliptic: projection_T0i_project_Async with the new phi, projectFTvector
+	if (sim->with_B)
+	{
+		std::fill(Bi, Bi + 3 * n3, 0.);
+		Field<Real> * f[2] = {&fBi, &fphi};
+		double coeff = 1.;
+		ps.pcls.projectParticles(particle_T0i_project_functor(), f, 2, &coeff);
+		for (int c = 0; c < 3; c++) g_r2c(N, Bi + c * n3, ft + 2 * c * nk);
+		projectFTvector(fBiFT, fBiFT, fourpiG * dx * dx);
+		for (int c = 0; c < 3; c++) g_c2r(N, ft + 2 * c * nk, Bi + c * n3);
+	}
+
+	// particle update and background
+	{
+		Field<Real> * f[3] = {&fphi, &fchi, &fBi};
+		double params[7] = {a, a * a * N, 0., 0., 0., 0., 0.};
+		double mv = ps.pcls.updateVel(update_q_functor(), (st->dtau + st->dtau_old) / 2., f, (1. / a < sim->z_relax + 1. ? 3 : 2), params);
+		rungekutta4bg(a, fourpiG, cosmo, 0.5 * st->dtau);
+		params[0] = a;
+		params[1] = a * a * N;
+		ps.pcls.moveParticles(update_pos_functor(), st->dtau, f, (1. / a < sim->z_relax + 1. ? 3 : 0), params);
+		rungekutta4bg(a, fourpiG, cosmo, 0.5 * st->dtau);
+		st->maxvel = mv / sqrt(mv * mv + 1.0);
+	}
+	for (int64_t p = 0; p < np; p++)
+		for (int i = 0; i < 3; i++)
+		{
+			pos[3 * p + i] = ps.parts[p].pos[i];
+			q[3 * p + i] = ps.parts[p].vel[i];
+		}
+
+	// step control
+	st->tau += st->dtau;
+	st->dtau_old = st->dtau;
+	const double Hn = Hconf(a, fourpiG, cosmo);
+	st->dtau = (sim->Cf * dx < sim->steplimit / Hn) ? sim->Cf * dx : sim->steplimit / Hn;
+	st->a = a;
+	st->cycle++;
+}
 
 } // extern "C"

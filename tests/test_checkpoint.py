@@ -9,7 +9,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from _fixtures import rel_err
+from _fixtures import particles, rel_err
 
 gev = pytest.importorskip("gevb200")
 from gevb200.ics import hconf  # noqa: E402
@@ -95,6 +95,16 @@ def test_rejects_mismatch_and_garbage(tmp_path):
         with pytest.raises(gev.GevError):
             c32.checkpoint_read(tmp_path / "bad")
         raw = (tmp_path / "ck").read_bytes()
-        (tmp_path / "short").write_bytes(raw[: len(raw) // 2])
+        # a truncated file is refused and leaves the context as it was
+        pos, q, ids = particles(32, n=500, seed=99)
+        c32.set_particles(pos, q, ids, 1e-3)
+        before = c32.get_particles()
+        (tmp_path / "short").write_bytes(raw[: len(raw) - 1000])
         with pytest.raises(gev.GevError):
             c32.checkpoint_read(tmp_path / "short")
+        for x, y in zip(c32.get_particles(), before):
+            assert np.array_equal(x, y)
+    # a different box size is refused
+    with gev.Context(32, precision=gev.MIXED, capacity=32 ** 3, boxsize=320.0) as cbox:
+        with pytest.raises(gev.GevError, match="box size"):
+            cbox.checkpoint_read(tmp_path / "ck")

@@ -253,3 +253,50 @@ def test_rel_err_sees_imaginary_parts():
     a = np.array([1 + 1j, 2 - 1j])
     assert rel_err(a, a) == 0
     assert rel_err(a + 0.1j, a) > 0.04
+
+
+class _Sim(ctypes.Structure):   # orc_sim (oracle.h), also ref_step's argument
+    _fields_ = [("N", ctypes.c_int), ("boxsize", ctypes.c_double), ("fourpiG", ctypes.c_double),
+                ("mass", ctypes.c_double), ("Om", ctypes.c_double), ("OL", ctypes.c_double),
+                ("Orad", ctypes.c_double), ("z_relax", ctypes.c_double), ("Cf", ctypes.c_double),
+                ("steplimit", ctypes.c_double), ("with_B", ctypes.c_int)]
+
+
+class _State(ctypes.Structure):   # orc_state
+    _fields_ = [("a", ctypes.c_double), ("tau", ctypes.c_double), ("dtau", ctypes.c_double),
+                ("dtau_old", ctypes.c_double), ("cycle", ctypes.c_int), ("T00hom", ctypes.c_double),
+                ("phi_hom", ctypes.c_double), ("maxvel", ctypes.c_double)]
+
+
+def test_cycle_matches_reference_cycle(libs):
+    """orc_step (the oracle's restated cycle) against ref_step, the same cycle
+    composed from the reference's own functors, solvers and background
+    integrator (main.cu:608-1317): four cycles from a perturbed lattice at 16^3
+    with B_i entering the geodesic (z < z_relax), FP64."""
+    o, r = libs
+    N = 16
+    pos, q, _ = particles(N, seed=5, lattice=True, disp=0.3, qscale=3e-3)
+    box = 320.0
+    fourpiG = 1.5 * box ** 2 / 2997.92458 ** 2
+    sim = _Sim(N, box, fourpiG, 0.32 / len(pos), 0.32, 0.68, 0.0, 100.0, 48.0, 0.04, 1)
+    for lib, fn in ((o.lib, "orc_step"), (r.lib, "ref_step")):
+        f = getattr(lib, fn)
+        f.argtypes = [ctypes.POINTER(_Sim), ctypes.POINTER(_State), ctypes.c_int64] + [ctypes.c_void_p] * 5
+        f.restype = None
+    out = []
+    for lib, fn in ((o.lib, "orc_step"), (r.lib, "ref_step")):
+        p_, q_ = pos.copy(), q.copy()
+        phi, chi, Bi = trough_phi(N, 1e-5), np.zeros(N ** 3), np.zeros(3 * N ** 3)
+        st = _State(1.0 / 31, 0.1, 0.02, 0.0, 0, 0, 0, 0)
+        for _ in range(4):
+            getattr(lib, fn)(ctypes.byref(sim), ctypes.byref(st), len(p_), ptr(p_), ptr(q_), ptr(phi), ptr(chi), ptr(Bi))
+        out.append((st, p_, q_, phi, chi, Bi))
+    (s1, p1, q1, f1, c1, b1), (s2, p2, q2, f2, c2, b2) = out
+    assert (s1.a, s1.tau, s1.dtau, s1.dtau_old, s1.cycle) == (s2.a, s2.tau, s2.dtau, s2.dtau_old, s2.cycle)
+    assert abs(s1.maxvel / s2.maxvel - 1) < 1e-12 and abs(s1.T00hom / s2.T00hom - 1) < 1e-12
+    d = p1 - p2
+    d -= np.round(d)
+    assert np.abs(d).max() < 1e-14
+    assert rel_err(q1, q2) < 1e-12
+    for x, y in ((f1, f2), (c1, c2), (b1, b2)):
+        assert rel_err(x, y) < 1e-10

@@ -63,7 +63,11 @@ def test_reference_arm_rank_handling(rank):
     if rank == 0:
         assert len(lines) == 1
         d = json.loads(lines[0])
-        assert d["impl"] == "reference" and d["value"] > 0
-        assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] == "port"
+        assert d["impl"] == "reference"
+        if "unavailable" in d:   # the reference's functions were not built in this tree
+            assert not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libgevref.so"))
+            return
+        assert d["value"] > 0 and d["config"]["N"] == 16
+        assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] == "reference"
     else:
         assert lines == []
