@@ -210,6 +210,8 @@ template <class R> struct Ctx final : CtxBase {
     DBuf<int> derr;
     DBuf<double> bins;
     DBuf<unsigned long long> occ;
+    DBuf<double> rho64;                  // mixed precision: FP64 density of the spectrum measurement
+    DBuf<double2> tw64_full, tw64_half;  // mixed precision: FP64 twiddles of that measurement
     DBuf<double> stage;                  // particle / field transfer staging
     DBuf<int64_t> stage_id;
     DBuf<float> lc_pos, lc_vel;
@@ -316,6 +318,19 @@ template <class R> struct Ctx final : CtxBase {
     }
 
     FftTables<R> tables() const { return FftTables<R>{tw_full.p, tw_half.p, k2.p, ks.p}; }
+
+    void make_tables64()
+    {
+        const int N = g.N;
+        std::vector<double2> tf(N), th(N / 2);
+        for (int k = 0; k < N; k++) tf[k] = make_double2(std::cos(-2.0 * M_PI * (double)k / N), std::sin(-2.0 * M_PI * (double)k / N));
+        for (int k = 0; k < N / 2; k++)
+            th[k] = make_double2(std::cos(-2.0 * M_PI * (double)k / (N / 2)), std::sin(-2.0 * M_PI * (double)k / (N / 2)));
+        tw64_full.alloc(N, "twiddles");
+        tw64_half.alloc(N / 2, "twiddles");
+        ck(cudaMemcpy(tw64_full.p, tf.data(), N * sizeof(double2), cudaMemcpyHostToDevice), "tables");
+        ck(cudaMemcpy(tw64_half.p, th.data(), (N / 2) * sizeof(double2), cudaMemcpyHostToDevice), "tables");
+    }
 
     PView<R> view(bool A) const
     {
@@ -776,13 +791,14 @@ template <class R> struct Ctx final : CtxBase {
         need_particles();
         if (nb <= 0) throw ArgError("numbins must be positive");
         const int N = g.N;
-        if (kmax <= 0.0) kmax = std::sqrt(3.0) * M_PI * N;   // tools.hpp:144-145 with KTYPE_LINEAR
-        project(GEV_PROJ_CIC, 1.0, 1.0, 0, 0);
-        const FftTables<R> tb = tables();
-        fx_forward<R>(N, FX_COPY, source.p, g.n3, 1, 0, nullptr, nullptr, 0, 0, 0, 0, W.p, g.nk, nullptr, tb, st);
-        launched("fx forward (CIC)");
-        fy_pass<R>(N, -1, W.p, g.nk, 1, derr.p, tb, st);
-        launched("fy forward (CIC)");
+        if (kmax <= 0.0) {
+            // tools.hpp:144-145 with KTYPE_LINEAR, in the reference's own order of
+            // operations: modes with |n|^2 = 3 m^2 lie exactly on bin edges, where
+            // one ulp of kmax decides their bin
+            double t = 2.0 * M_PI * (double)(N / 2);
+            t *= t;
+            kmax = std::sqrt(3.0 * t);
+        }
         if ((int)occ.n < nb) { bins.alloc(4 * nb, "bins"); occ.alloc(nb, "bins"); }
         ck(cudaMemsetAsync(bins.p, 0, 4 * nb * sizeof(double), st), "memset");
         ck(cudaMemsetAsync(occ.p, 0, nb * sizeof(unsigned long long), st), "memset");
@@ -793,8 +809,40 @@ template <class R> struct Ctx final : CtxBase {
         fp.p1 = kmax;
         fp.bins = bins.p;
         fp.occ = occ.p;
-        fz_pass<R>(N, fp, W.p, g.nk, nullptr, nullptr, nullptr, tb, st);
-        launched("fz binning");
+        if constexpr (sizeof(R) == 8) {
+            project(GEV_PROJ_CIC, 1.0, 1.0, 0, 0);
+            const FftTables<R> tb = tables();
+            fx_forward<R>(N, FX_COPY, source.p, g.n3, 1, 0, nullptr, nullptr, 0, 0, 0, 0, W.p, g.nk, nullptr, tb, st);
+            launched("fx forward (CIC)");
+            fy_pass<R>(N, -1, W.p, g.nk, 1, derr.p, tb, st);
+            launched("fy forward (CIC)");
+            fz_pass<R>(N, fp, W.p, g.nk, nullptr, nullptr, nullptr, tb, st);
+            launched("fz binning");
+        } else {
+            // Mixed precision measures in FP64: the density contrast of an early,
+            // nearly uniform box is ~1e-2 of the density, and FP32 rounding of the
+            // density itself would set the small-scale floor of the spectrum.
+            // FP64 CIC density of the FP64 positions (atomic adds), FP64
+            // transform and binning in the first two FP32 components of W; the
+            // FP32 copy of the density is left in the source field as in FP64.
+            if (!rho64.p) {
+                rho64.alloc(g.n3, "FP64 density");
+                make_tables64();
+            }
+            ck(cudaMemsetAsync(rho64.p, 0, g.n3 * sizeof(double), st), "memset");
+            launch_cic_f64<R>(cur(), N, mass * (double)g.n3, rho64.p, st);
+            launched("CIC density (FP64)");
+            launch_f64_to_f32(rho64.p, g.n3, reinterpret_cast<float *>(source.p), st);
+            launched("density to FP32");
+            const FftTables<double> tb{tw64_full.p, tw64_half.p, k2.p, ks.p};
+            double2 *W64 = reinterpret_cast<double2 *>(W.p);   // W holds 6 FP32 components = 3 FP64 ones
+            fx_forward<double>(N, FX_COPY, rho64.p, g.n3, 1, 0, nullptr, nullptr, 0, 0, 0, 0, W64, g.nk, nullptr, tb, st);
+            launched("fx forward (CIC, FP64)");
+            fy_pass<double>(N, -1, W64, g.nk, 1, derr.p, tb, st);
+            launched("fy forward (CIC, FP64)");
+            fz_pass<double>(N, fp, W64, g.nk, nullptr, nullptr, nullptr, tb, st);
+            launched("fz binning (FP64)");
+        }
         std::vector<double> acc(4 * nb);
         std::vector<unsigned long long> oc(nb);
         ck(cudaMemcpyAsync(acc.data(), bins.p, 4 * nb * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");

@@ -459,19 +459,25 @@ __device__ __forceinline__ void fz_apply(const FzArgs<R> &a, int N, int kx, int 
         // (tools.hpp:105-215); p0 = numbins, p1 = kmax
         if (kx == 0 && ky == 0 && kz == 0) return;
         const int weight = (kx == 0 || (kx == N / 2 && (N % 2) == 0)) ? 1 : 2;
-        auto lin = [&](int i) { double t = 2.0 * 3.14159265358979323846 * (double)(i <= N / 2 ? i : N - i); return t * t; };
+        // k^2 and the bin index with separately rounded operations (no fused
+        // multiply-add), as the reference evaluates them on the host: modes on a
+        // bin edge (|n|^2 = 3 m^2 for the default kmax) land in the same bin
+        auto lin = [&](int i) {
+            const double t = __dmul_rn(2.0 * 3.14159265358979323846, (double)(i <= N / 2 ? i : N - i));
+            return __dmul_rn(t, t);
+        };
         auto snc = [&](int i) {
             int j = i <= N / 2 ? i : N - i;
             if (j == 0) return 1.0;
             return sin(3.14159265358979323846 * (double)(float)j / (double)(float)N) * (double)(float)N / (3.14159265358979323846 * (double)(float)j);
         };
-        double kk2 = lin(kx) + lin(ky) + lin(kz);
+        double kk2 = __dadd_rn(__dadd_rn(lin(kx), lin(ky)), lin(kz));
         double s = snc(kx) * snc(ky) * snc(kz);
         s *= s;
         double pw = v[0].x * v[0].x + v[0].y * v[0].y;
         double sk = sqrt(kk2);
         int nb = (int)a.p0;
-        int bin = (int)floor((double)nb * sk / a.p1);
+        int bin = (int)floor(__ddiv_rn(__dmul_rn((double)nb, sk), a.p1));
         if (bin < nb) {
             atomicAdd(a.bins + bin, weight * sk);
             atomicAdd(a.bins + nb + bin, weight * kk2);

@@ -50,6 +50,12 @@ void launch_rebin(const PView<R> &src, PView<R> dst, const uint32_t *bstart, con
 
 void launch_reduce_sum(const double *partial, int64_t n, double *out, cudaStream_t st);
 
+// FP64 CIC mass density of the particles (m = mass / dx^3) added into rho, and
+// an FP64 -> FP32 copy: the power spectrum of a mixed-precision context is
+// measured in FP64
+template <class R> void launch_cic_f64(const PView<R> &p, int N, double m, double *rho, cudaStream_t st);
+void launch_f64_to_f32(const double *in, int64_t n, float *out, cudaStream_t st);
+
 // ---- Fourier passes ----
 template <class R> struct FftTables {
     const typename CT<R>::C *tw_full;   // exp(-2 pi i k / N), k < N

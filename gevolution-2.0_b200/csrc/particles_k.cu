@@ -11,6 +11,7 @@
 // inside each bucket into (cell, ID) order -- after an exclusive scan of the
 // bucket counts (the re-binning that LATfield2's moveParticles does into its
 // row buffers).
+#include <algorithm>
 #include "common.cuh"
 #include "kernels.h"
 #include "particles.cuh"
@@ -613,6 +614,43 @@ void launch_rebin(const PView<R> &src, PView<R> dst, const uint32_t *bstart, con
                                                                     FastDiv((uint32_t)N));
 }
 
+// CIC mass density in FP64 (scalarProjectionCIC_project, gevolution.hpp:1902,
+// with LATfield2's meshprojection weights) from the FP64 positions, by
+// atomic adds: the density a mixed-precision context measures its power
+// spectrum on.  m = particle mass / dx^3.
+template <class R>
+__global__ void k_cic_f64(PView<R> p, int N, FastDiv fN, double m, double *__restrict__ rho)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < p.n; i += (int64_t)gridDim.x * blockDim.x) {
+        int cx, cy, cz;
+        decode_cell(p.cell[i], fN, cx, cy, cz);
+        const double d[3] = {p.off[i], p.off[p.cap + i], p.off[2 * p.cap + i]};
+        const int x1 = cx + 1 == N ? 0 : cx + 1, y1 = cy + 1 == N ? 0 : cy + 1, z1 = cz + 1 == N ? 0 : cz + 1;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const double w = ((k & 1) ? d[0] : 1.0 - d[0]) * ((k & 2) ? d[1] : 1.0 - d[1]) * ((k & 4) ? d[2] : 1.0 - d[2]);
+            atomicAdd(rho + sidx(N, (k & 1) ? x1 : cx, (k & 2) ? y1 : cy, (k & 4) ? z1 : cz), m * w);
+        }
+    }
+}
+
+template <class R> void launch_cic_f64(const PView<R> &p, int N, double m, double *rho, cudaStream_t st)
+{
+    if (p.n <= 0) return;
+    k_cic_f64<R><<<(unsigned)std::min<int64_t>(cdiv(p.n, 256), 148 * 16), 256, 0, st>>>(p, N, FastDiv((uint32_t)N), m, rho);
+}
+
+__global__ void k_f64_to_f32(const double *__restrict__ in, int64_t n, float *__restrict__ out)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
+}
+
+void launch_f64_to_f32(const double *in, int64_t n, float *out, cudaStream_t st)
+{
+    if (n > 0) k_f64_to_f32<<<(unsigned)std::min<int64_t>(cdiv(n, 256), 148 * 16), 256, 0, st>>>(in, n, out);
+}
+
 // deterministic sum of per-block partials (fixed order)
 __global__ void k_reduce_sum(const double *partial, int64_t n, double *out)
 {
@@ -643,7 +681,8 @@ void launch_reduce_sum(const double *partial, int64_t n, double *out, cudaStream
                                             cudaStream_t);                                                            \
     template void launch_bin_count<R>(const PView<R> &, int, uint32_t *, uint32_t *, uint32_t *, cudaStream_t);       \
     template void launch_rebin<R>(const PView<R> &, PView<R>, const uint32_t *, const uint32_t *, const uint32_t *,   \
-                                  uint32_t *, int, int *, cudaStream_t);
+                                  uint32_t *, int, int *, cudaStream_t);                                              \
+    template void launch_cic_f64<R>(const PView<R> &, int, double, double *, cudaStream_t);
 GEV_INST(float)
 GEV_INST(double)
 #undef GEV_INST
