@@ -52,6 +52,7 @@ def parse():
     p.add_argument("--boxsize", type=float, default=None, help="Mpc/h (default: 5 Mpc/h per cell)")
     p.add_argument("--z-in", type=float, default=100.0)
     p.add_argument("--seed", type=int, default=42)
+    p.add_argument("--tensor", action="store_true", help="keep the h_ij / h_ij' state (full metric solve)")
     p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=2)
@@ -161,10 +162,11 @@ def ncu_traffic(stage, N):
     return None if t is None else t * (N / 256.0) ** 3
 
 
-def workload_config(N, box, world):
-    return {"workload": "PM cycle, box %g Mpc/h, grid %d^3, %d^3 particles, mixed precision, GR, elliptic B, "
-                        "full-sky lightcone shell 0.5-1.0 box lengths" % (box, N, N),
-            "N": N, "particles": N ** 3, "boxsize_mpc_h": box, "parallelism": "replicas" if world > 1 else "single GPU",
+def workload_config(N, box, world, tensor=False):
+    return {"workload": "PM cycle, box %g Mpc/h, grid %d^3, %d^3 particles, mixed precision, GR, elliptic B%s, "
+                        "full-sky lightcone shell 0.5-1.0 box lengths" % (box, N, N, ", h_ij evolved" if tensor else ""),
+            "N": N, "particles": N ** 3, "boxsize_mpc_h": box, "tensor": bool(tensor),
+            "parallelism": "replicas" if world > 1 else "single GPU",
             "l2": "inputs larger than L2 (particles %.1f GB, fields %.1f GB)" % (N ** 3 * 48 / 1e9, N ** 3 * 12 * 4 / 1e9)}
 
 
@@ -228,7 +230,8 @@ def run_gpu(args, rank, world, local_rank):
     lc_cap = int(0.2 * np_)
 
     def make(precision):
-        c = gev.Context(N, precision=precision, capacity=np_, boxsize=box, vector_method=gev.VECTOR_ELLIPTIC, device=local_rank)
+        c = gev.Context(N, precision=precision, capacity=np_, boxsize=box, vector_method=gev.VECTOR_ELLIPTIC,
+                        tensor=args.tensor, device=local_rank)
         c.set_particles(pos_h, q_h, ids_h, mass)
         c.set_field(gev.FIELD_PHI, phi_h)
         return c
@@ -242,6 +245,8 @@ def run_gpu(args, rank, world, local_rank):
         if world > 1:
             torch.distributed.barrier()
 
+    mem_used = {}
+
     def timed_run(precision, steps, warmup):
         log("context (%s)" % ("fp64" if precision == gev.FP64 else "mixed"))
         c = make(precision)
@@ -253,7 +258,9 @@ def run_gpu(args, rank, world, local_rank):
         for _ in range(warmup):
             cycle(c, st)
         c.synchronize()
-        log("timed cycles")
+        free_b, total_b = torch.cuda.mem_get_info(local_rank)
+        mem_used[precision] = (total_b - free_b) / 1e9
+        log("timed cycles (device memory in use %.1f GB)" % mem_used[precision])
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
         torch.cuda.synchronize()
@@ -302,7 +309,7 @@ def run_gpu(args, rank, world, local_rank):
     stage("deposit_T00_Tij_T0i", deposit)
     stage("solve_phi", lambda: c.solve_phi(True, OMEGA_M, 3 * Hc * dx * dx / st.dtau_old, fourpiG * dx * dx / a,
                                            3 * Hc * Hc * dx * dx, 1 / (dx * dx), 3 * Hc / st.dtau_old))
-    stage("solve_chi", lambda: c.solve_chi(2 * fourpiG * dx * dx / a))
+    stage("solve_chi", lambda: c.solve_chi(2 * fourpiG * dx * dx / a, False, Hc, st.dtau, st.dtau_old))
     # the B solve as the cycle runs it, completing the deposit's T0i sums: timed
     # after a deposit each time, less the deposit's own time
     stage("deposit_and_solve_B", lambda: (deposit(), c.solve_B(fourpiG * dx * dx)))
@@ -311,6 +318,11 @@ def run_gpu(args, rank, world, local_rank):
     stage("lightcone", lambda: c.lightcone(lc, st.tau, st.dtau, st.dtau_old, a, a * Hc, lc_cap, fetch=False))
 
     peak, peak_kind = measured_peaks()
+    # per-stage HBM fractions: algorithmic bytes of the stage / its event time / peak
+    stage_alg = {"deposit_T00_Tij_T0i": "deposit_T00_Tij_T0i", "solve_phi": "solve_phi",
+                 "solve_chi": "solve_chi_tensor" if args.tensor else "solve_chi", "solve_B": "solve_B_sums",
+                 "kick_drift": "kick_drift"}
+    stage_frac = {k: roofline.stage_bytes(v, N, "mixed") / (stages[k] * 1e-3) / 1e9 / peak for k, v in stage_alg.items()}
     # the dominant single kernel: the deposit is one launch; the other stages are
     # several launches (FFT passes; kick/drift + scan + re-bin), each shorter than
     # the deposit in the ncu launch list (profiles/)
@@ -318,6 +330,8 @@ def run_gpu(args, rank, world, local_rank):
     dom_bytes = roofline.stage_bytes(dom, N, "mixed")
     achieved = dom_bytes / (stages[dom] * 1e-3) / 1e9
     step_alg = roofline.step_bytes(N, "mixed")
+    if args.tensor:
+        step_alg += roofline.stage_bytes("solve_chi_tensor", N) - roofline.stage_bytes("solve_chi", N)
     step_gbs = step_alg / (ms_max / args.steps * 1e-3) / 1e9
 
     # ---- validation: P(k) of the mixed run vs an FP64 run from the same ICs ----
@@ -402,9 +416,11 @@ def run_gpu(args, rank, world, local_rank):
             "dtype": "f32 fields/FFT + f64 particle offsets, background and reductions",
             "data": "synthetic: Zel'dovich ICs at z=%g generated on the GPU by gev_ics_zeldovich (Philox4x32-10 white noise, "
                     "seed %d, linear EH no-wiggle P(k))" % (args.z_in, args.seed),
-            "config": workload_config(N, box, world),
+            "config": workload_config(N, box, world, args.tensor),
             "gpu_launches": launches,
             "stage_ms": stages,
+            "stage_hbm_frac": stage_frac,
+            "device_memory_gb": mem_used.get(gev.MIXED),
             "lightcone_counts": lc_counts,
             "lightcone_distance_box": [d_lc - lc_taus[0], d_lc - lc_taus[1]],
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",

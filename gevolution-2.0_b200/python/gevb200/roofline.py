@@ -30,6 +30,8 @@ def stage_bytes(stage, N, precision="mixed", np_=None):
         "solve_phi": n3 * F * (3 + 1 + 1 + 1),
         # read 6 Tij + phi, write 6 spectra; read 6 spectra (as the fused solve needs them), write chi
         "solve_chi": n3 * F * (7 + 6 + 6 + 1),
+        # the same with the tensor state (evolveFTtensor): read and write h_ij and h_ij' (12 spectra each)
+        "solve_chi_tensor": n3 * F * (7 + 6 + 6 + 1 + 12 + 12),
         # read 3 T0i, write 3 spectra; read 3, write 3 B
         "solve_B": n3 * F * (3 + 3 + 3 + 3),
         # the same from the T0i sums, which the x pass completes with phi (one more read)
