@@ -179,6 +179,8 @@ struct CtxBase {
     virtual void field_set(int f, const double *host) = 0;
     virtual void project(uint32_t which, double a, double coeff, int use_phi, int accumulate) = 0;
     virtual void solve_phi(int prepare, double bg, double c, double c2, double c3, double pc, double modif, double *sum, double *phom) = 0;
+    virtual double prepare_t00(double bg, double c, double c2, double c3) = 0;
+    virtual void prepare_tij(double coeff) = 0;
     virtual void solve_chi(double coeff, int cycle0, double hubble, double dtau, double dtau_old, double a2dtau) = 0;
     virtual void solve_B(double coeff, double modif) = 0;
     virtual double kick_drift(const KickDriftParams &kp) = 0;
@@ -709,6 +711,27 @@ template <class R> struct Ctx final : CtxBase {
         }
     }
 
+    // prepareFTsource on its own, in place (main.cu:725, :822): the T00 form
+    // returns the sum of the source field before the preparation
+    double prepare_t00(double bg, double c, double c2, double c3) override
+    {
+        const int N = g.N;
+        prep_t00_pass<R>(N, source.p, phi.p, chi.p, bg, c, c2, c3, partial.p, st);
+        launched("prepare T00");
+        launch_reduce_sum(partial.p, (int64_t)N * N, scal.p, st);
+        launched("reduce");
+        double h = 0.0;
+        ck(cudaMemcpyAsync(&h, scal.p, sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+        sync();
+        return h;
+    }
+
+    void prepare_tij(double coeff) override
+    {
+        prep_tij_pass<R>(g.N, Sij.p, phi.p, coeff, st);
+        launched("prepare Tij");
+    }
+
     void solve_chi(double coeff, int cycle0, double hubble, double dtau, double dtau_old, double a2dtau) override
     {
         const int N = g.N;
@@ -1093,6 +1116,19 @@ int gev_solve_phi(gev_ctx *ctx, int32_t prepare, double bgmodel, double coeff, d
                   double poisson_coeff, double modif, double *T00sum, double *phi_hom)
 {
     return guarded(ctx, [&](gev::CtxBase &c) { c.solve_phi(prepare, bgmodel, coeff, coeff2, coeff3, poisson_coeff, modif, T00sum, phi_hom); });
+}
+
+int gev_prepare_T00(gev_ctx *ctx, double bgmodel, double coeff, double coeff2, double coeff3, double *T00sum)
+{
+    return guarded(ctx, [&](gev::CtxBase &c) {
+        const double s = c.prepare_t00(bgmodel, coeff, coeff2, coeff3);
+        if (T00sum) *T00sum = s;
+    });
+}
+
+int gev_prepare_Tij(gev_ctx *ctx, double coeff)
+{
+    return guarded(ctx, [&](gev::CtxBase &c) { c.prepare_tij(coeff); });
 }
 
 int gev_solve_chi(gev_ctx *ctx, double coeff, int32_t cycle0, double hubble, double dtau, double dtau_old, double a2dtau)

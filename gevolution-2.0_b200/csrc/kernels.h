@@ -89,6 +89,12 @@ template <class R>
 void fz_pass(int N, const FzParams &fp, typename CT<R>::C *data, int64_t stride, typename CT<R>::C *hij,
              typename CT<R>::C *hijp, typename CT<R>::C *bstate, const FftTables<R> &tb, cudaStream_t st);
 int fx_rows_per_block(int N, bool fp64);   // T of the x passes (partial-sum count = N*N/T)
+// prepareFTsource in place: T00 form into source (partial[N*N]: sums of the
+// source per (y, z) row), Tij form on the six Sij planes
+template <class R>
+void prep_t00_pass(int N, R *source, const R *phi, const R *chi, double bg, double c, double c2, double c3, double *partial,
+                   cudaStream_t st);
+template <class R> void prep_tij_pass(int N, R *Sij, const R *phi, double coeff, cudaStream_t st);
 
 // ---- initial conditions ----
 template <class R> void launch_ics_noise(R *out, int64_t n3, uint64_t seed, cudaStream_t st);

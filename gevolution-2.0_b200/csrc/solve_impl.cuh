@@ -221,6 +221,61 @@ void fz_pass(int N, const FzParams &fp, typename CT<R>::C *data, int64_t stride,
     GEV_SWITCH_N(N, (fz_dispatch<R, NN>(fp, a, tb, st)))
 }
 
+// prepareFTsource as standalone passes, in place (the reference's call shape,
+// main.cu:725, :822): T00 form into the source field with per-block sums of
+// the source (row blocks of N points, one partial per (y, z) row); Tij form
+// on the six Sij planes
+template <class R>
+__global__ void k_prep_t00(FxArgs<R> a, int N, R *out, double *partial)
+{
+    __shared__ double red[256 / 32];
+    const int y = blockIdx.x, z = blockIdx.y;
+    double lsum = 0.0;
+    for (int x = threadIdx.x; x < N; x += blockDim.x) {
+        double src;
+        const double r = prep_t00(a, N, x, y, z, src);
+        lsum += src;
+        out[sidx(N, x, y, z)] = (R)r;   // the same point was read above: in place is safe
+    }
+    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = lsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x / 32); w++) s += red[w];
+        partial[y + (int64_t)N * z] = s;
+    }
+}
+
+template <class R>
+__global__ void k_prep_tij(R *Sij, int64_t n3, const R *__restrict__ phi, R coeff, int N)
+{
+    const int y = blockIdx.x, z = blockIdx.y;
+    for (int x = threadIdx.x; x < N; x += blockDim.x) {
+        R o[6];
+#pragma unroll
+        for (int c = 0; c < 6; c++) o[c] = prep_tij(Sij + c * n3, phi, coeff, c, N, x, y, z);
+#pragma unroll
+        for (int c = 0; c < 6; c++) Sij[c * n3 + sidx(N, x, y, z)] = o[c];
+    }
+}
+
+template <class R>
+void prep_t00_pass(int N, R *source, const R *phi, const R *chi, double bg, double c, double c2, double c3, double *partial,
+                   cudaStream_t st)
+{
+    FxArgs<R> a{};
+    a.in = source; a.phi = phi; a.chi = chi;
+    a.bg = bg; a.c = c; a.c2 = c2; a.c3 = c3;
+    k_prep_t00<R><<<dim3(N, N), 256, 0, st>>>(a, N, source, partial);
+}
+
+template <class R>
+void prep_tij_pass(int N, R *Sij, const R *phi, double coeff, cudaStream_t st)
+{
+    k_prep_tij<R><<<dim3(N, N), 128, 0, st>>>(Sij, (int64_t)N * N * N, phi, (R)coeff, N);
+}
+
 #define GEV_SOLVE_INST(R)                                                                                            \
     template void fx_forward<R>(int, int, const R *, int64_t, int, int, const R *, const R *, double, double, double, \
                                 double, CT<R>::C *, int64_t, double *, const FftTables<R> &, cudaStream_t);          \
@@ -228,6 +283,9 @@ void fz_pass(int N, const FzParams &fp, typename CT<R>::C *data, int64_t stride,
     template void fx_inverse<R>(int, const CT<R>::C *, int64_t, R *, int64_t, int, const FftTables<R> &,             \
                                 cudaStream_t);                                                                       \
     template void fz_pass<R>(int, const FzParams &, CT<R>::C *, int64_t, CT<R>::C *, CT<R>::C *, CT<R>::C *,          \
-                             const FftTables<R> &, cudaStream_t);
+                             const FftTables<R> &, cudaStream_t);                                                    \
+    template void prep_t00_pass<R>(int, R *, const R *, const R *, double, double, double, double, double *,          \
+                                   cudaStream_t);                                                                    \
+    template void prep_tij_pass<R>(int, R *, const R *, double, cudaStream_t);
 
 }  // namespace gev

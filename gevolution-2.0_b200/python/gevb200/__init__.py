@@ -86,6 +86,8 @@ _fcomp = _sig("gev_field_components", [_i])
 _project = _sig("gev_project", [_p, _u, _d, _d, _i, _i])
 _solve_phi = _sig("gev_solve_phi", [_p, _i, _d, _d, _d, _d, _d, _d, ctypes.POINTER(_d), ctypes.POINTER(_d)])
 _solve_chi = _sig("gev_solve_chi", [_p, _d, _i, _d, _d, _d, _d])
+_prep_t00 = _sig("gev_prepare_T00", [_p, _d, _d, _d, _d, ctypes.POINTER(_d)])
+_prep_tij = _sig("gev_prepare_Tij", [_p, _d])
 _solve_B = _sig("gev_solve_B", [_p, _d, _d])
 _kick = _sig("gev_kick", [_p, _d, _d, _d, _i, ctypes.POINTER(_d)])
 _drift = _sig("gev_drift", [_p, _d, _d, _d, _i])
@@ -233,6 +235,16 @@ class Context:
         self._ck(_solve_phi(self._h, int(bool(prepare)), bgmodel, coeff, coeff2, coeff3, poisson_coeff, modif,
                             ctypes.byref(s), ctypes.byref(h)))
         return s.value, h.value
+
+    def prepare_T00(self, bgmodel, coeff, coeff2, coeff3):
+        """prepareFTsource (T00 form) in place on the source field; returns the sum of T00."""
+        s = _d()
+        self._ck(_prep_t00(self._h, bgmodel, coeff, coeff2, coeff3, ctypes.byref(s)))
+        return s.value
+
+    def prepare_Tij(self, coeff):
+        """prepareFTsource (Tij form) in place on the Sij field."""
+        self._ck(_prep_tij(self._h, coeff))
 
     def solve_chi(self, coeff, cycle0=False, hubble=0.0, dtau=0.0, dtau_old=0.0, a2dtau=0.0):
         self._ck(_solve_chi(self._h, coeff, int(bool(cycle0)), hubble, dtau, dtau_old, a2dtau))

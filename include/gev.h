@@ -134,6 +134,19 @@ int gev_solve_phi(gev_ctx *ctx, int32_t prepare, double bgmodel, double coeff, d
                   double coeff3, double poisson_coeff, double modif, double *T00sum,
                   double *phi_hom);
 
+/* prepareFTsource as separate, in-place passes, for callers that keep the
+ * reference's unfused call sequence (main.cu:725 then :742, :822 then :829):
+ *   gev_prepare_T00: prepareFTsource(phi, chi, source, bgmodel, source, coeff,
+ *     coeff2, coeff3) (gevolution.hpp:183, :160-171) -- GEV_FIELD_SOURCE becomes
+ *     the nonlinear phi source; T00sum receives the sum of the source field
+ *     before the preparation (the reference's return value).  Follow it with
+ *     gev_solve_phi(prepare = 0, ...).
+ *   gev_prepare_Tij: prepareFTsource(phi, Sij, Sij, coeff) (gevolution.hpp:119,
+ *     :64-107) on GEV_FIELD_SIJ.  gev_solve_chi prepares Sij itself, so this
+ *     pass is for callers that transform Sij by other means. */
+int gev_prepare_T00(gev_ctx *ctx, double bgmodel, double coeff, double coeff2, double coeff3, double *T00sum);
+int gev_prepare_Tij(gev_ctx *ctx, double coeff);
+
 /* Chi update: prepareFTsource(phi, Sij, Sij, coeff) (gevolution.hpp:119;
  * main.cu:822) fused into the 6 forward FFTs (main.cu:829), projectFTscalar
  * (:251; main.cu:873) and the backward FFT into GEV_FIELD_CHI (main.cu:895).

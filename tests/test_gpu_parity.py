@@ -214,6 +214,41 @@ def test_solve_phi(prec, N):
 
 
 @pytest.mark.parametrize("prec", PRECS)
+def test_prepare_passes(prec):
+    """gev_prepare_T00 / gev_prepare_Tij (prepareFTsource as in-place passes,
+    gevolution.hpp:183, :119) against the oracle, and the unfused phi update
+    (prepare, then gev_solve_phi without preparation) against the fused one."""
+    N = 32
+    o = oracle()
+    dx = 1.0 / N
+    source = 0.32 * (1 + 50 * smooth_field(N, 81))
+    phi = smooth_field(N, 82, 1e-5)
+    chi = smooth_field(N, 83, 1e-6)
+    Tij = np.concatenate([smooth_field(N, 84 + k, 1e-3) for k in range(6)])
+    H, dtau_old, a, fourpiG = 0.8, 0.01, 0.3, 1.5 * 320 ** 2 / 2997.92458 ** 2
+    args = (0.32, 3 * H * dx * dx / dtau_old, fourpiG * dx * dx / a, 3 * H * H * dx * dx)
+    res = np.zeros(N ** 3)
+    s_ref = o.prepare_T00(N, ptr(phi), ptr(chi), ptr(source), *args, ptr(res))
+    S = np.zeros(6 * N ** 3)
+    coeff = 2 * fourpiG * dx * dx / a
+    o.prepare_Tij(N, ptr(phi), ptr(Tij), coeff, ptr(S))
+    with make_ctx(N, prec, 8) as c:
+        c.set_particles(np.zeros((1, 3)), np.zeros((1, 3)))
+        c.set_field(gev.FIELD_SOURCE, source); c.set_field(gev.FIELD_PHI, phi); c.set_field(gev.FIELD_CHI, chi)
+        c.set_field(gev.FIELD_SIJ, Tij)
+        s = c.prepare_T00(*args)
+        assert abs(s / s_ref - 1) < (1e-12 if prec == gev.FP64 else 1e-6)
+        assert rel_err(c.get_field(gev.FIELD_SOURCE), res) < TOL[prec]
+        c.prepare_Tij(coeff)
+        assert rel_err(c.get_field(gev.FIELD_SIJ).ravel(), S) < TOL[prec]
+        c.solve_phi(False, 0, 0, 0, 0, 1 / (dx * dx), 3 * H / dtau_old)
+        unfused = c.get_field(gev.FIELD_PHI)
+        c.set_field(gev.FIELD_SOURCE, source); c.set_field(gev.FIELD_PHI, phi)
+        c.solve_phi(True, *args, 1 / (dx * dx), 3 * H / dtau_old)
+        assert rel_err(unfused, c.get_field(gev.FIELD_PHI)) < (1e-13 if prec == gev.FP64 else 1e-6)
+
+
+@pytest.mark.parametrize("prec", PRECS)
 def test_fft_round_trip_full_size(prec):
     """A Poisson solve with modif >> k^2 is the identity up to k^2/modif: the
     forward + inverse passes reproduce the input at a production grid size."""
