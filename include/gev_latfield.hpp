@@ -47,10 +47,11 @@
 //     particle update;
 //   - plan_Bi.execute(FFT_FORWARD) and projectFTvector are recorded,
 //     plan_Bi.execute(FFT_BACKWARD) runs gev_solve_B;
-//   - a projection overwrites its target field on the first projection after
-//     that field was consumed by a solve (or after zero(field)), and adds to it
-//     afterwards -- the reference zeroes the targets with thrust::fill_n before
-//     projecting (main.cu:616, :681, :840), which this header replaces;
+//   - a projection overwrites its target field on the first projection of a
+//     cycle (after the particle update, after a solve consumed the field, or
+//     after zero(field)) and adds to it afterwards -- the reference zeroes the
+//     targets with thrust::fill_n before projecting (main.cu:616, :681, :840),
+//     which this header replaces;
 //   - updateHalo and projection_*_comm do nothing: neighbours on one GPU come
 //     from periodic indexing;
 //   - DeviceStagingBuffer keeps its values in host memory; the functions above
@@ -191,6 +192,14 @@ public:
         return acc;
     }
     void consumed(int field) { fresh_[field] = false; }
+    // the particle update ends a cycle: the next cycle's projections start
+    // from zero, as main.cu zeroes their targets at the top of its loop
+    void cycle_end()
+    {
+        consumed(GEV_FIELD_SOURCE);
+        consumed(GEV_FIELD_SIJ);
+        consumed(GEV_FIELD_BI);
+    }
 
     // backlog slot of a caller-side ID log (lightcone shells)
     int shell_of(const void *idlog)
@@ -388,6 +397,7 @@ public:
     Real updateVel(update_q_functor, double dtau, Field<Real> **, int nfield, double *params)
     {
         box().flush();
+        box().cycle_end();
         double maxvel = 0.;
         gev_b200::check(box().ctx(), gev_kick(box().ctx(), dtau, params[0], params[1], nfield, &maxvel));
         return (Real)maxvel;
@@ -395,6 +405,7 @@ public:
     void moveParticles(update_pos_functor, double dtau, Field<Real> **, int nfield, double *params)
     {
         box().flush();
+        box().cycle_end();
         gev_b200::check(box().ctx(), gev_drift(box().ctx(), dtau, params[0], params[1], nfield));
     }
     Real updateVel(update_q_Newton_functor, double, Field<Real> **, int, double *)

@@ -31,7 +31,10 @@ double maxrel(const std::vector<double> &x, const std::vector<double> &y)
     return m / s;
 }
 
-int run(bool mixed, bool elliptic, bool tensor, double tol_pos, double tol_field)
+// tol_hom: the zero mode phi_hom is the mean of the prepared source over
+// N^3 points, which nearly cancels (the background model is subtracted); in
+// FP32 its relative rounding is far above that of the fields
+int run(bool mixed, bool elliptic, bool tensor, double tol_pos, double tol_field, double tol_hom)
 {
     const int N = 32, ncycles = 3;
     const int64_t n = (int64_t)N * N * N;
@@ -189,7 +192,7 @@ int run(bool mixed, bool elliptic, bool tensor, double tol_pos, double tol_field
                 mixed ? "mixed" : "fp64", elliptic ? "elliptic" : "parabolic", tensor ? " tensor" : "", dp, dq, dphi, dchi, dB,
                 dh, da, dv, dT, dph);
     const bool ok = dp < tol_pos && dq < tol_field && dphi < tol_field && dchi < tol_field && dB < tol_field && dh < tol_field &&
-                    da < 1e-14 && dv < tol_field && dT < tol_field && dph < 10 * tol_field;
+                    da < 1e-14 && dv < tol_field && dT < tol_field && dph < tol_hom;
     return ok ? 0 : 1;
 }
 
@@ -198,8 +201,8 @@ int run(bool mixed, bool elliptic, bool tensor, double tol_pos, double tol_field
 int main()
 {
     try {
-        int rc = run(false, true, false, 1e-10, 1e-10);
-        rc |= run(true, false, true, 1e-5, 1e-4);
+        int rc = run(false, true, false, 1e-10, 1e-10, 1e-9);
+        rc |= run(true, false, true, 1e-5, 1e-4, 1e-2);
         return rc;
     } catch (const std::exception &e) {
         std::fprintf(stderr, "%s\n", e.what());
