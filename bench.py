@@ -152,7 +152,11 @@ def lightcone_args(gev, d):
 
 SINGLE_KERNEL_STAGES = ("deposit_T00_Tij_T0i",)
 
-# DRAM bytes per launch measured by ncu at 256^3 (mixed precision), per stage kernel
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
+# ncu --set full capture of each deposit kernel at 256^3 in mixed precision
+# (python bench.py --N 256 --steps 2 --warmup 3 --no-fp64 --no-e2e --no-cpu
+# --no-adjoint under ncu -k regex:k_deposit -c 5), scaled by the particle count;
+# valid while those kernels are unchanged
 NCU_TRAFFIC_256 = {"deposit_T00_Tij_T0i": 0.7494e9 + 0.6380e9, "deposit_T00_Tij": 0.7451e9 + 0.4423e9,
                    "deposit_T0i": 0.7434e9 + 0.1865e9}
 
@@ -425,8 +429,8 @@ def run_gpu(args, rank, world, local_rank):
             "lightcone_distance_box": [d_lc - lc_taus[0], d_lc - lc_taus[1]],
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": ncu_traffic(dom, N),
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the same kernel at 256^3 "
-                                           "(profiles/particle_kernels_256_mixed_ncu.md), scaled by the particle count",
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of the same "
+                                           "kernel at 256^3, mixed precision, scaled by the particle count",
                          "algorithmic_bytes_per_launch": dom_bytes,
                          "step_algorithmic_bytes": step_alg, "step_achieved_gbs": step_gbs, "step_frac": step_gbs / peak},
             "clocks": clk,
