@@ -31,6 +31,8 @@ assert ctypes.sizeof(Gadget2Header) == 256
 
 _write = _sig("gev_gadget2_write", [ctypes.c_char_p, ctypes.POINTER(Gadget2Header), _p, _p, _p, _l])
 _snapshot = _sig("gev_snapshot_gadget2", [_p, ctypes.c_char_p, ctypes.POINTER(Gadget2Header), _i32])
+_read = _sig("gev_gadget2_read", [ctypes.c_char_p, ctypes.POINTER(Gadget2Header), _p, _p, _p, _l, ctypes.POINTER(_l)])
+_load = _sig("gev_particles_load_gadget2", [_p, ctypes.c_char_p, _d, ctypes.POINTER(Gadget2Header)])
 
 
 def header(a, boxsize_mpc_h, omega_m, omega_lambda, h, numpcl, omega_cdm=None, tracer_factor=1):
@@ -62,8 +64,35 @@ def snapshot(ctx, path, hdr, tracer_factor=1):
         raise GevError(rc, "gev_snapshot_gadget2 failed for %s" % path)
 
 
+def read_c(path):
+    """gev_gadget2_read: (header, pos [n,3] float32, vel [n,3] float32, ids int64)."""
+    hdr = Gadget2Header()
+    n = _l()
+    rc = _read(str(path).encode(), ctypes.byref(hdr), None, None, None, 0, ctypes.byref(n))
+    if rc != 0:
+        raise GevError(rc, "gev_gadget2_read failed for %s" % path)
+    pos = np.empty((n.value, 3), dtype=np.float32)
+    vel = np.empty((n.value, 3), dtype=np.float32)
+    ids = np.empty(n.value, dtype=np.int64)
+    rc = _read(str(path).encode(), ctypes.byref(hdr), pos.ctypes.data_as(_p), vel.ctypes.data_as(_p),
+               ids.ctypes.data_as(_p), n.value, ctypes.byref(n))
+    if rc != 0:
+        raise GevError(rc, "gev_gadget2_read failed for %s" % path)
+    return hdr, pos, vel, ids
+
+
+def load(ctx, path, mass):
+    """gev_particles_load_gadget2: the file's particles into the context; returns the header."""
+    hdr = Gadget2Header()
+    rc = _load(ctx._h, str(path).encode(), float(mass), ctypes.byref(hdr))
+    if rc != 0:
+        raise GevError(rc, "gev_particles_load_gadget2 failed for %s" % path)
+    return hdr
+
+
 def read(path):
-    """(header, pos [n,3] float32, vel [n,3] float32, ids int64) of a Gadget-2 file."""
+    """(header, pos [n,3] float32, vel [n,3] float32, ids int64) of a Gadget-2 file, parsed in Python
+    (an independent reading of the byte layout)."""
     raw = open(path, "rb").read()
     off = 0
     blocks = []

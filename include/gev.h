@@ -335,6 +335,19 @@ typedef struct {
  * header's length unit) as one Gadget-2 file. */
 int gev_gadget2_write(const char *path, const gev_gadget2_header *hdr, const float *pos, const float *vel,
                       const int64_t *ids, int64_t n);
+/* Read one Gadget-2 file of this layout (one particle species, 8-byte IDs):
+ * the header, then -- when pos, vel and ids are given -- the POS, VEL and ID
+ * blocks into host arrays of `capacity` particles (GEV_ERR_CAPACITY if the
+ * file holds more; n_out receives the count either way).  With pos, vel and
+ * ids all NULL only the header and the count are read. */
+int gev_gadget2_read(const char *path, gev_gadget2_header *hdr, float *pos, float *vel, int64_t *ids, int64_t capacity,
+                     int64_t *n_out);
+/* The particles of a Gadget-2 file into the context, converted as
+ * perfParticles_gevolution::loadGadget2 does (Particles_gevolution.hpp:183,
+ * :2565-2568; the reference's particle-file ICs, ic_read.hpp): positions /
+ * BoxSize, momenta = vel a^1.5 GADGET_VELOCITY_CONVERSION with a = hdr.time.
+ * hdr_out (may be NULL) receives the header. */
+int gev_particles_load_gadget2(gev_ctx *ctx, const char *path, double mass, gev_gadget2_header *hdr_out);
 /* Snapshot of the context's particles (saveGadget2, Particles_gevolution.hpp:
  * 218-420 without the redshift interpolation): particles whose ID is a
  * multiple of tracer_factor, pos * hdr->BoxSize, vel = q / a^1.5 in Gadget

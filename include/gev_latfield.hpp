@@ -25,7 +25,8 @@
 //                  double dtau, double dtau_old)                                                               :537
 //   perfParticles::updateVel(update_q_functor(), dtau, fields, nfield, params) -> max velocity        main.cu:1232
 //   perfParticles::moveParticles(update_pos_functor(), dtau, fields, nfield, params)                   main.cu:1258
-//   perfParticles_gevolution::saveGadget2 (snapshot and lightcone forms)             Particles_gevolution.hpp:180-181
+//   perfParticles_gevolution::saveGadget2 (snapshot and lightcone forms), loadGadget2
+//                                                                                  Particles_gevolution.hpp:180-183
 //   PlanFFT<Imag>::execute(FFT_FORWARD | FFT_BACKWARD), Field<Real>::updateHalo()
 //   Hconf, rungekutta4bg, particleHorizon                                          background.hpp:200, :235, :268
 //
@@ -385,8 +386,13 @@ public:
     // the particles of the box (box units, momentum per unit mass; IDs may be null)
     void initialize(const double *pos, const double *q, const int64_t *ids, int64_t n, double mass)
     {
+        mass_ = mass;
         gev_b200::check(box().ctx(), gev_particles_set(box().ctx(), pos, q, ids, n, mass));
     }
+    // part_simple_info.mass of the particles loaded from files (the reference sets it after
+    // loadGadget2, ic_read.hpp)
+    void set_mass(double mass) { mass_ = mass; }
+    double mass() const { return mass_; }
     long num_particles() const
     {
         int64_t n = 0;
@@ -419,11 +425,22 @@ public:
 
 private:
     gev_b200::Box *box_ = nullptr;
+    double mass_ = 0.;
 };
 
 template <class part, class part_info> class perfParticles_gevolution : public perfParticles<part, part_info> {
 public:
     using perfParticles<part, part_info>::perfParticles;
+
+    // particle file (Particles_gevolution.hpp:183): every particle of one
+    // Gadget-2 file, with the mass given by set_mass / initialize
+    template <class Header> void loadGadget2(std::string filename, Header &hdr)
+    {
+        gev_gadget2_header h;
+        gev_b200::check(this->box().ctx(), gev_particles_load_gadget2(this->box().ctx(), filename.c_str(), this->mass(), &h));
+        static_assert(sizeof(Header) == sizeof(gev_gadget2_header), "gadget2_header is 256 bytes (metadata.hpp:159-178)");
+        std::memcpy(&hdr, &h, sizeof h);
+    }
 
     // snapshot (Particles_gevolution.hpp:180): particles whose ID is a multiple
     // of tracer_factor, positions x BoxSize, velocities q / a^1.5 with a =
