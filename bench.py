@@ -338,15 +338,43 @@ def run_gpu(args, rank, world, local_rank):
         step_alg += roofline.stage_bytes("solve_chi_tensor", N) - roofline.stage_bytes("solve_chi", N)
     step_gbs = step_alg / (ms_max / args.steps * 1e-3) / 1e9
 
-    # ---- validation: P(k) of the mixed run vs an FP64 run from the same ICs ----
+    # ---- validation: P(k) and particle displacements of the mixed run vs an
+    # FP64 run from the same ICs (the stage timings above leave the particle
+    # state as the timed cycles left it: their kick and drift use dtau = 0) ----
     log("stages %s" % json.dumps(stages))
     pk_mixed = c.power_spectrum(1024)
+
+    def by_id(ctx):
+        """final positions in ID order (IDs are the 0..N^3-1 cell indexes of the ICs)"""
+        p_, _, i_ = ctx.get_particles()
+        out = np.empty_like(p_)
+        out[i_] = p_
+        return out
+
+    pos0 = np.empty_like(pos_h)
+    pos0[ids_h] = pos_h
+    pos_mixed = None if args.no_fp64 else by_id(c)
     c.close()
     del c
     fp64 = None
     if not args.no_fp64:
         c64, st64, ms64, _, _, _, _ = timed_run(gev.FP64, args.steps, args.warmup)
         pk64 = c64.power_spectrum(1024)
+        pos64 = by_id(c64)
+
+        def disp(p):
+            d = p - pos0
+            d -= np.round(d)
+            return d
+
+        d64 = disp(pos64)
+        dmx = disp(pos_mixed)
+        rms64 = float(np.sqrt((d64 ** 2).sum(axis=1).mean()))
+        rmsmx = float(np.sqrt((dmx ** 2).sum(axis=1).mean()))
+        dd = dmx - d64
+        dd -= np.round(dd)
+        rms_diff = float(np.sqrt((dd ** 2).sum(axis=1).mean()))
+        del pos64, d64, dmx, dd
         occ = pk64[4] > 0
         kb = pk64[0][occ]
         kny = math.pi * N
@@ -355,6 +383,8 @@ def run_gpu(args, rank, world, local_rank):
         fp64 = {"value": np_ * args.steps / (ms64 * 1e-3) / 1e6, "ms_per_step": ms64 / args.steps,
                 "mixed_speedup": (np_ * args.steps / (ms_max * 1e-3)) / (np_ * args.steps / (ms64 * 1e-3)),
                 "pk_max_rel_err_vs_fp64": float(rel.max()), "pk_k_range_h_per_mpc": [float(kb[sel].min() / box), float(kb[sel].max() / box)],
+                "rms_displacement_cells_fp64": rms64 * N, "rms_disp_rel_err_vs_fp64": abs(rmsmx / rms64 - 1.0),
+                "per_particle_disp_rel_err_vs_fp64": rms_diff / rms64,
                 "cycles_compared": args.warmup + args.steps}
         c64.close()
         del c64
