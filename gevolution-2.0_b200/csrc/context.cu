@@ -203,7 +203,7 @@ template <class R> struct Ctx final : CtxBase {
     DBuf<C> tw_full, tw_half;
     DBuf<double> k2;
     DBuf<double2> ks;
-    DBuf<uint32_t> cellA, cellB, bucket, rank, inv, counts, bstart, bsums;
+    DBuf<uint32_t> cellA, cellB, bucket, rank, inv, counts, bstart, bsums, depwork;
     DBuf<double> offA, offB;
     DBuf<R> qA, qB;
     DBuf<int64_t> idA, idB;
@@ -270,6 +270,7 @@ template <class R> struct Ctx final : CtxBase {
         counts.alloc(nb, "bucket counts");
         bstart.alloc(nb + 1, "bucket starts");
         bsums.alloc((nb + 1023) / 1024 + 1, "scan");
+        depwork.alloc(g.ntiles + 2, "deposit work list");
         ck(cudaMemsetAsync(bstart.p, 0, (nb + 1) * sizeof(uint32_t), st), "memset");
         partial.alloc((int64_t)N * N, "partials");
         scal.alloc(4, "scalars");
@@ -352,6 +353,16 @@ template <class R> struct Ctx final : CtxBase {
     {
         ck(cudaGetLastError(), what);
         launch_count += kernels;
+    }
+
+    // a tile deposit: the tile launch and the dense-tile launch
+    void deposit(int kind, bool use_phi, const DepOut<R> &o, double a, double m00, double mij, double m0i, int accumulate,
+                 const char *what)
+    {
+        ck(cudaMemsetAsync(depwork.p, 0, 2 * sizeof(uint32_t), st), "memset");
+        launch_deposit<R>(kind, use_phi, cur(), bstart.p, g.N, phi.p, o, a, m00, mij, m0i, accumulate, depwork.p, derr.p,
+                          st);
+        launched(what, 2);
     }
     int64_t kernel_launches() const override { return launch_count; }
 
@@ -609,7 +620,6 @@ template <class R> struct Ctx final : CtxBase {
         if ((which & GEV_PROJ_CIC) && (which & GEV_PROJ_T00)) throw ArgError("CIC and T00 both target the source field");
         if (use_phi && a <= 0.0 && (which & (GEV_PROJ_T00 | GEV_PROJ_TIJ))) throw ArgError("scale factor must be positive");
         const double n3 = (double)g.n3;   // 1/dx^3
-        const PView<R> v = cur();
         if ((which & GEV_PROJ_T00) || (which & GEV_PROJ_TIJ)) {
             double m00 = mass * coeff * n3;
             if (use_phi) m00 /= a;                       // gevolution.hpp:1731, :1750
@@ -627,20 +637,17 @@ template <class R> struct Ctx final : CtxBase {
                 kind = DEP_TIJ;
                 for (int c = 0; c < 6; c++) o.p[c] = Sij.p + c * g.n3;
             }
-            launch_deposit<R>(kind, use_phi != 0, v, bstart.p, g.N, phi.p, o, a, m00, mij, 0.0, accumulate, derr.p, st);
-            launched("deposit T00/Tij");
+            deposit(kind, use_phi != 0, o, a, m00, mij, 0.0, accumulate, "deposit T00/Tij");
         }
         if (which & GEV_PROJ_CIC) {
             DepOut<R> o{};
             o.p[0] = source.p;
-            launch_deposit<R>(DEP_T00, false, v, bstart.p, g.N, phi.p, o, 1.0, mass * coeff * n3, 0.0, 0.0, accumulate, derr.p, st);
-            launched("deposit CIC");
+            deposit(DEP_T00, false, o, 1.0, mass * coeff * n3, 0.0, 0.0, accumulate, "deposit CIC");
         }
         if (which & GEV_PROJ_T0I) {
             DepOut<R> o{};
             for (int c = 0; c < 3; c++) o.p[c] = Bi.p + c * g.n3;
-            launch_deposit<R>(DEP_T0I, use_phi != 0, v, bstart.p, g.N, phi.p, o, 1.0, mass * coeff * n3, 0.0, 0.0, accumulate, derr.p, st);
-            launched("deposit T0i");
+            deposit(DEP_T0I, use_phi != 0, o, 1.0, mass * coeff * n3, 0.0, 0.0, accumulate, "deposit T0i");
             bi_sums = false;
             t0i_pending = false;
         }
@@ -670,9 +677,8 @@ template <class R> struct Ctx final : CtxBase {
         o.p[0] = source.p;
         for (int c = 0; c < 6; c++) o.p[1 + c] = Sij.p + c * g.n3;
         for (int c = 0; c < 3; c++) o.p[7 + c] = Bi.p + c * g.n3;
-        launch_deposit<R>(DEP_T00_TIJ_S0I, true, cur(), bstart.p, g.N, phi.p, o, a, mass * n3 / a, mass * n3 / a,
-                          mass * n3, 0, derr.p, st);   // gevolution.hpp:1731, :1750, :2584; T0i mass * coeff / dx^3
-        launched("deposit T00/Tij/T0i sums");
+        // gevolution.hpp:1731, :1750, :2584; T0i mass * coeff / dx^3
+        deposit(DEP_T00_TIJ_S0I, true, o, a, mass * n3 / a, mass * n3 / a, mass * n3, 0, "deposit T00/Tij/T0i sums");
         bi_sums = true;
     }
 

@@ -8,10 +8,13 @@
 //   1. turns each particle into a short record of per-particle factors (in the
 //      field precision R) and finds the one of the 9^3 cells of the tile's
 //      reach (relative cell -1..7 per axis) that it lies in;
-//   2. finds the records of each reach cell: when the reach fits one chunk
-//      (the common case) they already form one run, because the re-binning
-//      keeps small buckets in (cell, particle ID) order; denser tiles sort
-//      record indexes by cell (counting sort) chunk by chunk;
+//   2. finds the records of each reach cell: when every candidate bucket
+//      holds at most REBIN_SORT_MAX particles they already form one run of
+//      the candidates' concatenation, because the re-binning keeps buckets
+//      that small in (cell, particle ID) order -- the concatenation is taken
+//      in chunks of records that fit shared memory (one chunk in the common
+//      case); tiles that touch a larger bucket sort record indexes by cell
+//      (counting sort) chunk by chunk;
 //   3. lets every vertex thread walk the 8 cells whose stencil covers it and
 //      accumulate the contributions in registers -- no shared-memory atomics
 //      on the accumulation path, each output vertex written once with plain
@@ -19,10 +22,15 @@
 //      gevolution.hpp:1543, is not needed on one GPU).
 // The result does not depend on the order in which the particles were given
 // (bitwise reproducible, for unique particle IDs):
-//   - single chunk: each vertex sums in R in the fixed order (source cell, ID);
-//   - denser tiles take several chunks and accumulate 64-bit fixed point with
-//     a per-CTA, per-component scale from an upper bound of the contributions
-//     and the particle count, so the sum is exact integer arithmetic.
+//   - sorted candidates: each vertex sums in R in the fixed order (source
+//     cell, ID), chunk after chunk;
+//   - tiles that touch a bucket above REBIN_SORT_MAX (kept in slot order)
+//     accumulate 64-bit fixed point with a per-CTA, per-component scale from
+//     an upper bound of the contributions and the particle count, so the sum
+//     is exact integer arithmetic.
+// Tiles whose reach fits one chunk are done by the tile launch; it lists the
+// others for a second, dense-tile launch, so that the common case's kernel
+// holds only the single-chunk path (fewer registers, no spills).
 //
 // Arithmetic follows the reference functors term by term:
 //   particle_T00_project  gevolution.hpp:1729-1854
@@ -50,14 +58,23 @@ constexpr int DEP_NT = 512;   // one thread per tile vertex
 #define GEV_DEP_CH_S_F 768
 #endif
 
-// records per chunk (shared-memory budget) and the fixed-point exponent limit
-template <class R, int KIND = DEP_T00> struct DepCh;
-template <int KIND> struct DepCh<float, KIND> {
-    static constexpr int v = KIND == DEP_T00_TIJ_S0I ? GEV_DEP_CH_S_F : 1024;
+#ifndef GEV_DEP_CH_S_F_DENSE
+#define GEV_DEP_CH_S_F_DENSE 768
+#endif
+
+// records per chunk (shared-memory budget) and the fixed-point exponent limit;
+// DENSE: the chunks of the dense-tile launch
+template <class R, int KIND = DEP_T00, bool DENSE = false> struct DepCh;
+template <int KIND, bool DENSE> struct DepCh<float, KIND, DENSE> {
+    static constexpr int v = KIND == DEP_T00_TIJ_S0I ? (DENSE ? GEV_DEP_CH_S_F_DENSE : GEV_DEP_CH_S_F) : 1024;
     static constexpr int EMAX = 120;
 };
-template <int KIND> struct DepCh<double, KIND> { static constexpr int v = 768; static constexpr int EMAX = 1000; };
+template <int KIND, bool DENSE> struct DepCh<double, KIND, DENSE> {
+    static constexpr int v = 768;
+    static constexpr int EMAX = 1000;
+};
 static_assert(DepCh<float>::v <= REBIN_SORT_MAX && DepCh<float, DEP_T00_TIJ_S0I>::v <= REBIN_SORT_MAX &&
+                  DepCh<float, DEP_T00_TIJ_S0I, true>::v <= REBIN_SORT_MAX &&
                   DepCh<double>::v <= REBIN_SORT_MAX,
               "a single-chunk deposit must only see buckets that the re-binning keeps sorted");
 
@@ -317,11 +334,11 @@ template <class R, int NFP> __device__ __forceinline__ void load_record(const R 
     }
 }
 
-template <class R, int KIND>
+template <class R, int KIND, bool DENSE = false>
 __host__ __device__ constexpr size_t dep_smem_bytes()
 {
-    return (size_t)DepShape<KIND>::NFP * DepCh<R, KIND>::v * sizeof(R) + (size_t)(2 * 730) * sizeof(int) +
-           (size_t)3 * DepCh<R, KIND>::v * sizeof(uint16_t);
+    return (size_t)DepShape<KIND>::NFP * DepCh<R, KIND, DENSE>::v * sizeof(R) + (size_t)(2 * 730) * sizeof(int) +
+           (size_t)3 * DepCh<R, KIND, DENSE>::v * sizeof(uint16_t);
 }
 
 // Resident CTAs per SM the register budget is sized for.  The kernel is bound
@@ -333,15 +350,24 @@ template <class R, int KIND> struct DepMinBlocks { static constexpr int v = size
 template <> struct DepMinBlocks<float, DEP_T0I> { static constexpr int v = GEV_DEP_MINB_T0I_F; };
 template <> struct DepMinBlocks<float, DEP_T00_TIJ_S0I> { static constexpr int v = GEV_DEP_MINB_S_F; };
 
-// outputs: component c is written to out[c] (N^3 plane each)
-template <class R, int KIND, bool USE_PHI>
-__global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v) k_deposit(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt,
-                                                       const R *__restrict__ phi, DepOut<R> out, double a, double m00,
-                                                       double mij, double m0i, int accumulate, int *err, FastDiv fN)
+// The dense-tile launch holds only the paths for tiles whose reach takes
+// several chunks, with a register budget of its own.
+#ifndef GEV_DEP_MINB_DENSE
+#define GEV_DEP_MINB_DENSE 3
+#endif
+
+// One tile's deposit; outputs: component c is written to out[c] (N^3 plane
+// each).  The tile launch (DENSE = false) finishes every tile whose reach fits
+// one chunk and appends the others to the work list work[2..] (count in
+// work[0]); the dense-tile launch (DENSE = true) takes them from the list.
+template <class R, int KIND, bool USE_PHI, bool DENSE>
+__device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PView<R> &p, const uint32_t *__restrict__ bstart,
+                                             int N, int nt, const R *__restrict__ phi, const DepOut<R> &out, double a,
+                                             double m00, double mij, double m0i, int accumulate, int *err, FastDiv fN)
 {
     using S = DepShape<KIND>;
     constexpr int NC = S::NC, NF = S::NF, NFP = S::NFP;
-    constexpr int CH = DepCh<R, KIND>::v;
+    constexpr int CH = DepCh<R, KIND, DENSE>::v;
     extern __shared__ __align__(16) unsigned char dsm[];
     R *rec = reinterpret_cast<R *>(dsm);                      // [CH][NFP]
     int *cstart = reinterpret_cast<int *>(rec + CH * NFP);    // 730
@@ -358,7 +384,6 @@ __global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v) k_deposit(PV
     __shared__ int wsum[DEP_NT / 32];
 
     const int t = threadIdx.x;
-    const int tile = blockIdx.x;
     const int tx = tile % nt, ty = (tile / nt) % nt, tz = tile / (nt * nt);
     const int x0 = tx * 8, y0 = ty * 8, z0 = tz * 8;
 
@@ -410,6 +435,13 @@ __global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v) k_deposit(PV
         return;
     }
     const bool multi = total > (uint32_t)CH;
+    if constexpr (!DENSE) {
+        if (multi) {
+            // several chunks: the dense-tile launch takes this tile
+            if (t == 0) work[2 + atomicAdd(&work[0], 1u)] = (uint32_t)tile;
+            return;
+        }
+    }
 
     // exclusive scan of the 729 cell counts into cstart (two cells per thread)
     auto scan_cells = [&]() {
@@ -450,21 +482,11 @@ __global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v) k_deposit(PV
     }
     const int64_t gout = sidx(N, x0 + vx, y0 + vy, z0 + vz);
 
-    if (!multi) {
-        // Single chunk (the common case).  The re-binning keeps every bucket
-        // this small in (cell, particle ID) order, so in the concatenation of
-        // the candidate buckets the records of each reach cell form one run,
-        // already ordered by ID: records stay at their load position and every
-        // vertex sums its contributions in the field precision in a fixed
-        // order (source cell, then ID) -- independent of the order in which
-        // the particles were given.
-        const int n = (int)total;
-        // the neighbours' particles (the own ones are loaded already)
-#pragma unroll
-        for (int u = 0; u < PP; u++) {
-            const int j = t + u * DEP_NT;
-            if (j < n && (uint32_t)j >= own_n) raw[u] = load_particle(p, seg_find(seg_lo, seg_pre, (uint32_t)j));
-        }
+    // One chunk of n <= CH candidates whose particles are in raw[]: records
+    // stay at their load position and every vertex adds its contributions to
+    // acc in the field precision, in the fixed order (source cell, then ID).
+    const int lc0 = (vx + 1) + 9 * ((vy + 1) + 9 * (vz + 1));
+    auto sorted_chunk = [&](int n, RawParticle<R> (&raw)[PP], R (&acc)[NC]) {
         // 1. record j at position j, and the reach cell it came from
 #pragma unroll
         for (int u = 0; u < PP; u++) {
@@ -502,11 +524,7 @@ __global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v) k_deposit(PV
             }
             if (bad) atomicOr(err, ERR_BAD_ORDER);
         }
-        // 5. gather: the vertex receives from the cells v - b, b in {0,1}^3
-        R acc[NC];
-#pragma unroll
-        for (int c = 0; c < NC; c++) acc[c] = 0;
-        const int lc0 = (vx + 1) + 9 * ((vy + 1) + 9 * (vz + 1));
+        // 4. gather: the vertex receives from the cells v - b, b in {0,1}^3
 #pragma unroll
         for (int b = 0; b < 8; b++) {
             const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
@@ -518,11 +536,63 @@ __global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v) k_deposit(PV
                 gather_sum<R, KIND, USE_PHI>(r, bx, by, bz, phv, phx, phy, phz, acc);
             }
         }
+    };
+    auto write_acc = [&](const R (&acc)[NC]) {
 #pragma unroll
         for (int c = 0; c < NC; c++) {
             R *o = out.p[c];
             o[gout] = accumulate ? (R)(o[gout] + acc[c]) : acc[c];
         }
+    };
+
+    if constexpr (!DENSE) {
+        // Single chunk (the common case).  The re-binning keeps every bucket
+        // this small in (cell, particle ID) order, so in the concatenation of
+        // the candidate buckets the records of each reach cell form one run,
+        // already ordered by ID -- the sum is independent of the order in
+        // which the particles were given.
+        const int n = (int)total;
+        // the neighbours' particles (the own ones are loaded already)
+#pragma unroll
+        for (int u = 0; u < PP; u++) {
+            const int j = t + u * DEP_NT;
+            if (j < n && (uint32_t)j >= own_n) raw[u] = load_particle(p, seg_find(seg_lo, seg_pre, (uint32_t)j));
+        }
+        R acc[NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++) acc[c] = 0;
+        sorted_chunk(n, raw, acc);
+        write_acc(acc);
+        return;
+    } else {
+
+    // Every candidate bucket holds at most REBIN_SORT_MAX particles: the
+    // re-binning kept each in (cell, particle ID) order, so the concatenation
+    // of the candidates is in a canonical order in which each reach cell's
+    // records form one run.  It is taken in chunks of CH, each summed as the
+    // single chunk above; a run that crosses a chunk boundary is summed in two
+    // parts, at a position fixed by that canonical order -- still independent
+    // of the order in which the particles were given.
+    if (__syncthreads_and(t >= 64 || seg_hi[t] - seg_lo[t] <= (uint32_t)REBIN_SORT_MAX)) {
+        R acc[NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++) acc[c] = 0;
+        for (uint32_t base = 0; base < total; base += (uint32_t)CH) {
+            const int n = (int)min((uint32_t)CH, total - base);
+            if (base > 0) {
+                // records and runs of the previous chunk are done with
+                __syncthreads();
+                for (int c = t; c < 730; c += DEP_NT) { cstart[c] = 0; ccount[c] = 0; }
+            }
+            // the chunk's particles (of the first chunk, the own ones are loaded already)
+#pragma unroll
+            for (int u = 0; u < PP; u++) {
+                const uint32_t j = base + (uint32_t)(t + u * DEP_NT);
+                if (t + u * DEP_NT < n && (base > 0 || j >= own_n)) raw[u] = load_particle(p, seg_index(seg_lo, seg_pre, j));
+            }
+            sorted_chunk(n, raw, acc);
+        }
+        write_acc(acc);
         return;
     }
 
@@ -549,7 +619,7 @@ __global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v) k_deposit(PV
         }
     };
 
-    if (multi) {
+    {
         // bounds over every particle first: the scale must be fixed before the first chunk
         R lb[NC];
 #pragma unroll
@@ -626,31 +696,78 @@ __global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v) k_deposit(PV
         if (accumulate) o[gi] = (R)((double)o[gi] + val);
         else o[gi] = (R)val;
     }
+    }
+}
+
+template <class R, int KIND, bool USE_PHI>
+__global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v)
+    k_deposit(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt, const R *__restrict__ phi, DepOut<R> out,
+              double a, double m00, double mij, double m0i, int accumulate, uint32_t *work, int *err, FastDiv fN)
+{
+    deposit_tile<R, KIND, USE_PHI, false>((int)blockIdx.x, work, p, bstart, N, nt, phi, out, a, m00, mij, m0i, accumulate,
+                                          err, fN);
+}
+
+// The dense tiles, one at a time per CTA, each CTA claiming the next listed
+// tile when it is done with one (their costs differ widely).
+template <class R, int KIND, bool USE_PHI>
+__global__ void __launch_bounds__(DEP_NT, GEV_DEP_MINB_DENSE)
+    k_deposit_dense(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt, const R *__restrict__ phi,
+                    DepOut<R> out, double a, double m00, double mij, double m0i, int accumulate, uint32_t *work, int *err,
+                    FastDiv fN)
+{
+    __shared__ uint32_t next;
+    const uint32_t count = work[0];
+    for (;;) {
+        if (threadIdx.x == 0) next = atomicAdd(&work[1], 1u);
+        __syncthreads();
+        const uint32_t i = next;
+        if (i >= count) break;
+        deposit_tile<R, KIND, USE_PHI, true>((int)work[2 + i], work, p, bstart, N, nt, phi, out, a, m00, mij, m0i,
+                                             accumulate, err, fN);
+        __syncthreads();   // shared memory and `next` are reused for the next tile
+    }
+}
+
+static int sm_count()
+{
+    static int count[SMEM_ATTR_DEVICES] = {};
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < SMEM_ATTR_DEVICES && count[dev] > 0) return count[dev];
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    if (dev >= 0 && dev < SMEM_ATTR_DEVICES) count[dev] = n;
+    return n;
 }
 
 template <class R, int KIND, bool USE_PHI>
 static void launch_k(const PView<R> &p, const uint32_t *bstart, int N, const R *phi, const DepOut<R> &out, double a,
-                     double m00, double mij, double m0i, int accumulate, int *err, cudaStream_t st)
+                     double m00, double mij, double m0i, int accumulate, uint32_t *work, int *err, cudaStream_t st)
 {
-    constexpr size_t smem = dep_smem_bytes<R, KIND>();
-    static bool attr_set[SMEM_ATTR_DEVICES] = {};
+    constexpr size_t smem = dep_smem_bytes<R, KIND>(), smem_dense = dep_smem_bytes<R, KIND, true>();
+    static bool attr_set[SMEM_ATTR_DEVICES] = {}, attr_set_dense[SMEM_ATTR_DEVICES] = {};
     raise_smem_limit(k_deposit<R, KIND, USE_PHI>, smem, attr_set);
+    raise_smem_limit(k_deposit_dense<R, KIND, USE_PHI>, smem_dense, attr_set_dense);
     const int nt = N / 8;
-    const unsigned grid = (unsigned)nt * nt * nt;
-    k_deposit<R, KIND, USE_PHI><<<grid, DEP_NT, smem, st>>>(p, bstart, N, nt, phi, out, a, m00, mij, m0i, accumulate, err,
-                                                                      FastDiv((uint32_t)N));
+    const unsigned tiles = (unsigned)nt * nt * nt;
+    const FastDiv fN((uint32_t)N);
+    k_deposit<R, KIND, USE_PHI><<<tiles, DEP_NT, smem, st>>>(p, bstart, N, nt, phi, out, a, m00, mij, m0i, accumulate,
+                                                               work, err, fN);
+    // one wave of resident CTAs; those that find the list empty return at once
+    const unsigned grid = std::min(tiles, (unsigned)(sm_count() * GEV_DEP_MINB_DENSE));
+    k_deposit_dense<R, KIND, USE_PHI><<<grid, DEP_NT, smem_dense, st>>>(p, bstart, N, nt, phi, out, a, m00, mij, m0i,
+                                                                        accumulate, work, err, fN);
 }
 
 template <class R>
 void launch_deposit(int kind, bool use_phi, const PView<R> &p, const uint32_t *bstart, int N, const R *phi,
-                    const DepOut<R> &out, double a, double m00, double mij, double m0i, int accumulate, int *err,
-                    cudaStream_t st)
+                    const DepOut<R> &out, double a, double m00, double mij, double m0i, int accumulate, uint32_t *work,
+                    int *err, cudaStream_t st)
 {
-#define GEV_DEP(K)                                                                                         \
-    if (kind == K) {                                                                                       \
-        if (use_phi) launch_k<R, K, true>(p, bstart, N, phi, out, a, m00, mij, m0i, accumulate, err, st);  \
-        else launch_k<R, K, false>(p, bstart, N, phi, out, a, m00, mij, m0i, accumulate, err, st);         \
-        return;                                                                             \
+#define GEV_DEP(K)                                                                                                \
+    if (kind == K) {                                                                                              \
+        if (use_phi) launch_k<R, K, true>(p, bstart, N, phi, out, a, m00, mij, m0i, accumulate, work, err, st);   \
+        else launch_k<R, K, false>(p, bstart, N, phi, out, a, m00, mij, m0i, accumulate, work, err, st);          \
+        return;                                                                                                   \
     }
     GEV_DEP(DEP_T00)
     GEV_DEP(DEP_TIJ)
@@ -661,8 +778,10 @@ void launch_deposit(int kind, bool use_phi, const PView<R> &p, const uint32_t *b
 }
 
 template void launch_deposit<float>(int, bool, const PView<float> &, const uint32_t *, int, const float *,
-                                    const DepOut<float> &, double, double, double, double, int, int *, cudaStream_t);
+                                    const DepOut<float> &, double, double, double, double, int, uint32_t *, int *,
+                                    cudaStream_t);
 template void launch_deposit<double>(int, bool, const PView<double> &, const uint32_t *, int, const double *,
-                                     const DepOut<double> &, double, double, double, double, int, int *, cudaStream_t);
+                                     const DepOut<double> &, double, double, double, double, int, uint32_t *, int *,
+                                     cudaStream_t);
 
 }  // namespace gev

@@ -16,10 +16,13 @@ enum { DEP_T00 = 0, DEP_TIJ = 1, DEP_T00_TIJ = 2, DEP_T0I = 3, DEP_T00_TIJ_S0I =
 
 template <class R> struct DepOut { R *p[10]; };
 
+// Two launches: every tile whose reach fits one chunk, then the denser tiles
+// from the work list `work` (ntiles + 2 words; work[0] and work[1] must be
+// zero on entry).
 template <class R>
 void launch_deposit(int kind, bool use_phi, const PView<R> &p, const uint32_t *bstart, int N, const R *phi,
-                    const DepOut<R> &out, double a, double m00, double mij, double m0i, int accumulate, int *err,
-                    cudaStream_t st);
+                    const DepOut<R> &out, double a, double m00, double mij, double m0i, int accumulate, uint32_t *work,
+                    int *err, cudaStream_t st);
 
 // ---- particles ----
 struct KickDriftParams {

@@ -89,11 +89,13 @@ def test_project_cic_mass_and_accumulate(prec):
 
 
 @pytest.mark.parametrize("prec", PRECS)
-@pytest.mark.parametrize("n", [30000, 60000])
+@pytest.mark.parametrize("n", [30000, 60000, 90000, 200000])
 def test_deposit_is_order_independent_and_bitwise_reproducible(prec, n):
     """Identical bits for any particle order: tiles whose reach holds up to one
-    chunk of records (n = 30000) sum in a fixed (cell, particle ID) order,
-    denser tiles (n = 60000) in 64-bit fixed point."""
+    chunk of records (n = 30000) sum in a fixed (cell, particle ID) order;
+    denser tiles whose buckets stay (cell, ID)-sorted (n = 60000, 90000: two
+    and three chunks) in that order chunk after chunk; tiles with a bucket
+    above the sorted size (n = 200000) in 64-bit fixed point."""
     N = 32
     pos, q, ids = particles(N, n=n, seed=6)
     phi = trough_phi(N)
@@ -152,6 +154,41 @@ def test_t0i_sums_arguments():
                                     (gev.PROJ_T00 | gev.PROJ_TIJ | gev.PROJ_T0I_SUMS, True, True)):
             with pytest.raises(gev.GevError):
                 c.project(which, 0.5, 1.0, use_phi, acc)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("n", [90000, 200000])
+def test_deposit_dense_tiles(prec, n):
+    """Uniform particles at 2.7 and 6 per cell: every tile's reach takes
+    several chunks; at 2.7 per cell the buckets stay (cell, ID)-sorted and
+    are summed chunk by chunk in the field precision, at 6 per cell the
+    interior buckets exceed the sorted size and take the fixed-point path."""
+    N = 32
+    pos, q, ids = particles(N, n=n, seed=17)
+    phi = trough_phi(N)
+    o = oracle()
+    a = 0.41
+    T00 = np.zeros(N ** 3); Tij = np.zeros(6 * N ** 3); T0i = np.zeros(3 * N ** 3)
+    o.project_T00(N, len(pos), ptr(pos), ptr(q), MASS, ptr(phi), a, 1.0, ptr(T00))
+    o.project_Tij(N, len(pos), ptr(pos), ptr(q), MASS, ptr(phi), a, 1.0, ptr(Tij))
+    o.project_T0i(N, len(pos), ptr(pos), ptr(q), MASS, ptr(phi), 1.0, ptr(T0i))
+    with make_ctx(N, prec, len(pos)) as c:
+        c.set_particles(pos, q, ids, MASS)
+        c.set_field(gev.FIELD_PHI, phi)
+        c.project(gev.PROJ_T00 | gev.PROJ_TIJ | gev.PROJ_T0I, a, 1.0, True)
+        assert rel_err(c.get_field(gev.FIELD_SOURCE), T00) < TOL[prec]
+        g = c.get_field(gev.FIELD_SIJ)
+        for k in range(6):
+            assert rel_err(g[k], Tij[k * N ** 3:(k + 1) * N ** 3]) < TOL[prec], k
+        g = c.get_field(gev.FIELD_BI)
+        for k in range(3):
+            assert rel_err(g[k], T0i[k * N ** 3:(k + 1) * N ** 3]) < TOL[prec], k
+        # the fused T00 + Tij + T0i-sums deposit (the cycle's) on the same tiles
+        c.project(gev.PROJ_T00 | gev.PROJ_TIJ | gev.PROJ_T0I_SUMS, a, 1.0, True)
+        assert rel_err(c.get_field(gev.FIELD_SOURCE), T00) < TOL[prec]
+        g = c.get_field(gev.FIELD_SIJ)
+        for k in range(6):
+            assert rel_err(g[k], Tij[k * N ** 3:(k + 1) * N ** 3]) < TOL[prec], k
 
 
 @pytest.mark.parametrize("prec", PRECS)
