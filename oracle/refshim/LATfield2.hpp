@@ -56,6 +56,45 @@ typedef int MPI_Op;
 #define MPI_MAX 1
 inline int MPI_Reduce(const void *, void *, int, MPI_Datatype, MPI_Op, int, MPI_Comm) { return 0; }
 
+// ---- MPI file and point-to-point names that Particles_gevolution.hpp's output
+// routines use: declared so that the header compiles for its lightcone
+// selection kernels; the single-process stand-in writes no files, so calling
+// any of them aborts ----
+typedef int MPI_Request;
+typedef int MPI_File;
+typedef int MPI_Info;
+typedef long long MPI_Offset;
+struct MPI_Status { int MPI_SOURCE, MPI_TAG, MPI_ERROR; };
+#define MPI_BYTE 4
+#define MPI_UNSIGNED 5
+#define MPI_UNSIGNED_LONG_LONG 6
+#define MPI_MODE_WRONLY 4
+#define MPI_MODE_CREATE 1
+#define MPI_MODE_RDONLY 2
+#define MPI_INFO_NULL 0
+#define MPI_STATUS_IGNORE ((MPI_Status *)0)
+inline int MPI_File_open(MPI_Comm, const char *, int, MPI_Info, MPI_File *) { std::abort(); }
+inline int MPI_File_close(MPI_File *) { std::abort(); }
+inline int MPI_File_set_size(MPI_File, MPI_Offset) { std::abort(); }
+inline int MPI_File_write_at(MPI_File, MPI_Offset, const void *, int, MPI_Datatype, MPI_Status *) { std::abort(); }
+inline int MPI_File_write_at_all(MPI_File, MPI_Offset, const void *, int, MPI_Datatype, MPI_Status *) { std::abort(); }
+inline int MPI_File_read_at(MPI_File, MPI_Offset, void *, int, MPI_Datatype, MPI_Status *) { std::abort(); }
+inline int MPI_File_read_at_all(MPI_File, MPI_Offset, void *, int, MPI_Datatype, MPI_Status *) { std::abort(); }
+inline int MPI_Isend(const void *, int, MPI_Datatype, int, int, MPI_Comm, MPI_Request *) { std::abort(); }
+inline int MPI_Irecv(void *, int, MPI_Datatype, int, int, MPI_Comm, MPI_Request *) { std::abort(); }
+inline int MPI_Wait(MPI_Request *, MPI_Status *) { std::abort(); }
+inline int MPI_Waitall(int, MPI_Request *, MPI_Status *) { std::abort(); }
+inline int MPI_Allreduce(const void *, void *, int, MPI_Datatype, MPI_Op, MPI_Comm) { std::abort(); }
+#define MPI_SUCCESS 0
+#define MPI_SEEK_SET 0
+#define MPI_LONG_LONG 7
+#define MPI_FILE_NULL (-1)
+#define MPI_STATUSES_IGNORE ((MPI_Status *)0)
+inline int MPI_File_seek(MPI_File, MPI_Offset, int) { std::abort(); }
+inline int MPI_File_read_all(MPI_File, void *, int, MPI_Datatype, MPI_Status *) { std::abort(); }
+inline int MPI_Barrier(MPI_Comm) { std::abort(); }
+inline int MPI_Alltoall(const void *, int, MPI_Datatype, void *, int, MPI_Datatype, MPI_Comm) { std::abort(); }
+
 namespace LATfield2
 {
 
@@ -103,6 +142,10 @@ public:
 	__host__ __device__ long sitesLocalGross() const { return sitesLocal(); }
 	__host__ __device__ int N() const { return N_; }
 	__host__ __device__ bool fourier() const { return fourier_; }
+	// linear site indexes without halo: the first site is 0, a step along
+	// dimension i jumps by the product of the sizes below it
+	__host__ __device__ long siteFirst() const { return 0; }
+	__host__ __device__ long jump(int i) const { return i == 0 ? 1 : (i == 1 ? (long) size(0) : (long) size(0) * size(1)); }
 private:
 	int N_;
 	bool fourier_;
@@ -115,6 +158,15 @@ public:
 	__host__ __device__ Site() : lat_(nullptr) { c_[0] = c_[1] = c_[2] = 0; }
 	__host__ __device__ explicit Site(const Lattice & lat) : lat_(&lat) { c_[0] = c_[1] = c_[2] = 0; }
 	__host__ __device__ Site(const Lattice & lat, int x, int y, int z) : lat_(&lat) { c_[0] = x; c_[1] = y; c_[2] = z; }
+	// the site of linear index idx (Lattice::jump)
+	__host__ __device__ Site(const Lattice & lat, long idx) : lat_(&lat)
+	{
+		const long n = lat.N();
+		c_[0] = (int) (idx % n);
+		c_[1] = (int) ((idx / n) % n);
+		c_[2] = (int) (idx / (n * n));
+	}
+	__host__ __device__ void initialize(const Lattice & lat) { lat_ = &lat; first(); }
 	__host__ __device__ void first() { c_[0] = c_[1] = c_[2] = 0; }
 	__host__ __device__ bool test() const { return c_[2] < lat_->N(); }
 	__host__ __device__ void next()
@@ -217,6 +269,20 @@ public:
 	template <class T> void sendUpDown_dim0(T * s1, T * r1, long n1, T * s2, T * r2, long n2) { std::memcpy(r1, s1, sizeof(T) * n1); std::memcpy(r2, s2, sizeof(T) * n2); }
 	template <class T> void sendUpDown_dim1(T * s1, T * r1, long n1, T * s2, T * r2, long n2) { std::memcpy(r1, s1, sizeof(T) * n1); std::memcpy(r2, s2, sizeof(T) * n2); }
 	void abortForce() { std::abort(); }
+	// the process grid of one rank (1 x 1), and point-to-point transfers a
+	// single process never makes
+	const int * grid_rank() const { static const int r[2] = {0, 0}; return r; }
+	const int * grid_size() const { static const int s[2] = {1, 1}; return s; }
+	const MPI_Comm * dim0_comm() const { static const MPI_Comm c[1] = {0}; return c; }
+	const MPI_Comm * dim1_comm() const { static const MPI_Comm c[1] = {0}; return c; }
+	template <class T> void send(T &, int) { std::abort(); }
+	template <class T> void receive(T &, int) { std::abort(); }
+	template <class T> void send_dim0(T &, int) { std::abort(); }
+	template <class T> void receive_dim0(T &, int) { std::abort(); }
+	template <class T> void send_dim1(T &, int) { std::abort(); }
+	template <class T> void receive_dim1(T &, int) { std::abort(); }
+	template <class T> void broadcast_dim0(T &, int) {}
+	template <class T> void broadcast_dim1(T &, int) {}
 };
 
 inline Parallel parallel;

@@ -18,6 +18,7 @@
 #define GEV_REFSHIM_PERFPARTICLES_HPP
 
 #include <cmath>
+#include <cstdint>
 #include <vector>
 #include <omp.h>
 
@@ -169,6 +170,28 @@ private:
 	part * parts_ = nullptr;
 	long count_ = 0;
 	part_info info_{};
+
+public:
+	// The GPU particle layout that Particles_gevolution.hpp's output kernels
+	// read (count_tracer_particles, buffer_tracer_particles,
+	// bufferTracerParticle): per row buffer the positions p (box units,
+	// xyz-interleaved), momenta q and IDs (`other`); with the lattice size,
+	// the rank's coordinate skip (zero on one rank) and the box size (1: box
+	// units).  Filled by the caller, in memory the device can read.
+	struct RowBuffer
+	{
+		int count;
+		Real * p;
+		Real * q;
+		long * other;
+	};
+	RowBuffer * row_buffers_ = nullptr;
+	int num_row_buffers_ = 0;
+	int lat_size_[3] = {0, 0, 0};
+	int lat_size_local_[3] = {0, 0, 0};
+	int coordSkip_[2] = {0, 0};
+	Real boxSize_[3] = {1, 1, 1};
+	uint64_t total_capacity_ = 0;
 };
 
 } // namespace LATfield2

@@ -1,7 +1,8 @@
 // ref_entry.cu -- compiles gevolution-2.0's own hot-path sources (gevolution.hpp,
-// background.hpp, tools.hpp, metadata.hpp, taken from the reference tree where
-// they lie) against the single-rank LATfield2 stand-in in this directory, and
-// exposes their host-side arithmetic through plain C entry points.
+// background.hpp, tools.hpp, metadata.hpp, Particles_gevolution.hpp, taken from
+// the reference tree where they lie) against the single-rank LATfield2 stand-in
+// in this directory, and exposes their host-side arithmetic -- and, for the
+// lightcone output, their CUDA kernels -- through plain C entry points.
 //
 // TEST INFRASTRUCTURE ONLY: the result (oracle/_ref/libgevref.so) pins the oracle
 // restatement (oracle/oracle.c) to the reference's own code, and serves as the
@@ -21,6 +22,7 @@
 #include "tools.hpp"
 #include "background.hpp"
 #include "gevolution.hpp"
+#include "Particles_gevolution.hpp"
 
 #include <cstdint>
 #include <functional>
@@ -294,6 +296,220 @@ int ref_find_intersecting(const double * lc_vertex, const double * lc_direction,
 }
 
 int ref_max_intersects(void) { return MAX_INTERSECTS; }
+
+// The particle lightcone shell of one cycle as the reference writes it
+// (writeLightcones, output.hpp:2093-2135 -> perfParticles_gevolution::
+// saveGadget2, Particles_gevolution.hpp:1567-2160), run on the GPU with the
+// reference's own kernels: count_tracer_particles, buffer_tracer_IDs and
+// count_lightcone_duplicate_ids (the check-zone count), buffer_tracer_particles
+// with bufferTracerParticle (selection and EXACT_OUTPUT_REDSHIFTS
+// interpolation), mark_lightcone_kept_particles and
+// gather_lightcone_kept_particles (de-duplication against the ID backlog),
+// count/fill_lightcone_prelog_bins (the IDs logged for the next cycle's
+// backlog).  One rank, all rows in one chunk, no file: the caller gets the
+// buffers saveGadget2 would write.
+//   pos, q: np x 3 box units; id: np; phi: N^3 (or NULL); vertex, direction,
+//   opening: the lightcone geometry; dist = d - tau; backlog: the IDs logged
+//   in the previous cycle (any order; sorted and made unique here, as
+//   LightconeIDBacklog::finalize does); idlog_scatter selects the 9-bin ID log
+//   (saveGadget2<1>, output.hpp:1180).
+// Outputs: the kept particles (pos in boxsize units, vel, ids) in the order
+// the reference leaves them, n_out; n_header = the header's particle count
+// (selected minus check-zone duplicates); prelog: the IDs logged, bin by bin.
+// Returns 0, -1 on a CUDA error, -2 if capacity is too small (n_out holds the
+// count needed).
+int ref_lightcone_shell(int N, int64_t np, const double * pos, const double * q, const int64_t * id, const double * phi,
+                        const double * lc_vertex, const double * lc_direction, double opening, double dist, double dtau,
+                        double dtau_old, double a, double dadtau, double boxsize, int tracer_factor, int idlog_scatter,
+                        const int64_t * backlog, int64_t nbacklog, int64_t capacity, float * out_pos, float * out_vel,
+                        int64_t * out_id, int64_t * n_out, int64_t * n_header, int64_t * prelog, int64_t * n_prelog)
+{
+	typedef perfParticles_gevolution<part_simple, part_simple_info> PG;
+	typedef PG::RowBuffer Row;
+	std::vector<void *> allocs;
+	bool failed = false;
+	auto managed = [&](size_t bytes) -> void *
+	{
+		void * m = nullptr;
+		if (cudaMallocManaged(&m, bytes > 0 ? bytes : 1) != cudaSuccess) { failed = true; return nullptr; }
+		allocs.push_back(m);
+		return m;
+	};
+	auto release = [&](int rc) { cudaDeviceSynchronize(); for (void * m : allocs) cudaFree(m); return rc; };
+	auto sync = [&]() { return cudaDeviceSynchronize() == cudaSuccess && cudaGetLastError() == cudaSuccess; };
+
+	// vertices: output.hpp:1175-1190 (the whole box on one rank) and :2095
+	lightcone_geometry lc;
+	std::memset(&lc, 0, sizeof(lc));
+	for (int i = 0; i < 3; i++) { lc.vertex[i] = lc_vertex[i]; lc.direction[i] = lc_direction[i]; }
+	lc.opening = opening;
+	double domain[6];
+	for (int i = 0; i < 3; i++) { domain[i] = -0.5 / N; domain[i + 3] = (N + 0.5) / N; }
+	double vertex[MAX_INTERSECTS][3];
+	const int vertexcount = findIntersectingLightcones(lc, dist + (0.5 + LIGHTCONE_IDCHECK_ZONE) * dtau_old, dist - 0.5 * dtau, domain, vertex);
+	const Real inner = dist - 0.5 * dtau;                                     // Particles_gevolution.hpp:1602-1603
+	const Real outer = dist + (0.5 + LIGHTCONE_IDCHECK_ZONE) * dtau_old;
+
+	// particles into row buffers, one per (y, z) row of cells, in input order
+	const int nrows = N * N;
+	std::vector<int> rowcount(nrows, 0), rowof(np);
+	for (int64_t p = 0; p < np; p++)
+	{
+		int c[3];
+		for (int i = 0; i < 3; i++) c[i] = (((int) std::floor(pos[3 * p + i] * N)) % N + N) % N;
+		rowof[p] = c[1] + N * c[2];
+		rowcount[rowof[p]]++;
+	}
+	Real * pp = (Real *) managed(sizeof(Real) * 3 * np);
+	Real * pq = (Real *) managed(sizeof(Real) * 3 * np);
+	long * pid = (long *) managed(sizeof(long) * np);
+	Row * rows = (Row *) managed(sizeof(Row) * nrows);
+	PG * pcl = (PG *) managed(sizeof(PG));
+	double (*d_vertex)[3] = (double (*)[3]) managed(sizeof(double) * 3 * MAX_INTERSECTS);
+	Real * d_domain = (Real *) managed(sizeof(Real) * 4);
+	long * d_npart = (long *) managed(sizeof(long));
+	int * d_npart_row = (int *) managed(sizeof(int) * nrows);
+	int * d_npart_check_row = (int *) managed(sizeof(int) * nrows);
+	unsigned long long * counters = (unsigned long long *) managed(sizeof(unsigned long long) * 4);
+	if (failed) return release(-1);
+	{
+		std::vector<long> start(nrows + 1, 0);
+		for (int r = 0; r < nrows; r++) start[r + 1] = start[r] + rowcount[r];
+		std::vector<long> fill(start.begin(), start.end() - 1);
+		for (int64_t p = 0; p < np; p++)
+		{
+			const long k = fill[rowof[p]]++;
+			for (int i = 0; i < 3; i++) { pp[3 * k + i] = pos[3 * p + i]; pq[3 * k + i] = q[3 * p + i]; }
+			pid[k] = id ? (long) id[p] : (long) p;
+		}
+		for (int r = 0; r < nrows; r++) rows[r] = Row{rowcount[r], pp + 3 * start[r], pq + 3 * start[r], pid + start[r]};
+	}
+	new (pcl) PG();
+	pcl->row_buffers_ = rows;
+	pcl->num_row_buffers_ = nrows;
+	for (int i = 0; i < 3; i++) { pcl->lat_size_[i] = N; pcl->lat_size_local_[i] = N; pcl->boxSize_[i] = 1; }
+	for (int v = 0; v < vertexcount; v++)
+		for (int i = 0; i < 3; i++) d_vertex[v][i] = vertex[v][i];
+	// the rank's domain in box units (Particles_gevolution.hpp:1634-1637)
+	d_domain[0] = 0; d_domain[1] = 1; d_domain[2] = 0; d_domain[3] = 1;
+	Field<Real> * fphi = nullptr;
+	if (phi)
+	{
+		Lattice * lat = (Lattice *) managed(sizeof(Lattice));
+		Real * data = (Real *) managed(sizeof(Real) * (size_t) N * N * N);
+		fphi = (Field<Real> *) managed(sizeof(Field<Real>));
+		if (failed) return release(-1);
+		new (lat) Lattice(N, false);
+		for (long i = 0; i < (long) N * N * N; i++) data[i] = phi[i];
+		new (fphi) Field<Real>(*lat, data, 1);
+	}
+
+	// count (Particles_gevolution.hpp:1670)
+	*d_npart = 0;
+	for (int r = 0; r < nrows; r++) { d_npart_row[r] = 0; d_npart_check_row[r] = 0; }
+	count_tracer_particles<part_simple, part_simple_info><<<nrows, 128>>>(pcl, tracer_factor, lc, inner, outer, dtau_old, d_vertex, vertexcount, d_npart, d_npart_row, d_npart_check_row);
+	if (!sync()) return release(-1);
+	long total = 0, check = 0;
+	for (int r = 0; r < nrows; r++) { total += d_npart_row[r]; check += d_npart_check_row[r]; }
+
+	std::vector<long> bl(backlog, backlog + nbacklog);
+	std::sort(bl.begin(), bl.end());
+	bl.erase(std::unique(bl.begin(), bl.end()), bl.end());
+	long * d_backlog = (long *) managed(sizeof(long) * bl.size());
+	float * posdata = (float *) managed(sizeof(float) * 3 * total);
+	float * veldata = (float *) managed(sizeof(float) * 3 * total);
+	long * ids = (long *) managed(sizeof(long) * total);
+	unsigned char * loginfo = (unsigned char *) managed(total);
+	long * check_ids = (long *) managed(sizeof(long) * check);
+	if (failed) return release(-1);
+	for (size_t i = 0; i < bl.size(); i++) d_backlog[i] = bl[i];
+
+	// check-zone IDs against the backlog: the header count (:1806-1856)
+	long reject = 0;
+	counters[0] = 0;
+	buffer_tracer_IDs<part_simple, part_simple_info><<<nrows, 128>>>(pcl, tracer_factor, lc, inner, outer, dtau_old, d_vertex, vertexcount, check_ids, 0, counters);
+	if (!sync()) return release(-1);
+	if (counters[0] > 0 && !bl.empty())
+	{
+		counters[1] = 0;
+		const int blocks = std::min<long>((counters[0] + 255) / 256, 65535);
+		count_lightcone_duplicate_ids<<<blocks, 256>>>(check_ids, counters[0], d_backlog, (long) bl.size(), counters + 1);
+		if (!sync()) return release(-1);
+		reject = (long) counters[1];
+	}
+	*n_header = total - reject;
+
+	// buffer the particles: check zone first, the rest after it (:2000-2056)
+	counters[0] = 0;
+	counters[1] = (unsigned long long) check;
+	if (idlog_scatter)
+		buffer_tracer_particles<part_simple, part_simple_info, 1><<<nrows, 128>>>(pcl, tracer_factor, lc, (Real) dist, inner, outer, dtau, dtau_old, a, dadtau, boxsize, d_domain, fphi, d_vertex, vertexcount, posdata, veldata, ids, loginfo, 0, counters, counters + 1);
+	else
+		buffer_tracer_particles<part_simple, part_simple_info, 0><<<nrows, 128>>>(pcl, tracer_factor, lc, (Real) dist, inner, outer, dtau, dtau_old, a, dadtau, boxsize, d_domain, fphi, d_vertex, vertexcount, posdata, veldata, ids, loginfo, 0, counters, counters + 1);
+	if (!sync()) return release(-1);
+	long count = total;
+
+	// drop the check-zone particles logged in the previous cycle (:2065-2114);
+	// the flagged selection is stable, as cub::DeviceSelect::Flagged is
+	if (counters[0] > 0 && !bl.empty() && total > 0)
+	{
+		unsigned char * keep = (unsigned char *) managed(total);
+		unsigned long long * selected = (unsigned long long *) managed(sizeof(unsigned long long) * total);
+		float * cpos = (float *) managed(sizeof(float) * 3 * total);
+		float * cvel = (float *) managed(sizeof(float) * 3 * total);
+		long * cids = (long *) managed(sizeof(long) * total);
+		unsigned char * clog = (unsigned char *) managed(total);
+		if (failed) return release(-1);
+		int blocks = std::min<long>((total + 255) / 256, 65535);
+		mark_lightcone_kept_particles<<<blocks, 256>>>(ids, total, counters[0], d_backlog, (long) bl.size(), keep);
+		if (!sync()) return release(-1);
+		long kept = 0;
+		for (long i = 0; i < total; i++)
+			if (keep[i]) selected[kept++] = (unsigned long long) i;
+		if (kept < total)
+		{
+			if (kept > 0)
+			{
+				blocks = std::min<long>((kept + 255) / 256, 65535);
+				gather_lightcone_kept_particles<<<blocks, 256>>>(posdata, veldata, ids, loginfo, cpos, cvel, cids, clog, selected, kept);
+				if (!sync()) return release(-1);
+			}
+			posdata = cpos; veldata = cvel; ids = cids; loginfo = clog;
+			count = kept;
+		}
+	}
+	*n_out = count;
+
+	// the ID log for the next cycle, bin by bin (:2118-2165)
+	long nlog = 0;
+	if (count > 0)
+	{
+		const int log_bins = idlog_scatter ? 9 : 1;
+		unsigned long long * bins = (unsigned long long *) managed(sizeof(unsigned long long) * 27);
+		long * logged = (long *) managed(sizeof(long) * count);
+		if (failed) return release(-1);
+		for (int b = 0; b < 27; b++) bins[b] = 0;
+		const int blocks = std::min<long>((count + 255) / 256, 65535);
+		count_lightcone_prelog_bins<<<blocks, 256>>>(loginfo, count, log_bins, bins);
+		if (!sync()) return release(-1);
+		for (int b = 0; b < log_bins; b++) { bins[9 + b] = (unsigned long long) nlog; nlog += (long) bins[b]; }
+		if (nlog > 0)
+		{
+			fill_lightcone_prelog_bins<<<blocks, 256>>>(ids, loginfo, count, log_bins, bins + 9, bins + 18, logged);
+			if (!sync()) return release(-1);
+		}
+		if (nlog <= capacity)
+			for (long i = 0; i < nlog; i++) prelog[i] = logged[i];
+	}
+	*n_prelog = nlog;
+	if (count > capacity || nlog > capacity) return release(-2);
+	for (long i = 0; i < count; i++)
+	{
+		for (int k = 0; k < 3; k++) { out_pos[3 * i + k] = posdata[3 * i + k]; out_vel[3 * i + k] = veldata[3 * i + k]; }
+		out_id[i] = ids[i];
+	}
+	return release(0);
+}
 
 // One cycle of main.cu's loop (main.cu:608-1317) for CDM in the weak-field GR
 // gauge with the elliptic vector method, no radiation, ncdm, baryons or

@@ -73,6 +73,9 @@ _REF_EXTRA = {
     "particle_horizon": ([_d, _d, _d, _d, _d], _d),
     "find_intersecting": ([_p, _p, _d, _d, _d, _p, _p], _i),
     "max_intersects": ([], _i),
+    # the reference's own lightcone kernels, run on the GPU
+    "lightcone_shell": ([_i, _l, _p, _p, _p, _p, _p, _p, _d, _d, _d, _d, _d, _d, _d, _i, _i, _p, _l, _l,
+                         _p, _p, _p, _p, _p, _p, _p], _i),
 }
 
 _oracle = None
