@@ -127,7 +127,7 @@ template <class K> inline void raise_smem_limit(K kernel, size_t bytes, bool (&d
 // x-pass load modes (fused source preparation)
 enum { FX_COPY = 0, FX_PREP_T00 = 1, FX_PREP_TIJ = 2, FX_PREP_T0I = 3 };
 // z-pass Fourier-space operators
-enum { OP_POISSON = 0, OP_SCALAR = 1, OP_VECTOR = 2, OP_BIN = 3, OP_ZELD = 4 };
+enum { OP_POISSON = 0, OP_SCALAR = 1, OP_VECTOR = 2, OP_BIN = 3, OP_ZELD = 4, OP_ICS = 5 };
 // optional extras of OP_SCALAR
 enum { EXTRA_TENSOR_PROJECT = 1, EXTRA_TENSOR_EVOLVE = 2, EXTRA_VECTOR_EVOLVE = 4 };
 
@@ -137,6 +137,7 @@ constexpr int ERR_LC_OVERFLOW = 2;     // lightcone output exceeded its capacity
 constexpr int ERR_BAD_CELL = 4;        // a particle cell index outside the lattice
 constexpr int ERR_TMA_TIMEOUT = 8;     // a bulk tensor copy did not complete within the wait limit
 constexpr int ERR_BAD_ORDER = 16;      // a deposit found a cell's particles not contiguous in their bucket
+constexpr int ERR_DOMAIN = 32;         // a tabulated function was evaluated outside its table
 
 // kernel launch helper
 inline unsigned int cdiv(int64_t a, int64_t b) { return (unsigned int)((a + b - 1) / b); }

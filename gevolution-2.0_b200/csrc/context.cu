@@ -189,6 +189,7 @@ struct CtxBase {
                            int64_t cap, float *pos, float *vel, int64_t *ids, int64_t *n_out) = 0;
     virtual void fetch_lightcone(int64_t cap, float *pos, float *vel, int64_t *ids, int64_t *n_out) = 0;
     virtual void ics_zeldovich(const gev_ics_params &ip) = 0;
+    virtual void ics_basic(const gev_ics_basic_params &ip) = 0;
     virtual void sync() = 0;
     virtual cudaStream_t stream() = 0;
     virtual int64_t kernel_launches() const = 0;
@@ -494,29 +495,129 @@ template <class R> struct Ctx final : CtxBase {
         launched("ics lattice");
         rebin_from_cells();
         have_particles = true;
-        // 4. phi from the CIC density of the particles (ic_basic.hpp:2404-2427)
+        // 4-5. phi and the momenta
+        ics_phi_and_momenta(ip.a, ip.fourpiG, ip.Omega_m, ip.Omega_Lambda, ip.Omega_rad, ip.boxsize, ip.gr);
+        sync();
+    }
+
+    // phi from the CIC density of the particles (ic_basic.hpp:2404-2427) and
+    // the momenta from phi (:2431-2437; Omega_m(a), Omega_rad(a):
+    // background.hpp:211-213)
+    void ics_phi_and_momenta(double a, double fourpiG, double Om, double OL, double Orad, double boxsize, int gr)
+    {
+        const int N = g.N;
+        const FftTables<R> tb = tables();
         project(GEV_PROJ_CIC, 1.0, 1.0, 0, 0);
-        gev_cosmo cm{ip.Omega_m, ip.Omega_Lambda, ip.Omega_rad, ip.fourpiG, 0.0, 0.0, 0.0, ip.boxsize};
-        const double H = hconf(ip.a, ip.fourpiG, cm);
+        gev_cosmo cm{Om, OL, Orad, fourpiG, 0.0, 0.0, 0.0, boxsize};
+        const double H = hconf(a, fourpiG, cm);
         fx_forward<R>(N, FX_COPY, source.p, g.n3, 1, 0, nullptr, nullptr, 0, 0, 0, 0, W.p, g.nk, nullptr, tb, st);
         fy_pass<R>(N, -1, W.p, g.nk, 1, derr.p, tb, st);
         FzParams fp{};
         fp.op = OP_POISSON;
-        fp.p0 = (ip.fourpiG / ip.a) / -((double)N * (double)N * (double)N);
-        fp.p1 = ip.gr ? 3.0 * (H * H + ip.fourpiG * ip.Omega_m / ip.a) : 0.0;
+        fp.p0 = (fourpiG / a) / -((double)N * (double)N * (double)N);
+        fp.p1 = gr ? 3.0 * (H * H + fourpiG * Om / a) : 0.0;
         fp.p2 = 1.0;   // remove the k = 0 mode
         fp.err = derr.p;
         fz_pass<R>(N, fp, W.p, g.nk, nullptr, nullptr, nullptr, tb, st);
         fy_pass<R>(N, 1, W.p, g.nk, 1, derr.p, tb, st);
         fx_inverse<R>(N, W.p, g.nk, phi.p, g.n3, 1, tb, st);
         launched("ics phi", 5);
-        // 5. momenta (ic_basic.hpp:2431-2437; Omega_m(a), Omega_rad(a): background.hpp:211-213)
-        const double a = ip.a;
-        const double den = ip.Omega_m + ip.Omega_Lambda * a * a * a + ip.Omega_rad / a;
-        const double om_a = ip.Omega_m / den;
-        const double orad_a = ip.Omega_rad / (ip.Omega_m * a + ip.Omega_Lambda * a * a * a * a + ip.Omega_rad);
+        const double den = Om + OL * a * a * a + Orad / a;
+        const double om_a = Om / den;
+        const double orad_a = Orad / (Om * a + OL * a * a * a * a + Orad);
         launch_ics_velocity<R>(cur(), phi.p, N, a / H / (1.5 * om_a + 2.0 * orad_a), st);
         launched("ics velocity");
+    }
+
+    void ics_basic(const gev_ics_basic_params &ip) override
+    {
+        const int N = g.N;
+        const double L = ip.boxsize;
+        if (!(L > 0.0) || !(ip.a > 0.0) || !(ip.fourpiG > 0.0)) throw ArgError("boxsize, a and fourpiG must be positive");
+        if (ip.numtile < 1 || ip.template_n < 1 || !ip.template_pos) throw ArgError("the particle template is empty");
+        for (int64_t i = 0; i < 3 * ip.template_n; i++)   // ic_basic.hpp:325-333
+            if (!(ip.template_pos[i] >= 0.0f && ip.template_pos[i] <= 1.0f))
+                throw ArgError("template positions must lie in [0, 1]");
+        const int64_t T = ip.numtile;
+        if (ip.template_n > (int64_t)1 << 40 || T > 4096) throw ArgError("template or tiling factor too large");
+        const int64_t npart = ip.template_n * T * T * T;
+        if (npart > cfg.capacity) throw ArgError("the particle count n numtile^3 exceeds the context capacity");
+        if (npart > (int64_t)UINT32_MAX) throw ArgError("too many particles");
+        if (ip.n_pk < 3 || !ip.pk_k || !ip.pk_p) throw ArgError("the power spectrum table needs at least three points");
+        // loadPowerSpectrum's table (k L, sqrt(P L / 2)), ic_basic.hpp:431-432, and the
+        // 1 / L^2 of :1905-1913, as a natural cubic spline
+        std::vector<double> x(ip.n_pk), y(ip.n_pk), sb, sc, sd;
+        for (int i = 0; i < ip.n_pk; i++) {
+            if (!(ip.pk_k[i] >= 0.0) || !(ip.pk_p[i] >= 0.0)) throw ArgError("negative k or P(k) in the power spectrum table");
+            x[i] = ip.pk_k[i] * L;
+            if (i > 0 && !(x[i - 1] < x[i])) throw ArgError("power spectrum table: k must increase");
+            y[i] = std::sqrt(0.5 * ip.pk_p[i] * L) / L / L;
+        }
+        ics_natural_spline(x, y, sb, sc, sd);
+        // the table must cover every |2 pi n| a non-zero mode evaluates (GSL's
+        // spline fails outside it): |n|^2 from 1 to 3 (N/2 - 2)^2, below (N/2 - 1)^2 with ksphere
+        {
+            const int kmax = N / 2 - 1;
+            const double fp2 = (4.0 * 3.14159265358979323846) * 3.14159265358979323846;
+            auto xk = [&](long m) { return (double)std::sqrt((float)((double)(float)m * fp2)); };
+            const long mhi = ip.ksphere ? (long)kmax * kmax - 1 : 3L * (kmax - 1) * (kmax - 1);
+            if (kmax >= 2 && (x.front() > xk(1) || x.back() < xk(mhi)))
+                throw ArgError("the power spectrum table does not cover 2 pi / L <= k <= 2 pi sqrt(3) (N/2 - 2) / L");
+        }
+        gev_cosmo cm{ip.Omega_m, ip.Omega_Lambda, ip.Omega_rad, ip.fourpiG, 0.0, 0.0, 0.0, L};
+        const double H = hconf(ip.a, ip.fourpiG, cm);
+        const FftTables<R> tb = tables();
+        // 1. the convolution kernel in the source field
+        std::vector<std::pair<int64_t, R>> ker;
+        ics_cic_kernel<R>(N, ip.correct_displacement ? ip.template_n : 0, ip.correct_displacement ? ip.template_pos : nullptr,
+                          ip.numtile, ker);
+        ck(cudaMemsetAsync(source.p, 0, g.n3 * sizeof(R), st), "memset");
+        for (const auto &e : ker) ck(cudaMemcpyAsync(source.p + e.first, &e.second, sizeof(R), cudaMemcpyHostToDevice, st), "H2D");
+        ck(cudaStreamSynchronize(st), "synchronize");
+        // 2. the modes' numerators, line by line from the reference's stream
+        const int nspl = ip.n_pk;
+        DBuf<double> spl;
+        spl.alloc(5 * (int64_t)nspl, "P(k) spline");
+        std::vector<double> packed;
+        for (const auto *v : {&x, &y, &sb, &sc, &sd}) packed.insert(packed.end(), v->begin(), v->end());
+        ck(cudaMemcpyAsync(spl.p, packed.data(), packed.size() * sizeof(double), cudaMemcpyHostToDevice, st), "H2D");
+        DBuf<double2> modes;
+        modes.alloc((int64_t)(N / 2 + 1) * N * N, "IC modes");
+        const IcsSpline sp{spl.p, spl.p + nspl, spl.p + 2 * nspl, spl.p + 3 * nspl, spl.p + 4 * nspl, nspl};
+        launch_ics_modes(modes.p, N, ip.seed, ip.ksphere, (float)(ip.gr ? H * H : 0.0), sp, derr.p, st);
+        launched("ics modes");
+        // 3. kernel transform, numerator / kernel, backward transform: the displacement potential in chi
+        fx_forward<R>(N, FX_COPY, source.p, g.n3, 1, 0, nullptr, nullptr, 0, 0, 0, 0, W.p, g.nk, nullptr, tb, st);
+        fy_pass<R>(N, -1, W.p, g.nk, 1, derr.p, tb, st);
+        FzParams fz{};
+        fz.op = OP_ICS;
+        fz.modes = modes.p;
+        fz.err = derr.p;
+        fz_pass<R>(N, fz, W.p, g.nk, nullptr, nullptr, nullptr, tb, st);
+        fy_pass<R>(N, 1, W.p, g.nk, 1, derr.p, tb, st);
+        fx_inverse<R>(N, W.p, g.nk, chi.p, g.n3, 1, tb, st);
+        launched("ics displacement potential", 5);
+        // 4. the tiled, displaced template
+        DBuf<float> tmpl;
+        tmpl.alloc(3 * ip.template_n, "particle template");
+        ck(cudaMemcpyAsync(tmpl.p, ip.template_pos, 3 * ip.template_n * sizeof(float), cudaMemcpyHostToDevice, st), "H2D");
+        np = npart;
+        mass = ip.Omega_m / (double)npart;
+        cur_is_A = true;
+        launch_ics_template<R>(view(true), chi.p, tmpl.p, ip.template_n, ip.numtile, N, npart, st);
+        launched("ics template");
+        bi_sums = false;
+        t0i_pending = false;
+        rebin_from_cells();
+        have_particles = true;
+        // 5. phi and the momenta
+        ics_phi_and_momenta(ip.a, ip.fourpiG, ip.Omega_m, ip.Omega_Lambda, ip.Omega_rad, L, ip.gr);
+        // 6. B_i: T0i with phi, projectFTvector(fourpiG / N^2) (ic_basic.hpp:2468-2477)
+        project(GEV_PROJ_T0I, 1.0, 1.0, 1, 0);
+        solve_B(ip.fourpiG / (double)N / (double)N, 0.0);
+        // 7. chi: Tij with phi, prepareFTsource(2 fourpiG / a / N^2), projectFTscalar (:2479-2489)
+        project(GEV_PROJ_TIJ, ip.a, 1.0, 1, 0);
+        chi_pass(2.0 * ip.fourpiG / ip.a / (double)N / (double)N, 0, 0.0, 0.0, 0.0, 0.0);
         sync();
     }
 
@@ -740,6 +841,16 @@ template <class R> struct Ctx final : CtxBase {
 
     void solve_chi(double coeff, int cycle0, double hubble, double dtau, double dtau_old, double a2dtau) override
     {
+        int extra = 0;
+        if (cfg.tensor) extra |= cycle0 ? EXTRA_TENSOR_PROJECT : EXTRA_TENSOR_EVOLVE;
+        if (cfg.vector_method == GEV_VECTOR_PARABOLIC) extra |= EXTRA_VECTOR_EVOLVE;
+        chi_pass(coeff, extra, hubble, dtau, dtau_old, a2dtau);
+    }
+
+    // prepareFTsource(phi, Sij, Sij, coeff), the six forward FFTs,
+    // projectFTscalar with the given extras, the backward FFT(s)
+    void chi_pass(double coeff, int extra, double hubble, double dtau, double dtau_old, double a2dtau)
+    {
         const int N = g.N;
         const FftTables<R> tb = tables();
         fx_forward<R>(N, FX_PREP_TIJ, Sij.p, g.n3, 6, 0, phi.p, chi.p, 0, coeff, 0, 0, W.p, g.nk, nullptr, tb, st);
@@ -749,10 +860,8 @@ template <class R> struct Ctx final : CtxBase {
         FzParams fp{};
         fp.err = derr.p;
         fp.op = OP_SCALAR;
-        fp.extra = 0;
-        if (cfg.tensor) fp.extra |= cycle0 ? EXTRA_TENSOR_PROJECT : EXTRA_TENSOR_EVOLVE;
-        const bool parab = cfg.vector_method == GEV_VECTOR_PARABOLIC;
-        if (parab) fp.extra |= EXTRA_VECTOR_EVOLVE;
+        fp.extra = extra;
+        const bool parab = (extra & EXTRA_VECTOR_EVOLVE) != 0;
         fp.p0 = hubble; fp.p1 = dtau; fp.p2 = dtau_old; fp.p3 = a2dtau;
         fz_pass<R>(N, fp, W.p, g.nk, hij.p, hijp.p, bstate.p, tb, st);
         launched("fz scalar projection");
@@ -1299,6 +1408,12 @@ int gev_ics_zeldovich(gev_ctx *ctx, const gev_ics_params *p)
 {
     if (!p) return fail(ctx, GEV_ERR_ARG, "null argument");
     return guarded(ctx, [&](gev::CtxBase &c) { c.ics_zeldovich(*p); });
+}
+
+int gev_ics_basic(gev_ctx *ctx, const gev_ics_basic_params *p)
+{
+    if (!p) return fail(ctx, GEV_ERR_ARG, "null argument");
+    return guarded(ctx, [&](gev::CtxBase &c) { c.ics_basic(*p); });
 }
 
 // ---- checkpoint / restart ----

@@ -402,6 +402,7 @@ template <class R> struct FzArgs {
     int *err;                  // device error word (may be null)
     const double *tab;         // OP_ZELD: ln k [h/Mpc] (ntab values) then ln P(k) (ntab values)
     int ntab;
+    const double2 *modes;      // OP_ICS: [kz][ky][kx] numerators of the displacement potential
 };
 
 __device__ __forceinline__ double2 zmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
@@ -436,8 +437,8 @@ __device__ __forceinline__ void tt_num(const double *g, const double2 *k, double
 }
 
 template <int OP, int EXTRA> struct OpShape {
-    static constexpr int CIN = (OP == OP_POISSON || OP == OP_BIN || OP == OP_ZELD) ? 1 : (OP == OP_SCALAR ? 6 : 3);
-    static constexpr int COUT = (OP == OP_BIN) ? 0 : ((OP == OP_POISSON) ? 1 : (OP == OP_SCALAR ? ((EXTRA & EXTRA_VECTOR_EVOLVE) ? 4 : 1) : 3));
+    static constexpr int CIN = (OP == OP_POISSON || OP == OP_BIN || OP == OP_ZELD || OP == OP_ICS) ? 1 : (OP == OP_SCALAR ? 6 : 3);
+    static constexpr int COUT = (OP == OP_BIN) ? 0 : ((OP == OP_POISSON || OP == OP_ICS) ? 1 : (OP == OP_SCALAR ? ((EXTRA & EXTRA_VECTOR_EVOLVE) ? 4 : 1) : 3));
     static constexpr int CMAX = CIN > COUT ? CIN : COUT;   // columns the pass holds at once
     // projectFTscalar alone needs only three kz-independent combinations of the
     // six S_ij (see k_fz), so the z pass transforms three columns instead of six
@@ -514,6 +515,20 @@ __device__ __forceinline__ void fz_apply(const FzArgs<R> &a, int N, int kx, int 
         const double nc[3] = {(double)n0, (double)n1, (double)n2};
 #pragma unroll
         for (int c = 0; c < 3; c++) v[c] = make_double2(-nc[c] * amp * w.y, nc[c] * amp * w.x);   // i nc amp w
+    } else if constexpr (OP == OP_ICS) {
+        // generateDisplacementField's last factor (ic_basic.hpp:1270-1281):
+        // potFT(k) = numerator(k) / potFT(k), the field holding the Fourier
+        // transform of the CIC kernel; modes the generator sets to zero stay
+        // zero (their numerator is exactly zero).  Complex division as
+        // (n ker*) / |ker|^2.
+        const double2 num = __ldg(a.modes + (int64_t)kx + (int64_t)(N / 2 + 1) * ((int64_t)ky + (int64_t)N * kz));
+        if (num.x == 0.0 && num.y == 0.0) {
+            v[0] = make_double2(0.0, 0.0);
+        } else {
+            const double2 ker = v[0];
+            const double den = ker.x * ker.x + ker.y * ker.y;
+            v[0] = make_double2((num.x * ker.x + num.y * ker.y) / den, (num.y * ker.x - num.x * ker.y) / den);
+        }
     } else if constexpr (OP == OP_POISSON) {
         // solveModifiedPoissonFT: gevolution.hpp:806-852; p0 = coeff / (-N^3), p1 = modif;
         // p2 != 0 removes the k = 0 mode first (ic_basic.hpp:2419-2421)

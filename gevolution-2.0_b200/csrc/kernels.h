@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <utility>
+#include <vector>
 
 #include "common.cuh"
 #include "particles.cuh"
@@ -87,6 +89,7 @@ struct FzParams {
     int *err;   // device error word for the transfer timeout (may be null)
     const double *tab = nullptr;   // OP_ZELD: ln k then ln P(k), device
     int ntab = 0;
+    const double2 *modes = nullptr;   // OP_ICS: mode numerators, device (ics.cu)
 };
 template <class R>
 void fz_pass(int N, const FzParams &fp, typename CT<R>::C *data, int64_t stride, typename CT<R>::C *hij,
@@ -103,6 +106,18 @@ template <class R> void prep_tij_pass(int N, R *Sij, const R *phi, double coeff,
 template <class R> void launch_ics_noise(R *out, int64_t n3, uint64_t seed, cudaStream_t st);
 template <class R> void launch_ics_lattice(PView<R> p, const R *psi, int N, cudaStream_t st);
 template <class R> void launch_ics_velocity(const PView<R> &p, const R *phi, int N, double coeff, cudaStream_t st);
+// natural cubic spline on the device: knots x, values y, coefficients b, c, d
+struct IcsSpline { const double *x, *y, *b, *c, *d; int n; };
+void launch_ics_modes(double2 *modes, int N, uint32_t seed, int ksphere, float coeff, const IcsSpline &sp, int *err,
+                      cudaStream_t st);
+template <class R>
+void launch_ics_template(PView<R> p, const R *chi, const float *tmpl, int64_t ntmpl, int numtile, int N, int64_t np,
+                         cudaStream_t st);
+// host side of the reference's generator (ics.cu)
+void ics_natural_spline(const std::vector<double> &x, const std::vector<double> &y, std::vector<double> &b,
+                        std::vector<double> &c, std::vector<double> &d);
+template <class R>
+void ics_cic_kernel(int N, int64_t numpcl, const float *pcl, int numtile, std::vector<std::pair<int64_t, R>> &sites);
 
 // ---- lightcone ----
 struct LcKernelArgs {

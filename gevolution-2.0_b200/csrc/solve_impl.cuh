@@ -162,7 +162,7 @@ void fz_n(const FzArgs<R> &a, const FftTables<R> &tb, cudaStream_t st)
 {
     using C = typename CT<R>::C;
     constexpr int T = OpShape<OP, EXTRA>::CONTRACT ? PassCfg<R>::TZC
-                      : (OP == OP_POISSON || OP == OP_BIN) ? PassCfg<R>::TZ1
+                      : (OP == OP_POISSON || OP == OP_BIN || OP == OP_ICS) ? PassCfg<R>::TZ1
                       : ((OP == OP_VECTOR || OP == OP_ZELD) ? PassCfg<R>::TZ3 : PassCfg<R>::TZ6);
     constexpr int NT = PassCfg<R>::NTZ;
 #if GEV_FZ_TMA
@@ -187,6 +187,7 @@ void fz_dispatch(const FzParams &fp, const FzArgs<R> &a, const FftTables<R> &tb,
 {
     if (fp.op == OP_POISSON) fz_n<R, N, OP_POISSON, 0>(a, tb, st);
     else if (fp.op == OP_ZELD) fz_n<R, N, OP_ZELD, 0>(a, tb, st);
+    else if (fp.op == OP_ICS) fz_n<R, N, OP_ICS, 0>(a, tb, st);
     else if (fp.op == OP_BIN) fz_n<R, N, OP_BIN, 0>(a, tb, st);
     else if (fp.op == OP_VECTOR) fz_n<R, N, OP_VECTOR, 0>(a, tb, st);
     else {
@@ -218,6 +219,7 @@ void fz_pass(int N, const FzParams &fp, typename CT<R>::C *data, int64_t stride,
     a.err = fp.err;
     a.tab = fp.tab;
     a.ntab = fp.ntab;
+    a.modes = fp.modes;
     GEV_SWITCH_N(N, (fz_dispatch<R, NN>(fp, a, tb, st)))
 }
 

@@ -61,6 +61,13 @@ class IcsParams(ctypes.Structure):
                 ("ksphere", _i), ("gr", _i), ("reserved", _i), ("noise", _p), ("noise_out", _p)]
 
 
+class IcsBasicParams(ctypes.Structure):
+    _fields_ = [("boxsize", _d), ("a", _d), ("fourpiG", _d), ("Omega_m", _d), ("Omega_Lambda", _d),
+                ("Omega_rad", _d), ("pk_k", _p), ("pk_p", _p), ("n_pk", _i), ("seed", ctypes.c_uint32),
+                ("ksphere", _i), ("correct_displacement", _i), ("gr", _i), ("numtile", _i), ("template_pos", _p),
+                ("template_n", _l)]
+
+
 class LightconeArgs(ctypes.Structure):
     _fields_ = [("vertex", _d * 3), ("direction", _d * 3), ("opening", _d), ("distance", _d * 2),
                 ("d", _d), ("tracer_factor", _i), ("shell", _i)]
@@ -118,6 +125,18 @@ def version():
 
 _poisson_noalloc = _sig("gev_poisson_noalloc", [_i, _i, _p, _p, _d, _d, _p])
 _ics = _sig("gev_ics_zeldovich", [_p, ctypes.POINTER(IcsParams)])
+_ics_basic = _sig("gev_ics_basic", [_p, ctypes.POINTER(IcsBasicParams)])
+_sitmo = _sig("gev_sitmo_words", [ctypes.c_uint32, ctypes.c_uint64, _l, _p])
+
+
+def sitmo_words(seed, start, n):
+    """Words [start, start + n) of the reference IC generator's random stream
+    (sitmo::prng_engine of `seed`), as uint32."""
+    out = np.zeros(max(int(n), 1), dtype=np.uint32)
+    rc = _sitmo(int(seed), int(start), int(n), out.ctypes.data_as(_p))
+    if rc != GEV_OK:
+        raise GevError(rc, "gev_sitmo_words failed")
+    return out[:int(n)]
 _ckw = _sig("gev_checkpoint_write", [_p, ctypes.c_char_p, ctypes.POINTER(State)])
 _ckr = _sig("gev_checkpoint_read", [_p, ctypes.c_char_p, ctypes.POINTER(State)])
 
@@ -319,6 +338,21 @@ class Context:
                         int(bool(gr)), 0, _ptr(w), _ptr(out))
         self._ck(_ics(self._h, ctypes.byref(prm)))
         return out
+
+    def ics_basic(self, boxsize, a, fourpiG, omega_m, omega_l, pk_k, pk_p, template_pos, numtile, seed=0,
+                  omega_rad=0.0, ksphere=False, correct_displacement=True, gr=True):
+        """The reference's own initial conditions (gev_ics_basic): the tabulated
+        spectrum pk_k [h/Mpc], pk_p [(Mpc/h)^3] as read from an mPk file, the
+        particle template (n x 3 positions in [0, 1]) tiled numtile times per
+        axis.  Replaces the particles, phi, chi and B_i."""
+        k = np.ascontiguousarray(pk_k, dtype=np.float64)
+        pk = np.ascontiguousarray(pk_p, dtype=np.float64)
+        t = np.ascontiguousarray(template_pos, dtype=np.float32).reshape(-1, 3)
+        prm = IcsBasicParams(float(boxsize), float(a), float(fourpiG), float(omega_m), float(omega_l), float(omega_rad),
+                             k.ctypes.data_as(_p), pk.ctypes.data_as(_p), len(k), int(seed) & 0xFFFFFFFF,
+                             int(bool(ksphere)), int(bool(correct_displacement)), int(bool(gr)), int(numtile),
+                             t.ctypes.data_as(_p), len(t))
+        self._ck(_ics_basic(self._h, ctypes.byref(prm)))
 
     def checkpoint_write(self, path, state):
         self._ck(_ckw(self._h, str(path).encode(), ctypes.byref(state)))

@@ -304,6 +304,55 @@ typedef struct {
 
 int gev_ics_zeldovich(gev_ctx *ctx, const gev_ics_params *p);
 
+/* The reference's own initial conditions: generateIC_basic with a tabulated
+ * power spectrum (ic_basic.hpp:1834-2509, the "mPk" branch; CDM only, baryon
+ * treatment "ignore", no ncdm), reproduced realisation for realisation:
+ *   1. the convolution kernel of generateCICKernel (:805-1118) -- built from
+ *      the particle template when correct_displacement != 0, the standard
+ *      lattice Laplacian kernel otherwise -- Fourier transformed;
+ *   2. generateDisplacementField (:1165-1610) with the reference's random
+ *      stream (sitmo::prng_engine of `seed`, Threefry-4x64-20, the same word
+ *      for every mode: gev_sitmo_words gives the stream), the spectrum as
+ *      loadPowerSpectrum (:370-516) and :1903-1913 turn it into a natural
+ *      cubic spline of sqrt(P L / 2) / L^2 over k L, the sinc deconvolution,
+ *      the gauge factor 1 + 7.5 gr H_conf^2 / k^2 and the k-sphere cut;
+ *      inverse transform into the displacement potential;
+ *   3. the template tiled numtile times per axis (initializeParticlePositions,
+ *      :1613-1668: particle j of tile (x, y, z) gets ID
+ *      j + n (x + T (y + T z))), displaced by the potential's gradient
+ *      (displace_pcls_ic_basic, :65-96), mass Omega_m / (n T^3);
+ *   4. phi from the particles' CIC density (:2404-2427), momenta from phi
+ *      (initialize_q_ic_basic, :2431-2437), B_i (:2468-2477: T0i projection,
+ *      projectFTvector with fourpiG / N^2) and chi (:2479-2489: Tij
+ *      projection, prepareFTsource with 2 fourpiG / (a N^2), projectFTscalar).
+ * Replaces the context's particles, phi, chi and B_i.  The particle count
+ * n T^3 must fit the context's capacity.  The parabolic vector method's
+ * Fourier state and the tensor state are left as they are (zero after
+ * gev_ctx_create). */
+typedef struct {
+    double boxsize;                 /* L, Mpc/h */
+    double a;                       /* 1 / (1 + z_in) */
+    double fourpiG;                 /* 4 pi G in the code's units */
+    double Omega_m, Omega_Lambda, Omega_rad;
+    const double *pk_k;             /* host: the mPk file's k [h/Mpc], strictly increasing */
+    const double *pk_p;             /* host: its P(k) [(Mpc/h)^3] >= 0 */
+    int32_t n_pk;                   /* >= 3 (a cubic spline) */
+    uint32_t seed;                  /* ic.seed */
+    int32_t ksphere;                /* k-domain = sphere */
+    int32_t correct_displacement;   /* correct displacement = yes */
+    int32_t gr;                     /* gravity theory = GR (sim.gr_flag) */
+    int32_t numtile;                /* tiling factor T (ic.numtile) */
+    const float *template_pos;      /* host: the template's n positions in [0, 1], xyz (loadHomogeneousTemplate) */
+    int64_t template_n;
+} gev_ics_basic_params;
+
+int gev_ics_basic(gev_ctx *ctx, const gev_ics_basic_params *p);
+
+/* Words [start, start + n) of the reference IC generator's random stream for
+ * `seed` (sitmo::prng_engine after seed(seed) and discard(start)), on the
+ * host. */
+int gev_sitmo_words(uint32_t seed, uint64_t start, int64_t n, uint32_t *out);
+
 /* ---- Gadget-2 files (the lightcone output and snapshots) ----
  * The header mirrors gadget2_header (metadata.hpp:159-178), 256 bytes.  Files
  * hold four blocks with uint32 record lengths before and after each: header,

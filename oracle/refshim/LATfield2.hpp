@@ -119,6 +119,11 @@ public:
 	__host__ __device__ Imag operator*(const Imag & o) const { return Imag(re_ * o.re_ - im_ * o.im_, re_ * o.im_ + im_ * o.re_); }
 	__host__ __device__ Imag operator*(Real s) const { return Imag(re_ * s, im_ * s); }
 	__host__ __device__ Imag operator/(Real s) const { return Imag(re_ / s, im_ / s); }
+	__host__ __device__ Imag operator/(const Imag & o) const
+	{
+		const Real den = o.re_ * o.re_ + o.im_ * o.im_;
+		return Imag((re_ * o.re_ + im_ * o.im_) / den, (im_ * o.re_ - re_ * o.im_) / den);
+	}
 	__host__ __device__ Imag & operator+=(const Imag & o) { re_ += o.re_; im_ += o.im_; return *this; }
 	__host__ __device__ Imag & operator-=(const Imag & o) { re_ -= o.re_; im_ -= o.im_; return *this; }
 	__host__ __device__ Imag & operator*=(Real s) { re_ *= s; im_ *= s; return *this; }
@@ -145,6 +150,7 @@ public:
 	// linear site indexes without halo: the first site is 0, a step along
 	// dimension i jumps by the product of the sizes below it
 	__host__ __device__ long siteFirst() const { return 0; }
+	__host__ __device__ long siteLast() const { return sitesLocal() - 1; }
 	__host__ __device__ long jump(int i) const { return i == 0 ? 1 : (i == 1 ? (long) size(0) : (long) size(0) * size(1)); }
 private:
 	int N_;
@@ -167,6 +173,13 @@ public:
 		c_[2] = (int) (idx / (n * n));
 	}
 	__host__ __device__ void initialize(const Lattice & lat) { lat_ = &lat; first(); }
+	__host__ __device__ bool setCoord(int x, int y, int z)
+	{
+		const int n = lat_->N();
+		if (x < 0 || x >= n || y < 0 || y >= n || z < 0 || z >= n) return false;
+		c_[0] = x; c_[1] = y; c_[2] = z;
+		return true;
+	}
 	__host__ __device__ void first() { c_[0] = c_[1] = c_[2] = 0; }
 	__host__ __device__ bool test() const { return c_[2] < lat_->N(); }
 	__host__ __device__ void next()
@@ -197,6 +210,14 @@ class rKSite
 {
 public:
 	__host__ __device__ explicit rKSite(const Lattice & lat) : lat_(&lat) { c_[0] = c_[1] = c_[2] = 0; }
+	// the site of linear index idx (x fastest)
+	__host__ __device__ void initialize(const Lattice & lat, long idx)
+	{
+		lat_ = &lat;
+		c_[0] = (int) (idx % lat.size(0));
+		c_[1] = (int) ((idx / lat.size(0)) % lat.size(1));
+		c_[2] = (int) (idx / ((long) lat.size(0) * lat.size(1)));
+	}
 	__host__ __device__ bool setCoord(int x, int y, int z)
 	{
 		if (x < 0 || x >= lat_->size(0) || y < 0 || y >= lat_->size(1) || z < 0 || z >= lat_->size(2)) return false;
@@ -282,10 +303,52 @@ public:
 	template <class T> void send_dim1(T &, int) { std::abort(); }
 	template <class T> void receive_dim1(T &, int) { std::abort(); }
 	template <class T> void broadcast_dim0(T &, int) {}
+	template <class T> void broadcast_dim0(T *, int, int) {}
 	template <class T> void broadcast_dim1(T &, int) {}
 };
 
 inline Parallel parallel;
+
+// ---- PlanFFT: R2C / C2R over every component of a field pair.  The
+// transforms themselves (the oracle's FFT by default) are supplied by the
+// caller through gev_shim_r2c / gev_shim_c2r, with the conventions of the
+// oracle's: unnormalised, half spectrum kx + (N/2+1)(ky + N kz) ----
+#define FFT_FORWARD 0
+#define FFT_BACKWARD 1
+typedef void (*gev_shim_fft_fn)(int N, const double * in, double * out);
+inline gev_shim_fft_fn gev_shim_r2c = nullptr;
+inline gev_shim_fft_fn gev_shim_c2r = nullptr;
+
+template <class C>
+class PlanFFT
+{
+public:
+	PlanFFT() {}
+	PlanFFT(Field<Real> * r, Field<C> * k, int components = 1) : r_(r), k_(k), comp_(components) {}
+	void initialize(Field<Real> * r, Field<C> * k, int components = 1) { r_ = r; k_ = k; comp_ = components; }
+	void preallocate(size_t) {}
+	void execute(int dir)
+	{
+		if (!r_ || !k_ || !gev_shim_r2c || !gev_shim_c2r) std::abort();
+		const int N = r_->lattice().N();
+		const long n3 = (long) N * N * N, nk = (long) (N / 2 + 1) * N * N;
+		for (int c = 0; c < comp_; c++)
+		{
+			double * re = r_->data() + c * n3;
+			double * ft = reinterpret_cast<double *>(k_->data() + c * nk);
+			if (dir == FFT_FORWARD) gev_shim_r2c(N, re, ft);
+			else gev_shim_c2r(N, ft, re);
+		}
+	}
+private:
+	Field<Real> * r_ = nullptr;
+	Field<C> * k_ = nullptr;
+	int comp_ = 1;
+};
+
+// scalarProjectionCIC_comm, projection_T0i_comm, projection_Tij_comm: the
+// stand-in's projections wrap periodically, there is no halo to fold
+inline void scalarProjectionCIC_comm(Field<Real> *) {}
 
 struct TempMemory
 {

@@ -41,8 +41,27 @@ struct part_simple_dataType {};
 namespace LATfield2
 {
 
+// LATfield2's general particle handler: the reference's non-CDM species use
+// it; the runs here have none, so it only has to compile
 template <typename part, typename part_info, typename part_dataType>
-class Particles;
+class Particles
+{
+public:
+	struct CellList { std::vector<part> parts; };
+	struct CellField { CellList cell; CellList & operator()(const Site &) { return cell; } };
+	const Lattice & lattice() const { return *lat_; }
+	CellField & field() { return field_; }
+	template <class... A> void initialize(A &&...) { std::abort(); }
+	template <class... A> void addParticle_global(A &&...) { std::abort(); }
+	template <class... A> void moveParticles(A &&...) { std::abort(); }
+	template <class... A> Real updateVel(A &&...) { std::abort(); }
+private:
+	const Lattice * lat_ = nullptr;
+	CellField field_;
+};
+
+template <typename part, typename part_info, typename part_dataType>
+void scalarProjectionCIC_project(Particles<part, part_info, part_dataType> *, Field<Real> *) { std::abort(); }
 
 template <typename part, typename part_info>
 class perfParticles
@@ -54,6 +73,28 @@ public:
 		lat_ = lat; parts_ = parts; count_ = count; info_ = info;
 	}
 	long num_particles() const { return count_; }
+	const Lattice & lattice() const { return *lat_; }
+
+	// particle handler of its own (the initial-condition generator's use):
+	// initialize, then addParticle_global for each particle
+	void initialize(const part_info & info, const Lattice * lat, const Real * boxSize, long capacity, long extra)
+	{
+		(void) boxSize; (void) extra;
+		lat_ = lat;
+		info_ = info;
+		owned_.clear();
+		owned_.reserve(capacity > 0 ? (size_t) capacity : 0);
+		parts_ = owned_.data();
+		count_ = 0;
+	}
+	void addParticle_global(const part & p)
+	{
+		owned_.push_back(p);
+		parts_ = owned_.data();
+		count_ = (long) owned_.size();
+	}
+	void updateRowBuffers() {}
+	const part * particles() const { return parts_; }
 
 	template <class F>
 	void projectParticles(F f, Field<Real> ** fields, int nfield, double * params)
@@ -66,7 +107,7 @@ public:
 		for_each_particle(f, 0., fields, nfield, params);
 	}
 	template <class F>
-	Real updateVel(F f, double dtau, Field<Real> ** fields, int nfield, double * params)
+	Real updateVel(F f, double dtau, Field<Real> ** fields, int nfield, double * params = nullptr)
 	{
 		Real vmax = 0;
 #pragma omp parallel for reduction(max : vmax) schedule(static)
@@ -92,6 +133,25 @@ public:
 			f(dtau, 1.0 / lat_->N(), parts_ + p, ref_dist, info_, fields, sites, nfield, params, nullptr, 0);
 			for (int i = 0; i < 3; i++) parts_[p].pos[i] -= std::floor(parts_[p].pos[i]);
 		}
+	}
+	// moveParticles with the functor's outputs reduced over the particles
+	// (MAX or SUM per output, as LATfield2's reductionOp)
+	template <class F>
+	void moveParticles(F f, double dtau, Field<Real> ** fields, int nfield, double * params, double * outputs, int * ops, int noutputs)
+	{
+		std::vector<double> red(noutputs > 0 ? noutputs : 1, 0.0);
+		for (long p = 0; p < count_; p++)
+		{
+			double ref_dist[3];
+			double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+			Site sites[4];
+			locate(p, fields, nfield, ref_dist, sites);
+			f(dtau, 1.0 / lat_->N(), parts_ + p, ref_dist, info_, fields, sites, nfield, params, out, noutputs);
+			for (int i = 0; i < 3; i++) parts_[p].pos[i] -= std::floor(parts_[p].pos[i]);
+			for (int o = 0; o < noutputs && o < 8; o++)
+				red[o] = (ops && ops[o] == MAX) ? (out[o] > red[o] ? out[o] : red[o]) : red[o] + out[o];
+		}
+		for (int o = 0; o < noutputs; o++) outputs[o] = red[o];
 	}
 	void meshprojection_project(Field<Real> * field)
 	{
@@ -167,6 +227,7 @@ private:
 		});
 	}
 	const Lattice * lat_;
+	std::vector<part> owned_;
 	part * parts_ = nullptr;
 	long count_ = 0;
 	part_info info_{};

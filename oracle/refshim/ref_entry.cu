@@ -23,6 +23,7 @@
 #include "background.hpp"
 #include "gevolution.hpp"
 #include "Particles_gevolution.hpp"
+#include "ic_basic.hpp"
 
 #include <cstdint>
 #include <functional>
@@ -31,6 +32,10 @@
 #include "../oracle.h"
 
 using namespace LATfield2;
+
+// the transforms of ref_step and PlanFFT (ref_set_fft)
+typedef void (*ref_fft_fn)(int N, const double * in, double * out);
+static ref_fft_fn g_r2c = orc_r2c, g_c2r = orc_c2r;
 
 namespace
 {
@@ -297,6 +302,177 @@ int ref_find_intersecting(const double * lc_vertex, const double * lc_direction,
 
 int ref_max_intersects(void) { return MAX_INTERSECTS; }
 
+// the natural cubic spline of the GSL stand-in (gsl_spline_init, gsl_spline_eval)
+// through (x, y), n knots, at m points v
+void ref_spline_eval(const double * x, const double * y, int n, const double * v, int m, double * out)
+{
+	gsl_spline * s = gsl_spline_alloc(gsl_interp_cspline, n);
+	gsl_spline_init(s, x, y, n);
+	for (int i = 0; i < m; i++) out[i] = gsl_spline_eval(s, v[i], nullptr);
+	gsl_spline_free(s);
+}
+
+// n words of sitmo::prng_engine (prng_engine.hpp) after seed(seed) and
+// discard(start): the random stream of generateDisplacementField
+void ref_sitmo_words(uint32_t seed, uint64_t start, int64_t n, uint32_t * out)
+{
+	sitmo::prng_engine e;
+	e.seed(seed);
+	if (start) e.discard(start);
+	for (int64_t i = 0; i < n; i++) out[i] = e();
+}
+
+// The reference's initial-condition generator for a tabulated power spectrum:
+// generateIC_basic (ic_basic.hpp:1834-2509), CDM only (baryon treatment
+// "ignore", no ncdm), composed like ref_step from the reference's own
+// functions in its order.  The spectrum and the particle template are
+// written to temporary files that the reference's loadPowerSpectrum and
+// loadHomogeneousTemplate read; generateCICKernel, generateDisplacementField,
+// initializeParticlePositions, the displacement and velocity functors, the
+// CIC projection and the Fourier solvers are called unchanged.  The
+// driver-level wrappers that stage their parameters on the GPU
+// (projection_T0i_project, projection_Tij_project, prepareFTsource) are
+// replaced by their functors applied on the host, as in ref_step.  The
+// oracle's FFT (or ref_set_fft's) stands behind PlanFFT; thrust's device
+// system is OpenMP in this build (oracle/Makefile), so generateCICKernel's
+// thrust::fill_n runs on the host.
+// Outputs: the n_tmpl numtile^3 particles in ID order (pos, q box units; ids),
+// phi, chi (N^3) and B_i (3 N^3), maxvel[0] (:2433).  Returns 0, -1 on a file
+// error.
+int ref_ics_basic(int N, double boxsize, double a, double fourpiG, double Om, double OL, double Orad, const double * pk_k,
+                  const double * pk_p, int n_pk, uint32_t seed, int ksphere, int correct, int gr, int numtile,
+                  const float * tmpl, int64_t ntmpl, double * pos, double * q, int64_t * ids, double * phi, double * chi,
+                  double * Bi, double * maxvel)
+{
+	// the input files
+	char pkname[] = "/tmp/gev_ref_pk_XXXXXX", pclname[] = "/tmp/gev_ref_pcl_XXXXXX";
+	int fd1 = mkstemp(pkname), fd2 = mkstemp(pclname);
+	if (fd1 < 0 || fd2 < 0) return -1;
+	{
+		FILE * f = fdopen(fd1, "w");
+		for (int i = 0; i < n_pk; i++) fprintf(f, "%.17g %.17g\n", pk_k[i], pk_p[i]);
+		fclose(f);
+		gadget2_header hdr;
+		std::memset(&hdr, 0, sizeof(hdr));
+		hdr.npart[1] = (uint32_t) ntmpl;
+		hdr.npartTotal[1] = (uint32_t) ntmpl;
+		hdr.num_files = 1;
+		hdr.BoxSize = 1.0;
+		FILE * g = fdopen(fd2, "wb");
+		uint32_t b = sizeof(hdr);
+		fwrite(&b, 4, 1, g); fwrite(&hdr, sizeof(hdr), 1, g); fwrite(&b, 4, 1, g);
+		b = (uint32_t) (12 * ntmpl);
+		fwrite(&b, 4, 1, g); fwrite(tmpl, sizeof(float), 3 * ntmpl, g); fwrite(&b, 4, 1, g);
+		fclose(g);
+	}
+	const cosmology cosmo = make_cosmo(Om, OL, Orad);
+	const int64_t n3 = (int64_t) N * N * N, nk = (int64_t) (N / 2 + 1) * N * N;
+	const double dx = 1. / N;
+	std::vector<double> vsrc(n3, 0.), vSij(6 * n3, 0.);
+	std::vector<Imag> vscalar(nk), vBiFT(3 * nk), vSijFT(6 * nk);
+	Lattice lat(N, false), klat(N, true);
+	Field<Real> fphi(lat, phi, 1), fchi(lat, chi, 1), fsource(lat, vsrc.data(), 1), fBi(lat, Bi, 3), fSij(lat, vSij.data(), 6, symmetric);
+	Field<Imag> fscalar(klat, vscalar.data(), 1), fBiFT(klat, vBiFT.data(), 3), fSijFT(klat, vSijFT.data(), 6, symmetric);
+	gev_shim_r2c = g_r2c;
+	gev_shim_c2r = g_c2r;
+	PlanFFT<Imag> plan_phi(&fphi, &fscalar), plan_chi(&fchi, &fscalar), plan_source(&fsource, &fscalar);
+	PlanFFT<Imag> plan_Bi(&fBi, &fBiFT, 3), plan_Sij(&fSij, &fSijFT, 6);
+	const double H = Hconf(a, fourpiG, cosmo);
+
+	// template (:1873), kernel and its transform (:1892-1899)
+	long numpcl = 0;
+	float * pcldata = nullptr;
+	loadHomogeneousTemplate(pclname, numpcl, pcldata);
+	if (correct) generateCICKernel(fsource, numpcl, pcldata, numtile);
+	else generateCICKernel(fsource);
+	plan_source.execute(FFT_FORWARD);
+	// spectrum (:1903-1920) and displacement potential (:1922, :2190)
+	gsl_spline * pkspline = nullptr;
+	loadPowerSpectrum(pkname, pkspline, boxsize);
+	{
+		std::vector<double> x(pkspline->x, pkspline->x + pkspline->size), y(pkspline->size);
+		for (size_t i = 0; i < pkspline->size; i++) y[i] = pkspline->y[i] / boxsize / boxsize;
+		const size_t size = pkspline->size;
+		gsl_spline_free(pkspline);
+		pkspline = gsl_spline_alloc(gsl_interp_cspline, size);
+		gsl_spline_init(pkspline, x.data(), y.data(), size);
+	}
+	generateDisplacementField(fscalar, gr * H * H, pkspline, seed, ksphere ? ICFLAG_KSPHERE : 0);
+	plan_chi.execute(FFT_BACKWARD);
+	// particles (:2198-2219)
+	perfParticles<part_simple, part_simple_info> pcls_cdm;
+	part_simple_info info;
+	std::memset(&info, 0, sizeof(info));
+	info.mass = cosmo.Omega_cdm / (Real) (numpcl * (long) numtile * (long) numtile * (long) numtile);
+	Real boxSize[3] = {1., 1., 1.};
+	const long capacity = 16L * numpcl * numtile * numtile * numtile / 15L;
+	pcls_cdm.initialize(info, &lat, boxSize, capacity + PCL_EXTRA_CAPACITY, PCL_EXTRA_CAPACITY);
+	initializeParticlePositions(numpcl, pcldata, numtile, pcls_cdm);
+	{
+		Field<Real> * f[1] = {&fchi};
+		double maxdisp = 0.;
+		int op = MAX;
+		pcls_cdm.moveParticles(displace_pcls_ic_basic_functor(), 1., f, 1, nullptr, &maxdisp, &op, 1);
+	}
+	free(pcldata);
+	// phi from the CIC density (:2407-2425)
+	std::fill(vsrc.begin(), vsrc.end(), 0.);
+	scalarProjectionCIC_project(&pcls_cdm, &fsource);
+	plan_source.execute(FFT_FORWARD);
+	vscalar[0] = Imag(0., 0.);
+	solveModifiedPoissonFT(fscalar, fscalar, fourpiG / a, 3. * gr * (H * H + fourpiG * cosmo.Omega_m / a));
+	plan_phi.execute(FFT_BACKWARD);
+	// momenta (:2429-2434)
+	{
+		const double rescale = a / H / (1.5 * Omega_m(a, cosmo) + 2. * Omega_rad(a, cosmo));
+		Field<Real> * f[1] = {&fphi};
+		*maxvel = pcls_cdm.updateVel(initialize_q_ic_basic_functor(), rescale, f, 1) / a;
+	}
+	// B_i (:2469-2477): projection_T0i_project(pcls, Bi, phi) through its functor
+	std::fill(Bi, Bi + 3 * n3, 0.);
+	{
+		Field<Real> * f[2] = {&fBi, &fphi};
+		double coeff = 1.;
+		pcls_cdm.projectParticles(particle_T0i_project_functor(), f, 2, &coeff);
+	}
+	plan_Bi.execute(FFT_FORWARD);
+	projectFTvector(fBiFT, fBiFT, fourpiG / (double) N / (double) N);
+	plan_Bi.execute(FFT_BACKWARD);
+	// chi (:2481-2491): projection_Tij_project(pcls, Sij, a, phi) and
+	// prepareFTsource(phi, Sij, Sij, 2 fourpiG / a / N^2) through their functors
+	std::fill(vSij.begin(), vSij.end(), 0.);
+	{
+		Field<Real> * f[2] = {&fSij, &fphi};
+		double params[7] = {a, 1., 0., 0., 0., 0., 0.};
+		pcls_cdm.projectParticles(particle_Tij_project_functor(), f, 2, params);
+	}
+	{
+		Field<Real> * f[3] = {&fSij, &fSij, &fphi};
+		double coeff = 2. * fourpiG / a / (double) N / (double) N;
+		site_loop(N, [&](int x, int y, int z) {
+			Site st(lat, x, y, z);
+			Site sites[3] = {st, st, st};
+			prepareFTsource_Tij(f, sites, 3, &coeff, nullptr);
+		});
+	}
+	plan_Sij.execute(FFT_FORWARD);
+	projectFTscalar(fSijFT, fscalar);
+	plan_chi.execute(FFT_BACKWARD);
+	gsl_spline_free(pkspline);
+	std::remove(pkname);
+	std::remove(pclname);
+	(void) dx;
+
+	const long np = pcls_cdm.num_particles();
+	const part_simple * pp = pcls_cdm.particles();
+	for (long i = 0; i < np; i++)
+	{
+		for (int k = 0; k < 3; k++) { pos[3 * i + k] = pp[i].pos[k]; q[3 * i + k] = pp[i].vel[k]; }
+		ids[i] = pp[i].ID;
+	}
+	return 0;
+}
+
 // The particle lightcone shell of one cycle as the reference writes it
 // (writeLightcones, output.hpp:2093-2135 -> perfParticles_gevolution::
 // saveGadget2, Particles_gevolution.hpp:1567-2160), run on the GPU with the
@@ -526,8 +702,6 @@ int ref_lightcone_shell(int N, int64_t np, const double * pos, const double * q,
 // sim and st have the layouts of orc_sim and orc_state (oracle.h); pos and q
 // are advanced in place (particle p has ID p), phi, chi and Bi are the
 // persistent fields.
-typedef void (*ref_fft_fn)(int N, const double * in, double * out);
-static ref_fft_fn g_r2c = orc_r2c, g_c2r = orc_c2r;
 
 // transforms used by ref_step, with the conventions of orc_r2c / orc_c2r
 // (unnormalised, half spectrum kx + (N/2+1)(ky + N kz)); null restores those

@@ -73,6 +73,10 @@ _REF_EXTRA = {
     "particle_horizon": ([_d, _d, _d, _d, _d], _d),
     "find_intersecting": ([_p, _p, _d, _d, _d, _p, _p], _i),
     "max_intersects": ([], _i),
+    "sitmo_words": ([ctypes.c_uint32, ctypes.c_uint64, _l, _p], None),
+    "spline_eval": ([_p, _p, _i, _p, _i, _p], None),
+    "ics_basic": ([_i, _d, _d, _d, _d, _d, _d, _p, _p, _i, ctypes.c_uint32, _i, _i, _i, _i, _p, _l,
+                   _p, _p, _p, _p, _p, _p, _p], _i),
     # the reference's own lightcone kernels, run on the GPU
     "lightcone_shell": ([_i, _l, _p, _p, _p, _p, _p, _p, _d, _d, _d, _d, _d, _d, _d, _i, _i, _p, _l, _l,
                          _p, _p, _p, _p, _p, _p, _p], _i),
