@@ -194,7 +194,7 @@ def run_gpu(args, rank, world, local_rank):
 
     import gevb200 as gev
     from gevb200 import roofline
-    from gevb200.ics import linear_pk
+    from gevb200.ics import linear_pk, sc1_template
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -202,17 +202,21 @@ def run_gpu(args, rank, world, local_rank):
     box = args.boxsize or 5.0 * N
     np_ = N ** 3
     log("initial conditions %d^3" % N)
-    # Zel'dovich ICs generated by the library (gev_ics_zeldovich) in FP64 from the
-    # linear EH no-wiggle P(k) at z_in; every replica has its own seed
+    # the reference's initial conditions (generateIC_basic's tabulated-spectrum
+    # branch, gev_ics_basic) in FP64: the linear EH no-wiggle P(k) at z_in, the
+    # sc1 template tiled N/4 times, k-sphere, corrected displacement; every
+    # replica has its own seed
     a0 = 1.0 / (1.0 + args.z_in)
     fourpiG = 1.5 * box * box / C_LIGHT ** 2
     mass = OMEGA_M / np_
     kt = np.logspace(-5, 3, 4096)
     pt = linear_pk(kt, a0, H_LITTLE, OMEGA_M)
     with gev.Context(N, precision=gev.FP64, capacity=np_, boxsize=box, device=local_rank) as gen:
-        gen.ics_zeldovich(box, a0, fourpiG, OMEGA_M, OMEGA_L, kt, pt, seed=args.seed + 1000 * rank)
+        gen.ics_basic(box, a0, fourpiG, OMEGA_M, OMEGA_L, kt, pt, sc1_template(), N // 4,
+                      seed=args.seed + 1000 * rank, ksphere=True, correct_displacement=True, gr=True)
         p_, q_, i_ = gen.get_particles()
         phi_h = gen.get_field(gev.FIELD_PHI).ravel()
+        chi_h = gen.get_field(gev.FIELD_CHI).ravel()
     log("initial conditions done")
     # host copies in pinned memory: the C ABI takes host buffers
     pos_h = torch.from_numpy(p_).pin_memory().numpy()
@@ -238,6 +242,7 @@ def run_gpu(args, rank, world, local_rank):
                         tensor=args.tensor, device=local_rank)
         c.set_particles(pos_h, q_h, ids_h, mass)
         c.set_field(gev.FIELD_PHI, phi_h)
+        c.set_field(gev.FIELD_CHI, chi_h)
         return c
 
     def cycle(c, st):
@@ -448,8 +453,9 @@ def run_gpu(args, rank, world, local_rank):
             "value": value, "unit": "Mpart-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 fields/FFT + f64 particle offsets, background and reductions",
-            "data": "synthetic: Zel'dovich ICs at z=%g generated on the GPU by gev_ics_zeldovich (Philox4x32-10 white noise, "
-                    "seed %d, linear EH no-wiggle P(k))" % (args.z_in, args.seed),
+            "data": "synthetic: the reference's Zel'dovich ICs at z=%g (generateIC_basic's tabulated-spectrum branch, "
+                    "reproduced on the GPU by gev_ics_basic: sitmo stream seed %d, sc1 template tiled N/4, k-sphere, "
+                    "corrected displacement, linear EH no-wiggle P(k))" % (args.z_in, args.seed),
             "config": workload_config(N, box, world, args.tensor),
             "gpu_launches": launches,
             "stage_ms": stages,
@@ -490,9 +496,11 @@ def reference_cycle_rate(Ns, steps, warmup, seed, z_in=100.0):
     """Time ref_step -- one cycle of main.cu:608-1317 composed from the
     reference's own functors, Fourier solvers and background integrator,
     compiled for the host by oracle/Makefile with the single-rank LATfield2
-    stand-in (OpenMP) -- on an Ns^3 box with 5 Mpc/h cells and Zel'dovich
-    initial conditions at z_in (synthesised on the host).  LATfield2's FFT is
-    stood in for by pocketfft (scipy.fft, all host threads).  Returns
+    stand-in (OpenMP) -- on an Ns^3 box with 5 Mpc/h cells from the initial
+    conditions of the reference's own generator (ref_ics_basic:
+    generateIC_basic's tabulated-spectrum branch at z_in, sc1 template,
+    k-sphere, corrected displacement).  LATfield2's FFT is stood in for by
+    pocketfft (scipy.fft, all host threads).  Returns
     (Mpart-steps/s, seconds of the timed cycles, threads) or None when the
     reference build is absent."""
     import numpy as np
@@ -539,13 +547,19 @@ def reference_cycle_rate(Ns, steps, warmup, seed, z_in=100.0):
 
     box = 5.0 * Ns
     ics = _load_ics_module()
-    pos, q, _, phi, mass, a0, fourpiG = ics.zeldovich(Ns, box, z_in, seed, device="cpu", omega_m=OMEGA_M,
-                                                      omega_l=OMEGA_L, h=H_LITTLE)
-    pos, q = np.ascontiguousarray(pos.numpy()), np.ascontiguousarray(q.numpy())
-    phi = np.ascontiguousarray(phi.numpy())
+    a0 = 1.0 / (1.0 + z_in)
+    fourpiG = 1.5 * box * box / C_LIGHT ** 2
+    mass = OMEGA_M / Ns ** 3
+    kt = np.logspace(-5, 3, 4096)
+    pt = ics.linear_pk(kt, a0, H_LITTLE, OMEGA_M)
+    tmpl = ics.sc1_template()
+    n3 = Ns ** 3
+    pos, q, ids = np.zeros((n3, 3)), np.zeros((n3, 3)), np.zeros(n3, dtype=np.int64)
+    phi, chi, Bi, mv = np.zeros(n3), np.zeros(n3), np.zeros(3 * n3), np.zeros(1)
+    if r.ics_basic(Ns, box, a0, fourpiG, OMEGA_M, OMEGA_L, 0.0, ptr(kt), ptr(pt), len(kt), seed, 1, 1, 1, Ns // 4,
+                   ptr(tmpl), len(tmpl), ptr(pos), ptr(q), ptr(ids), ptr(phi), ptr(chi), ptr(Bi), ptr(mv)) != 0:
+        return None
     del torch
-    chi = np.zeros(Ns ** 3)
-    Bi = np.zeros(3 * Ns ** 3)
     sim = Sim(Ns, box, fourpiG, mass, OMEGA_M, OMEGA_L, 0.0, z_in, 48.0, 0.04, 1)
     H = math.sqrt((2 * fourpiG / 3) * (OMEGA_M / a0 + OMEGA_L * a0 * a0))
     st = State(a0, 0.0, min(48.0 / Ns, 0.04 / H), 0.0, 0, 0, 0, 0)
@@ -674,7 +688,7 @@ def cpu_sample(args):
     rate, dt, threads = res
     return {"value": rate, "unit": "Mpart-steps/s", "cores": threads, "kind": "reference",
             "sample": "%d cycles of the reference's own cycle functions (ref_step, oracle/_ref) on a %d^3 box with %d^3 "
-                      "Zel'dovich particles from z = 100, %.1f s, FFT by pocketfft" % (args.cpu_sample_steps, args.cpu_sample_N,
+                      "particles from the reference's IC generator at z = 100, %.1f s, FFT by pocketfft" % (args.cpu_sample_steps, args.cpu_sample_N,
                                                                                      args.cpu_sample_N, dt)}
 
 
@@ -694,7 +708,8 @@ def run_reference(args, rank):
             "value": rate, "unit": "Mpart-steps/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": max(1, args.warmup), "ms_per_step": dt / args.steps * 1e3, "ms_per_step_grid": "%d^3" % Ns,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic: Zel'dovich ICs at z=100 (EH no-wiggle P(k)), synthesised on the host, seed %d" % args.seed,
+            "data": "synthetic: the reference's Zel'dovich ICs at z=100 (ref_ics_basic: generateIC_basic's tabulated-"
+                    "spectrum branch, EH no-wiggle P(k), sc1 template), on the host, seed %d" % args.seed,
             "config": reference_sample_config(Ns, args.N),
             "cpu_baseline": {"value": rate, "unit": "Mpart-steps/s", "cores": threads, "kind": "reference",
                              "sample": "the reference's own cycle functions (ref_step: gevolution.hpp projections, "

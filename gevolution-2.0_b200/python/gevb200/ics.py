@@ -43,6 +43,18 @@ def linear_pk(k_hmpc, a, h=0.67, omega_m=0.32, A_s=2.1e-9, n_s=0.965, k_pivot=0.
     return np.where(k > 0, 2.0 * math.pi ** 2 * delta2 / ks ** 3, 0.0)
 
 
+def sc1_template():
+    """The 64-particle simple-cubic template of gevolution's sc1 crystal
+    (settings.ini's particle file): one particle at the centre of each cell
+    of a 4^3 grid, (i + 1/2) / 4 per axis, x fastest.  Tiled N/4 times per
+    axis it puts one particle at every cell centre.  (The reference's file
+    lists the same 64 positions in another order, which permutes the IDs
+    within each tile.)"""
+    g = (np.arange(4, dtype=np.float32) + np.float32(0.5)) / np.float32(4.0)
+    z, y, x = np.meshgrid(g, g, g, indexing="ij")
+    return np.ascontiguousarray(np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1), dtype=np.float32)
+
+
 def hconf(a, fourpiG, om, ol):
     return math.sqrt((2.0 * fourpiG / 3.0) * (om / a + ol * a * a))
 

@@ -1,11 +1,14 @@
-"""Whole runs against the reference's own cycle, from identical particles.
+"""Whole runs against the reference's own code, from the same configuration.
 
-ref_step (oracle/_ref, built from the reference's own gevolution.hpp and
-background.hpp with the single-rank LATfield2 stand-in) advances one cycle of
-main.cu:608-1317 on the host cores; gev_step advances the same cycle on the
-GPU.  Both start from the same Zel'dovich particles and potential, generated
-once by gev_ics_zeldovich in FP64 (the reference's mPk branch,
-ic_basic.hpp:1896-1922, 2404-2437), and run the same number of cycles.
+The reference side runs on the host cores from oracle/_ref (the reference's
+own sources with the single-rank LATfield2 stand-in): its initial-condition
+generator (ref_ics_basic: generateIC_basic's tabulated-spectrum branch with
+the sc1 template tiled N/4 times, k-sphere, corrected displacement, as the
+configurations set it) and then ref_step, one cycle of main.cu:608-1317 at a
+time.  The library side generates the same initial conditions with
+gev_ics_basic (FP64 context) and runs gev_step on the GPU -- in FP64, and in
+mixed precision from the FP64 context's initial state.  Both run the same
+number of cycles.
 
 Compared at the end, as the north star states them:
   * the matter power spectrum, the reference's extractPowerSpectrum
@@ -30,7 +33,7 @@ import pytest
 from _libs import oracle, ptr, ref
 
 gev = pytest.importorskip("gevb200")
-from gevb200.ics import linear_pk  # noqa: E402
+from gevb200.ics import linear_pk, sc1_template  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -68,18 +71,32 @@ def _report(rec):
             f.write(json.dumps(rec) + "\n")
 
 
-def _ics(N, box, a0, seed):
-    """Zel'dovich particles (ID order, ID = cell index) and phi, FP64 on the GPU."""
-    fourpiG = 1.5 * box * box / C_LIGHT ** 2
+def _table(a0):
     kt = np.logspace(-5, 3, 4096)
-    pt = linear_pk(kt, a0, H_LITTLE, OM)
-    with gev.Context(N, precision=gev.FP64, capacity=N ** 3, boxsize=box) as c:
-        c.ics_zeldovich(box, a0, fourpiG, OM, OL, kt, pt, seed=seed, ksphere=True)
-        pos, q, ids = c.get_particles()
-        phi = c.get_field(gev.FIELD_PHI).ravel()
-    o = np.argsort(ids)
-    assert np.array_equal(ids[o], np.arange(N ** 3))
-    return np.ascontiguousarray(pos[o]), np.ascontiguousarray(q[o]), ids[o], phi
+    return kt, linear_pk(kt, a0, H_LITTLE, OM)
+
+
+def _ref_ics(N, box, a0, seed):
+    """The reference generator's particles (ID order), phi, chi and B_i."""
+    r = _reference()
+    fourpiG = 1.5 * box * box / C_LIGHT ** 2
+    kt, pt = _table(a0)
+    tmpl = sc1_template()
+    n = N ** 3
+    pos, q, ids = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n, dtype=np.int64)
+    phi, chi, Bi, mv = np.zeros(n), np.zeros(n), np.zeros(3 * n), np.zeros(1)
+    rc = r.ics_basic(N, box, a0, fourpiG, OM, OL, 0.0, ptr(kt), ptr(pt), len(kt), seed, 1, 1, 1, N // 4, ptr(tmpl),
+                     len(tmpl), ptr(pos), ptr(q), ptr(ids), ptr(phi), ptr(chi), ptr(Bi), ptr(mv))
+    assert rc == 0 and np.array_equal(ids, np.arange(n))
+    return pos, q, ids, phi, chi, Bi
+
+
+def _lib_ics(c, N, box, a0, seed):
+    """gev_ics_basic with the same arguments into context c."""
+    fourpiG = 1.5 * box * box / C_LIGHT ** 2
+    kt, pt = _table(a0)
+    c.ics_basic(box, a0, fourpiG, OM, OL, kt, pt, sc1_template(), N // 4, seed=seed, ksphere=True,
+                correct_displacement=True, gr=True)
 
 
 def _ref_spectrum(N, pos, mass, nb):
@@ -100,12 +117,12 @@ def _displacement(p, p0):
 
 
 def _run(N, box, z_in, seed, cycles=None, nbins=1024):
-    """Both codes from the same particles; cycles=None runs to z = 0."""
+    """Both codes from the same configuration; cycles=None runs to z = 0."""
     r = _reference()
     a0 = 1.0 / (1.0 + z_in)
     fourpiG = 1.5 * box * box / C_LIGHT ** 2
     mass = OM / N ** 3
-    pos0, q0, ids, phi0 = _ics(N, box, a0, seed)
+    pos0, q0, ids, phi0, chi0, Bi0 = _ref_ics(N, box, a0, seed)
     cosmo = gev.Cosmo(OM, OL, 0.0, fourpiG, 48.0, 0.04, z_in, box)
     H = gev.hconf(a0, fourpiG, ctypes.byref(cosmo))
     tau0 = gev.particle_horizon(a0, fourpiG, ctypes.byref(cosmo))
@@ -115,7 +132,7 @@ def _run(N, box, z_in, seed, cycles=None, nbins=1024):
     sim = _Sim(N, box, fourpiG, mass, OM, OL, 0.0, z_in, 48.0, 0.04, 1)
     st = _State(a0, tau0, dtau0, 0.0, 0, 0, 0, 0)
     p_ref, q_ref = pos0.copy(), q0.copy()
-    phi, chi, Bi = phi0.copy(), np.zeros(N ** 3), np.zeros(3 * N ** 3)
+    phi, chi, Bi = phi0.copy(), chi0.copy(), Bi0.copy()
     n = 0
     while (cycles is None and 1.0 / st.a - 1.0 > 0.0) or (cycles is not None and n < cycles):
         r.lib.ref_step(ctypes.byref(sim), ctypes.byref(st), len(p_ref), ptr(p_ref), ptr(q_ref), ptr(phi), ptr(chi), ptr(Bi))
@@ -126,11 +143,25 @@ def _run(N, box, z_in, seed, cycles=None, nbins=1024):
     sel = (occ > 0) & (kb < 0.5 * math.pi * N)
 
     out = {}
+    # the library's initial conditions, FP64, and their distance from the reference's
+    with gev.Context(N, precision=gev.FP64, capacity=N ** 3, boxsize=box) as g:
+        _lib_ics(g, N, box, a0, seed)
+        lp, lq, li = g.get_particles()
+        lphi, lchi = g.get_field(gev.FIELD_PHI).ravel(), g.get_field(gev.FIELD_CHI).ravel()
+    o = np.argsort(li)
+    lp, lq, li = np.ascontiguousarray(lp[o]), np.ascontiguousarray(lq[o]), li[o]
+    assert np.array_equal(li, ids)
+    d0 = _displacement(pos0, (np.floor(pos0 * N) + 0.5) / N)
+    ics_err = float(np.abs(_displacement(lp, pos0)).max() / np.abs(d0).max())
     for prec, name in ((gev.FP64, "fp64"), (gev.MIXED, "mixed")):
         gst = gev.State(a0, tau0, dtau0, 0.0, 0, 0.0, 0.0, 0.0)
         with gev.Context(N, precision=prec, capacity=N ** 3, boxsize=box) as c:
-            c.set_particles(pos0, q0, ids, mass)
-            c.set_field(gev.FIELD_PHI, phi0)
+            if prec == gev.FP64:
+                _lib_ics(c, N, box, a0, seed)
+            else:
+                c.set_particles(lp, lq, li, mass)
+                c.set_field(gev.FIELD_PHI, lphi)
+                c.set_field(gev.FIELD_CHI, lchi)
             for _ in range(n):
                 c.step(cosmo, gst)
             phi_g = c.get_field(gev.FIELD_PHI).ravel()
@@ -149,7 +180,8 @@ def _run(N, box, z_in, seed, cycles=None, nbins=1024):
             "bins_differing": int((occ_g != occ).sum()),
         }
     rec = {"N": N, "boxsize": box, "z_in": z_in, "cycles": n, "z_end": 1.0 / st.a - 1.0, "seed": seed,
-           "rms_displacement_box": rms_ref, "pk_bins_compared": int(sel.sum()), **out}
+           "rms_displacement_box": rms_ref, "pk_bins_compared": int(sel.sum()),
+           "ics_max_disp_rel_err": ics_err, **out}
     _report(rec)
     return rec
 
@@ -166,6 +198,7 @@ def test_c1_run_to_z0_matches_reference():
         assert r["pk_max_rel_err"] < 1e-4, (name, r)
         assert r["rms_disp_rel_err"] < 1e-4, (name, r)
     assert rec["fp64"]["per_particle_disp_rel"] < 1e-6, rec["fp64"]
+    assert rec["ics_max_disp_rel_err"] < 1e-7, rec
 
 
 def test_c2_window_matches_reference():
@@ -179,3 +212,4 @@ def test_c2_window_matches_reference():
         assert r["pk_max_rel_err"] < 1e-4, (name, r)
         assert r["rms_disp_rel_err"] < 1e-4, (name, r)
     assert rec["fp64"]["per_particle_disp_rel"] < 1e-6, rec["fp64"]
+    assert rec["ics_max_disp_rel_err"] < 1e-7, rec

@@ -52,6 +52,27 @@ def test_spline_standin_matches_scipy():
     assert np.max(np.abs(out - want)) < 1e-12 * np.max(np.abs(want))
 
 
+def test_sc1_template_holds_the_reference_positions():
+    """gevb200.ics.sc1_template() has the positions of the reference's
+    sc1_crystal.dat (read where the reference tree is present)."""
+    import os
+    import struct
+    from gevb200.ics import sc1_template
+    t = sc1_template()
+    assert t.shape == (64, 3) and t.dtype == np.float32
+    path = os.path.join(os.environ.get("GEV_REFERENCE_DIR", "/root/reference"), "sc1_crystal.dat")
+    if not os.path.exists(path):
+        pytest.skip("the reference tree is not present")
+    b = open(path, "rb").read()
+    n = struct.unpack("<I", b[:4])[0]
+    npart = struct.unpack("<6I", b[4:28])[1]
+    box = struct.unpack("<d", b[4 + 128:4 + 136])[0]          # gadget2_header.BoxSize
+    start = 4 + n + 4 + 4
+    pos = np.frombuffer(b[start:start + 12 * npart], dtype="<f4").reshape(-1, 3) / np.float32(box)
+    assert npart == 64
+    assert sorted(map(tuple, pos.tolist())) == sorted(map(tuple, t.tolist()))
+
+
 def template_4x4x4(seed=5):
     """A 64-particle simple-cubic template, (i + 1/2) / 4 per axis (the
     positions of the reference's sc1 template), in a seeded order."""
