@@ -1446,6 +1446,128 @@ struct FileCloser {
 };
 }  // namespace
 
+// ---- express particle files (Particles_gevolution.hpp:98-143, saveExpress
+// :2641-2767, loadExpress :2769-2902) ----
+// One file per rank, "<base>.<rank>" (a numeric suffix of the given name
+// replaced): the 120-byte express header (magic "GEXPCDM", version 1, the
+// writer's sizeof(Real), sizeof(long) and sizeof(gadget2_header), its rank and
+// process grid, lattice sizes and coordinate skip, particle counts and block
+// sizes), then positions (3 n Real, box units), momenta (3 n Real), IDs (n
+// long) and the Gadget-2 header.  This library is one rank of a 1 x 1 grid.
+namespace {
+struct ExpressHeader {
+    char magic[8];
+    uint32_t version, header_size, endian, sizeof_real, sizeof_long, sizeof_gadget2_header;
+    int32_t rank, size;
+    int32_t grid_size[2];
+    int32_t lat_size[3];
+    int32_t lat_size_local[3];
+    int32_t coord_skip[2];
+    uint64_t local_npart, global_npart, position_bytes, momentum_bytes, id_bytes;
+};
+static_assert(sizeof(ExpressHeader) == 120, "express header layout");
+const char EXPRESS_MAGIC_[8] = {'G', 'E', 'X', 'P', 'C', 'D', 'M', '\0'};
+
+// express_rank_filename (Particles_gevolution.hpp:124-143) for rank 0
+std::string express_file(const char *name)
+{
+    std::string f(name);
+    const size_t dot = f.find_last_of('.');
+    if (dot != std::string::npos && dot + 1 < f.size()) {
+        bool digits = true;
+        for (size_t i = dot + 1; i < f.size(); i++) digits = digits && f[i] >= '0' && f[i] <= '9';
+        if (digits) f.resize(dot);
+    }
+    return f + ".0";
+}
+}  // namespace
+
+int gev_express_write(gev_ctx *ctx, const char *filename, const gev_gadget2_header *hdr_in, int32_t real_bytes)
+{
+    if (!ctx || !ctx->impl || !filename || !hdr_in || (real_bytes != 4 && real_bytes != 8)) return GEV_ERR_ARG;
+    return guarded(ctx, [&](gev::CtxBase &c) {
+        const int64_t np = c.particles_count();
+        std::vector<double> pos(3 * (size_t)np), q(3 * (size_t)np);
+        std::vector<int64_t> id((size_t)np);
+        int64_t got = 0;
+        if (np > 0) c.particles_get(pos.data(), q.data(), id.data(), np, &got);
+        gev_gadget2_header hdr = *hdr_in;   // saveExpress:2656-2659
+        hdr.num_files = 1;
+        hdr.npart[1] = (uint32_t)((uint64_t)np & 0xffffffffull);
+        hdr.npartTotal[1] = (uint32_t)((uint64_t)np & 0xffffffffull);
+        hdr.npartTotalHW[1] = (uint32_t)((uint64_t)np >> 32);
+        ExpressHeader e;
+        std::memset(&e, 0, sizeof e);
+        std::memcpy(e.magic, EXPRESS_MAGIC_, 8);
+        e.version = 1;
+        e.header_size = sizeof e;
+        e.endian = 0x01020304u;
+        e.sizeof_real = (uint32_t)real_bytes;
+        e.sizeof_long = 8;
+        e.sizeof_gadget2_header = sizeof(gev_gadget2_header);
+        e.rank = 0;
+        e.size = 1;
+        e.grid_size[0] = e.grid_size[1] = 1;
+        for (int i = 0; i < 3; i++) e.lat_size[i] = e.lat_size_local[i] = c.cfg.N;
+        e.local_npart = e.global_npart = (uint64_t)np;
+        e.position_bytes = e.momentum_bytes = 3 * (uint64_t)np * (uint64_t)real_bytes;
+        e.id_bytes = (uint64_t)np * 8;
+        const std::string path = express_file(filename);
+        FileCloser fc{fopen(path.c_str(), "wb")};
+        if (!fc.f) throw gev::ArgError("cannot open " + path + " for writing");
+        auto put_real = [&](const std::vector<double> &v) {
+            if (real_bytes == 8) return fwrite(v.data(), 8, v.size(), fc.f) == v.size();
+            std::vector<float> f(v.begin(), v.end());
+            return fwrite(f.data(), 4, f.size(), fc.f) == f.size();
+        };
+        bool ok = fwrite(&e, sizeof e, 1, fc.f) == 1 && put_real(pos) && put_real(q) &&
+                  fwrite(id.data(), 8, id.size(), fc.f) == id.size() && fwrite(&hdr, sizeof hdr, 1, fc.f) == 1;
+        if (!ok) throw gev::ArgError("write error on " + path);
+        if (fclose(fc.f) != 0) { fc.f = nullptr; throw gev::ArgError("write error on " + path); }
+        fc.f = nullptr;
+    });
+}
+
+int gev_express_read(gev_ctx *ctx, const char *filename, double mass, gev_gadget2_header *hdr_out)
+{
+    if (!ctx || !ctx->impl || !filename) return GEV_ERR_ARG;
+    return guarded(ctx, [&](gev::CtxBase &c) {
+        const std::string path = express_file(filename);
+        FileCloser fc{fopen(path.c_str(), "rb")};
+        if (!fc.f) throw gev::ArgError("cannot open " + path);
+        ExpressHeader e;
+        if (fread(&e, sizeof e, 1, fc.f) != 1) throw gev::ArgError(path + ": no express header");
+        // loadExpress's layout checks (:2786-2812) for a one-rank reader; either Real size
+        bool ok = std::memcmp(e.magic, EXPRESS_MAGIC_, 8) == 0 && e.version == 1 && e.header_size == sizeof e &&
+                  e.endian == 0x01020304u && (e.sizeof_real == 4 || e.sizeof_real == 8) && e.sizeof_long == 8 &&
+                  e.sizeof_gadget2_header == sizeof(gev_gadget2_header) && e.rank == 0 && e.size == 1 &&
+                  e.grid_size[0] == 1 && e.grid_size[1] == 1 && e.coord_skip[0] == 0 && e.coord_skip[1] == 0;
+        for (int i = 0; i < 3; i++) ok = ok && e.lat_size[i] == c.cfg.N && e.lat_size_local[i] == c.cfg.N;
+        ok = ok && e.local_npart == e.global_npart && e.position_bytes == 3 * e.local_npart * e.sizeof_real &&
+             e.momentum_bytes == 3 * e.local_npart * e.sizeof_real && e.id_bytes == e.local_npart * 8;
+        if (!ok) throw gev::ArgError(path + " is not an express file of one rank on this lattice");
+        const int64_t np = (int64_t)e.local_npart;
+        if (np > c.cfg.capacity) throw gev::CapacityError("the express file holds more particles than the capacity");
+        std::vector<double> pos(3 * (size_t)np), q(3 * (size_t)np);
+        std::vector<int64_t> id((size_t)np);
+        auto get_real = [&](std::vector<double> &v) {
+            if (e.sizeof_real == 8) return fread(v.data(), 8, v.size(), fc.f) == v.size();
+            std::vector<float> f(v.size());
+            if (fread(f.data(), 4, f.size(), fc.f) != f.size()) return false;
+            for (size_t i = 0; i < v.size(); i++) v[i] = f[i];
+            return true;
+        };
+        gev_gadget2_header hdr;
+        if (!get_real(pos) || !get_real(q) || fread(id.data(), 8, id.size(), fc.f) != id.size() ||
+            fread(&hdr, sizeof hdr, 1, fc.f) != 1)
+            throw gev::ArgError(path + ": truncated express file");
+        const uint64_t total = (uint64_t)hdr.npartTotal[1] + ((uint64_t)hdr.npartTotalHW[1] << 32);
+        if (total != e.global_npart || hdr.num_files != 1) throw gev::ArgError(path + ": Gadget-2 metadata does not match");
+        c.particles_set(pos.data(), q.data(), id.data(), np, mass);
+        if (hdr_out) *hdr_out = hdr;
+    });
+}
+
 int gev_checkpoint_write(gev_ctx *ctx, const char *path, const gev_state *st)
 {
     if (!ctx || !ctx->impl || !path || !st) return GEV_ERR_ARG;

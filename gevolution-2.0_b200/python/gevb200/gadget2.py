@@ -33,6 +33,8 @@ _write = _sig("gev_gadget2_write", [ctypes.c_char_p, ctypes.POINTER(Gadget2Heade
 _snapshot = _sig("gev_snapshot_gadget2", [_p, ctypes.c_char_p, ctypes.POINTER(Gadget2Header), _i32])
 _read = _sig("gev_gadget2_read", [ctypes.c_char_p, ctypes.POINTER(Gadget2Header), _p, _p, _p, _l, ctypes.POINTER(_l)])
 _load = _sig("gev_particles_load_gadget2", [_p, ctypes.c_char_p, _d, ctypes.POINTER(Gadget2Header)])
+_xwrite = _sig("gev_express_write", [_p, ctypes.c_char_p, ctypes.POINTER(Gadget2Header), _i32])
+_xread = _sig("gev_express_read", [_p, ctypes.c_char_p, _d, ctypes.POINTER(Gadget2Header)])
 
 
 def header(a, boxsize_mpc_h, omega_m, omega_lambda, h, numpcl, omega_cdm=None, tracer_factor=1):
@@ -87,6 +89,23 @@ def load(ctx, path, mass):
     rc = _load(ctx._h, str(path).encode(), float(mass), ctypes.byref(hdr))
     if rc != 0:
         raise GevError(rc, "gev_particles_load_gadget2 failed for %s" % path)
+    return hdr
+
+
+def express_write(ctx, filename, hdr, real_bytes=8):
+    """gev_express_write: the context's particles as the reference's express
+    file "<filename without numeric suffix>.0" (Real of real_bytes)."""
+    rc = _xwrite(ctx._h, str(filename).encode(), ctypes.byref(hdr), int(real_bytes))
+    if rc != 0:
+        raise GevError(rc, "gev_express_write failed for %s" % filename)
+
+
+def express_read(ctx, filename, mass):
+    """gev_express_read: an express file's particles into the context; returns its Gadget-2 header."""
+    hdr = Gadget2Header()
+    rc = _xread(ctx._h, str(filename).encode(), float(mass), ctypes.byref(hdr))
+    if rc != 0:
+        raise GevError(rc, "gev_express_read failed for %s" % filename)
     return hdr
 
 

@@ -412,6 +412,19 @@ int gev_snapshot_gadget2(gev_ctx *ctx, const char *path, const gev_gadget2_heade
  * reference's GPU build stops at its hibernation points instead of writing a
  * checkpoint (main.cu:1288-1303; the CPU build's writer is hibernation.hpp),
  * so this is the restart path of this library. */
+/* Express particle files: saveExpress / loadExpress
+ * (Particles_gevolution.hpp:98-143, :2641-2902), the reference's fast
+ * particle dump and restart input (ic.flags ICFLAG_EXPRESSREADER).  One file
+ * per rank named "<filename without a numeric suffix>.<rank>"; this library is
+ * one rank, so it writes and reads "<base>.0": the express header, positions
+ * (box units) and momenta in Real (real_bytes 4 or 8: the writing build's
+ * sizeof(Real)), IDs, and the Gadget-2 header (hdr with npart / npartTotal /
+ * num_files set to this file, as saveExpress sets them).  The reader accepts
+ * either Real size, checks the layout as loadExpress does (one rank, 1 x 1
+ * grid, this context's N) and replaces the context's particles. */
+int gev_express_write(gev_ctx *ctx, const char *filename, const gev_gadget2_header *hdr, int32_t real_bytes);
+int gev_express_read(gev_ctx *ctx, const char *filename, double mass, gev_gadget2_header *hdr_out);
+
 int gev_checkpoint_write(gev_ctx *ctx, const char *path, const gev_state *st);
 int gev_checkpoint_read(gev_ctx *ctx, const char *path, gev_state *st);
 

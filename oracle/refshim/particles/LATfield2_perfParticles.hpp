@@ -246,6 +246,14 @@ public:
 		Real * q;
 		long * other;
 	};
+	// the particle arrays saveExpress / loadExpress copy from and to (device
+	// memory in LATfield2: managed memory here), their count and capacity
+	Real * p = nullptr;
+	Real * q = nullptr;
+	long * other = nullptr;
+	long num_particles_ = 0;
+	uint64_t extra_capacity_ = 0;
+	void resizeGlobalBuffers(uint64_t) { std::abort(); }
 	RowBuffer * row_buffers_ = nullptr;
 	int num_row_buffers_ = 0;
 	int lat_size_[3] = {0, 0, 0};

@@ -302,6 +302,66 @@ int ref_find_intersecting(const double * lc_vertex, const double * lc_direction,
 
 int ref_max_intersects(void) { return MAX_INTERSECTS; }
 
+// perfParticles_gevolution::saveExpress (Particles_gevolution.hpp:2641-2767)
+// of np particles (pos, q box units, ids) on an N^3 lattice, one rank; hdr is
+// the 256-byte gadget2_header.  Particle arrays in managed memory (the writer
+// copies them from the device), so the call needs a GPU.  0, or -1.
+int ref_express_write(const char * filename, int N, int64_t np, const double * pos, const double * q, const int64_t * ids,
+                      const void * hdr)
+{
+	typedef perfParticles_gevolution<part_simple, part_simple_info> PG;
+	PG pcl;
+	Real * mp = nullptr, * mq = nullptr;
+	long * mid = nullptr;
+	if (cudaMallocManaged(&mp, sizeof(Real) * 3 * (np + 1)) != cudaSuccess ||
+	    cudaMallocManaged(&mq, sizeof(Real) * 3 * (np + 1)) != cudaSuccess ||
+	    cudaMallocManaged(&mid, sizeof(long) * (np + 1)) != cudaSuccess)
+		return -1;
+	for (int64_t i = 0; i < 3 * np; i++) { mp[i] = pos[i]; mq[i] = q[i]; }
+	for (int64_t i = 0; i < np; i++) mid[i] = ids[i];
+	pcl.p = mp; pcl.q = mq; pcl.other = mid;
+	pcl.num_particles_ = np;
+	pcl.total_capacity_ = np;
+	for (int i = 0; i < 3; i++) { pcl.lat_size_[i] = N; pcl.lat_size_local_[i] = N; }
+	gadget2_header h;
+	std::memcpy(&h, hdr, sizeof(h));
+	int rc = 0;
+	try { pcl.saveExpress(filename, h); } catch (...) { rc = -1; }
+	cudaFree(mp); cudaFree(mq); cudaFree(mid);
+	return rc;
+}
+
+// perfParticles_gevolution::loadExpress (:2769-2902) into arrays of capacity
+// cap; n receives the count, hdr the 256-byte gadget2_header.  0, or -1 if the
+// reader rejects the file.
+int ref_express_read(const char * filename, int N, int64_t cap, double * pos, double * q, int64_t * ids, int64_t * n,
+                     void * hdr)
+{
+	typedef perfParticles_gevolution<part_simple, part_simple_info> PG;
+	PG pcl;
+	Real * mp = nullptr, * mq = nullptr;
+	long * mid = nullptr;
+	if (cudaMallocManaged(&mp, sizeof(Real) * 3 * (cap + 1)) != cudaSuccess ||
+	    cudaMallocManaged(&mq, sizeof(Real) * 3 * (cap + 1)) != cudaSuccess ||
+	    cudaMallocManaged(&mid, sizeof(long) * (cap + 1)) != cudaSuccess)
+		return -1;
+	pcl.p = mp; pcl.q = mq; pcl.other = mid;
+	pcl.total_capacity_ = cap;
+	for (int i = 0; i < 3; i++) { pcl.lat_size_[i] = N; pcl.lat_size_local_[i] = N; }
+	gadget2_header h;
+	int rc = 0;
+	try { pcl.loadExpress(filename, h); } catch (...) { rc = -1; }
+	if (rc == 0)
+	{
+		*n = pcl.num_particles_;
+		for (int64_t i = 0; i < 3 * pcl.num_particles_; i++) { pos[i] = mp[i]; q[i] = mq[i]; }
+		for (int64_t i = 0; i < pcl.num_particles_; i++) ids[i] = mid[i];
+		std::memcpy(hdr, &h, sizeof(h));
+	}
+	cudaFree(mp); cudaFree(mq); cudaFree(mid);
+	return rc;
+}
+
 // the natural cubic spline of the GSL stand-in (gsl_spline_init, gsl_spline_eval)
 // through (x, y), n knots, at m points v
 void ref_spline_eval(const double * x, const double * y, int n, const double * v, int m, double * out)

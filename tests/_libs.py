@@ -74,6 +74,8 @@ _REF_EXTRA = {
     "find_intersecting": ([_p, _p, _d, _d, _d, _p, _p], _i),
     "max_intersects": ([], _i),
     "sitmo_words": ([ctypes.c_uint32, ctypes.c_uint64, _l, _p], None),
+    "express_write": ([ctypes.c_char_p, _i, _l, _p, _p, _p, _p], _i),
+    "express_read": ([ctypes.c_char_p, _i, _l, _p, _p, _p, _p, _p], _i),
     "spline_eval": ([_p, _p, _i, _p, _i, _p], None),
     "ics_basic": ([_i, _d, _d, _d, _d, _d, _d, _p, _p, _i, ctypes.c_uint32, _i, _i, _i, _i, _p, _l,
                    _p, _p, _p, _p, _p, _p, _p], _i),
