@@ -25,7 +25,8 @@
 //                  double dtau, double dtau_old)                                                               :537
 //   perfParticles::updateVel(update_q_functor(), dtau, fields, nfield, params) -> max velocity        main.cu:1232
 //   perfParticles::moveParticles(update_pos_functor(), dtau, fields, nfield, params)                   main.cu:1258
-//   perfParticles_gevolution::saveGadget2 (snapshot and lightcone forms), loadGadget2
+//   perfParticles_gevolution::saveGadget2 (snapshot and lightcone forms), loadGadget2,
+//   saveExpress, loadExpress
 //                                                                                  Particles_gevolution.hpp:180-183
 //   PlanFFT<Imag>::execute(FFT_FORWARD | FFT_BACKWARD), Field<Real>::updateHalo()
 //   Hconf, rungekutta4bg, particleHorizon                                          background.hpp:200, :235, :268
@@ -438,6 +439,21 @@ public:
     {
         gev_gadget2_header h;
         gev_b200::check(this->box().ctx(), gev_particles_load_gadget2(this->box().ctx(), filename.c_str(), this->mass(), &h));
+        static_assert(sizeof(Header) == sizeof(gev_gadget2_header), "gadget2_header is 256 bytes (metadata.hpp:159-178)");
+        std::memcpy(&hdr, &h, sizeof h);
+    }
+
+    // express files (Particles_gevolution.hpp:185-186): the reference's rank-file
+    // naming and layout, one rank; the file's Real is the caller's Real
+    template <class Header> void saveExpress(std::string filename, Header &hdr)
+    {
+        const gev_gadget2_header h = to_header(hdr);
+        gev_b200::check(this->box().ctx(), gev_express_write(this->box().ctx(), filename.c_str(), &h, (int32_t)sizeof(Real)));
+    }
+    template <class Header> void loadExpress(std::string filename, Header &hdr)
+    {
+        gev_gadget2_header h;
+        gev_b200::check(this->box().ctx(), gev_express_read(this->box().ctx(), filename.c_str(), this->mass(), &h));
         static_assert(sizeof(Header) == sizeof(gev_gadget2_header), "gadget2_header is 256 bytes (metadata.hpp:159-178)");
         std::memcpy(&hdr, &h, sizeof h);
     }

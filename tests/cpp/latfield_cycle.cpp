@@ -8,6 +8,9 @@
 // tensor state.  Exit status 0 when the particles and fields agree.
 #include <cmath>
 #include <cstdio>
+#include <cstring>
+#include <string>
+#include <unistd.h>
 #include <random>
 #include <vector>
 
@@ -149,6 +152,24 @@ int run(bool mixed, bool elliptic, bool tensor, double tol_pos, double tol_field
         dtau = std::fmin(48.0 * dx, 0.04 / Hconf(a, fourpiG, cosmo));
 
         gev_b200::check(ref.ctx(), gev_step(ref.ctx(), &gc, &st));
+    }
+
+    // the particles through an express file (saveExpress / loadExpress) and back
+    {
+        gev_gadget2_header hdr;
+        std::memset(&hdr, 0, sizeof hdr);
+        hdr.num_files = 1;
+        hdr.time = a;
+        char name[] = "/tmp/gev_latfield_express_XXXXXX";
+        const int fd = mkstemp(name);
+        if (fd < 0) throw std::runtime_error("mkstemp");
+        close(fd);
+        pcls_cdm.saveExpress(name, hdr);
+        gev_gadget2_header back;
+        pcls_cdm.loadExpress(name, back);
+        std::remove(name);
+        std::remove((std::string(name) + ".0").c_str());
+        if (back.time != a || back.npartTotal[1] != (uint32_t)n) throw std::runtime_error("express header mismatch");
     }
 
     std::vector<double> p1(3 * n), q1(3 * n), p2(3 * n), q2(3 * n);
