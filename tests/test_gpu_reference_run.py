@@ -213,3 +213,19 @@ def test_c2_window_matches_reference():
         assert r["rms_disp_rel_err"] < 1e-4, (name, r)
     assert rec["fp64"]["per_particle_disp_rel"] < 1e-6, rec["fp64"]
     assert rec["ics_max_disp_rel_err"] < 1e-7, rec
+
+
+def test_128_run_to_z0_matches_reference():
+    """Grid and particles 128^3 in a 640 Mpc/h box (5 Mpc/h cells, as the
+    configurations), z = 100 -> 0: the full run against the reference's own
+    initial conditions and cycle."""
+    rec = _run(128, 640.0, 100.0, seed=13)
+    assert rec["z_end"] <= 0.0
+    for name in ("fp64", "mixed"):
+        r = rec[name]
+        assert r["bins_differing"] == 0, (name, r)
+        assert r["a_rel"] < 1e-13, name
+        assert r["pk_max_rel_err"] < 1e-4, (name, r)
+        assert r["rms_disp_rel_err"] < 1e-4, (name, r)
+    assert rec["fp64"]["per_particle_disp_rel"] < 1e-6, rec["fp64"]
+    assert rec["ics_max_disp_rel_err"] < 1e-7, rec
