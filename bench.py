@@ -58,6 +58,7 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-run measurement")
+    p.add_argument("--no-late", action="store_true", help="skip the run on to z = 0")
     p.add_argument("--adj-N", type=int, default=128)
     p.add_argument("--adj-steps", type=int, default=32)
     p.add_argument("--adj-modes", type=int, default=64)
@@ -328,15 +329,62 @@ def run_gpu(args, rank, world, local_rank):
     stage("kick_drift", lambda: c.kick_drift(0.0, a, a * a * N, 3, 0.0, a, a * a * N, 3))
     stage("lightcone", lambda: c.lightcone(lc, st.tau, st.dtau, st.dtau_old, a, a * Hc, lc_cap, fetch=False))
 
+    # ---- late times: the same initial conditions run on to z = 0 with gev_step
+    # (most of a run's cycles are at low redshift, where the particles cluster):
+    # the whole run's rate, then cycles and the particle stages at z ~ 0 ----
+    late = None
+    if not args.no_late:
+        log("late times")
+        cl = make(gev.MIXED)
+        sl = gev.State(a0, tau0, dtau0, 0.0, 0, 0.0, 0.0, 0.0)
+        sl_stream = torch.cuda.ExternalStream(cl.stream())
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        cl.synchronize()
+        ev0.record(sl_stream)
+        n_run = 0
+        while 1.0 / sl.a - 1.0 > 0.0:
+            cl.step(cosmo, sl)
+            n_run += 1
+        ev1.record(sl_stream)
+        ev1.synchronize()
+        run_ms = ev0.elapsed_time(ev1)
+        z0_steps = 5
+        ev0.record(sl_stream)
+        for _ in range(z0_steps):
+            cl.step(cosmo, sl)
+        ev1.record(sl_stream)
+        ev1.synchronize()
+        z0_ms = ev0.elapsed_time(ev1) / z0_steps
+        al = sl.a
+        late_stages = {}
+        for name, fn in (("deposit_T00_Tij_T0i", lambda: cl.project(gev.PROJ_T00 | gev.PROJ_TIJ | gev.PROJ_T0I_SUMS, al, 1.0, True)),
+                         ("kick_drift", lambda: cl.kick_drift(0.0, al, al * al * N, 3, 0.0, al, al * al * N, 3))):
+            fn()
+            cl.synchronize()
+            ev0.record(sl_stream)
+            for _ in range(3):
+                fn()
+            ev1.record(sl_stream)
+            ev1.synchronize()
+            late_stages[name] = ev0.elapsed_time(ev1) / 3
+        late = {"workload": "the same box from z = %g to z = 0 with gev_step (no lightcone shell), then %d cycles at z ~ 0"
+                            % (args.z_in, z0_steps),
+                "cycles_to_z0": n_run, "run_ms_per_step": run_ms / n_run,
+                "run_value": np_ * n_run / (run_ms * 1e-3) / 1e6, "unit": "Mpart-steps/s",
+                "z_end": 1.0 / sl.a - 1.0, "ms_per_step_at_z0": z0_ms, "stage_ms_at_z0": late_stages}
+        cl.close()
+        del cl
+
     peak, peak_kind = measured_peaks()
     # per-stage HBM fractions: algorithmic bytes of the stage / its event time / peak
     stage_alg = {"deposit_T00_Tij_T0i": "deposit_T00_Tij_T0i", "solve_phi": "solve_phi",
                  "solve_chi": "solve_chi_tensor" if args.tensor else "solve_chi", "solve_B": "solve_B_sums",
                  "kick_drift": "kick_drift"}
     stage_frac = {k: roofline.stage_bytes(v, N, "mixed") / (stages[k] * 1e-3) / 1e9 / peak for k, v in stage_alg.items()}
-    # the dominant single kernel: the deposit is one launch; the other stages are
-    # several launches (FFT passes; kick/drift + scan + re-bin), each shorter than
-    # the deposit in the ncu launch list (profiles/)
+    # the dominant kernel: the deposit (its tile launch; the dense-tile launch is
+    # empty at z = 100); the other stages are several launches (FFT passes;
+    # kick/drift + scan + re-bin), each shorter than the deposit in the ncu
+    # launch list (profiles/)
     dom = max(SINGLE_KERNEL_STAGES, key=lambda s: stages[s])
     dom_bytes = roofline.stage_bytes(dom, N, "mixed")
     achieved = dom_bytes / (stages[dom] * 1e-3) / 1e9
@@ -476,6 +524,7 @@ def run_gpu(args, rank, world, local_rank):
             "e2e": e2e,
             "cpu_baseline": cpu,
             "adjoint": adj,
+            "late_time": late,
         }
         print(json.dumps(line), flush=True)
 
