@@ -8,6 +8,13 @@
 // Lengths are compile-time constants factored into radices 2, 3, 4 and 8.
 // Twiddles come from a table tw[k] = exp(-2 pi i k / L) computed on the host in
 // double precision; inverse transforms use the conjugates.
+//
+// Padded rows (PAD): between two passes, row n lives at row n + n / 8, so the
+// buffer needs L + L / 8 rows.  For dense buffers (ld = T) whose rows are
+// narrower than a 128-byte bank line this makes the first pass's scattered
+// writes (rows R j + r, a multiple of 128 bytes apart) conflict-free, while
+// the other accesses of a warp (8 consecutive rows aligned to 8) stay
+// contiguous.  The transform's input and output stay dense, in natural order.
 #pragma once
 
 #include "common.cuh"
@@ -24,12 +31,14 @@ GEV_PLAN(8, 1, 8, 1, 1, 1)
 GEV_PLAN(16, 2, 4, 4, 1, 1)
 GEV_PLAN(32, 2, 4, 8, 1, 1)
 GEV_PLAN(64, 2, 8, 8, 1, 1)
-GEV_PLAN(128, 3, 2, 8, 8, 1)
-GEV_PLAN(192, 4, 3, 8, 8, 1)
+// radix-8 passes first: with padded rows every pass of a dense buffer is then
+// free of bank conflicts
+GEV_PLAN(128, 3, 8, 8, 2, 1)
+GEV_PLAN(192, 3, 3, 8, 8, 1)
 GEV_PLAN(256, 3, 4, 8, 8, 1)
-GEV_PLAN(384, 4, 3, 2, 8, 8)
+GEV_PLAN(384, 4, 8, 8, 2, 3)
 GEV_PLAN(512, 3, 8, 8, 8, 1)
-GEV_PLAN(768, 4, 3, 4, 8, 8)
+GEV_PLAN(768, 4, 8, 8, 4, 3)
 #undef GEV_PLAN
 
 // ---- R-point DFTs in registers, exponent sign S (-1 forward, +1 inverse) ----
@@ -101,8 +110,24 @@ template <int R, int S, class C> __device__ __forceinline__ void dftR(C *v)
     else if constexpr (R == 8) { dft8v<S>(v); }
 }
 
-// One Stockham pass of radix R with span NS over T lines.
-template <int L, int R, int NS, int S, int T, int NT, class C>
+// row n0 + r * STRIDE of the buffer, padded if PAD; n0 + (n0 >> 3) is hoisted
+// out of the loop over r where the block of 8 rows of each r is known:
+// STRIDE a multiple of 8, or STRIDE = 1 with n0 a multiple of a radix RAD
+// that divides 8 (the rows n0 .. n0 + RAD - 1 share their block)
+template <bool PAD, int STRIDE, int RAD> __device__ __forceinline__ int pad_row(int n0, int r)
+{
+    if constexpr (!PAD) return n0 + r * STRIDE;
+    else if constexpr (STRIDE % 8 == 0) return n0 + (n0 >> 3) + r * (STRIDE + STRIDE / 8);
+    else if constexpr (STRIDE == 1 && 8 % RAD == 0) return n0 + (n0 >> 3) + r;
+    else {
+        const int n = n0 + r * STRIDE;
+        return n + (n >> 3);
+    }
+}
+
+// One Stockham pass of radix R with span NS over T lines; rows are read
+// padded if PI and written padded if PO.
+template <int L, int R, int NS, int S, int T, int NT, bool PI, bool PO, class C>
 __device__ __forceinline__ void stockham_pass(C *buf, int ld, const C *__restrict__ tw)
 {
     constexpr int NB = L / R;
@@ -115,7 +140,7 @@ __device__ __forceinline__ void stockham_pass(C *buf, int ld, const C *__restric
         if (BPT * NT == TOT || idx < TOT) {
             int t = idx % T, j = idx / T;
 #pragma unroll
-            for (int r = 0; r < R; r++) v[b][r] = buf[(j + r * NB) * ld + t];
+            for (int r = 0; r < R; r++) v[b][r] = buf[pad_row<PI, NB, R>(j, r) * ld + t];
         }
     }
     __syncthreads();
@@ -136,29 +161,34 @@ __device__ __forceinline__ void stockham_pass(C *buf, int ld, const C *__restric
             dftR<R, S>(v[b]);
             int idxD = (j / NS) * NS * R + jm;
 #pragma unroll
-            for (int r = 0; r < R; r++) buf[(idxD + r * NS) * ld + t] = v[b][r];
+            for (int r = 0; r < R; r++) buf[pad_row<PO, NS, R>(idxD, r) * ld + t] = v[b][r];
         }
     }
     __syncthreads();
 }
 
-template <int L, int S, int T, int NT, int STAGE, int NS> struct FftStages {
+template <int L, int S, int T, int NT, bool PAD, int STAGE, int NS> struct FftStages {
     template <class C> static __device__ __forceinline__ void run(C *buf, int ld, const C *__restrict__ tw)
     {
         if constexpr (STAGE < Plan<L>::ns) {
             constexpr int R = Plan<L>::r(STAGE);
-            stockham_pass<L, R, NS, S, T, NT>(buf, ld, tw);
-            FftStages<L, S, T, NT, STAGE + 1, NS * R>::run(buf, ld, tw);
+            constexpr bool PI = PAD && STAGE > 0, PO = PAD && STAGE < Plan<L>::ns - 1;
+            stockham_pass<L, R, NS, S, T, NT, PI, PO>(buf, ld, tw);
+            FftStages<L, S, T, NT, PAD, STAGE + 1, NS * R>::run(buf, ld, tw);
         }
     }
 };
 
 // Transform T lines of length L in place (unnormalised).  Caller must have
-// issued __syncthreads() after filling buf; returns after a barrier.
-template <int L, int S, int T, int NT, class C>
+// issued __syncthreads() after filling buf; returns after a barrier.  With
+// PAD the buffer holds L + L / 8 rows.
+template <int L, int S, int T, int NT, bool PAD = false, class C>
 __device__ __forceinline__ void fft_lines(C *buf, int ld, const C *__restrict__ tw)
 {
-    FftStages<L, S, T, NT, 0, 1>::run(buf, ld, tw);
+    FftStages<L, S, T, NT, PAD, 0, 1>::run(buf, ld, tw);
 }
+
+// rows of a dense buffer (ld = T) that padding spreads over the banks
+template <int T, class C> constexpr bool pad_helps() { return T * (int)sizeof(C) < 128; }
 
 }  // namespace gev

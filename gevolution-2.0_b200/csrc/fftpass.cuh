@@ -750,7 +750,9 @@ template <class R, int OP, int EXTRA, int NT> struct FzMinBlocks {
                                  : (sizeof(R) == 4 ? GEV_FZ_MINB : GEV_FZ_MINB_D) * 256 / NT;
 };
 
-template <class R, int N, int T, int NT, int OP, int EXTRA>
+// PAD: the transforms use padded rows (fft.cuh), each component buffer then
+// holds N + N / 8 rows of T values
+template <class R, int N, int T, int NT, int OP, int EXTRA, bool PAD>
 __global__ void __launch_bounds__(NT, (FzMinBlocks<R, OP, EXTRA, NT>::v))
     k_fz_tma(FzArgs<R> a, const typename CT<R>::C *__restrict__ tw, const __grid_constant__ CUtensorMap tmap)
 {
@@ -760,6 +762,7 @@ __global__ void __launch_bounds__(NT, (FzMinBlocks<R, OP, EXTRA, NT>::v))
     constexpr bool CONTRACT = OpShape<OP, EXTRA>::CONTRACT;
     constexpr int ZB = ZBox<N>::ZB, NZB = ZBox<N>::NZB;
     constexpr int CS = N * T;   // one component: [kz][t], dense
+    constexpr int CSTR = PAD ? (N + N / 8) * T : CS;   // component buffer stride
     // bulk tensor copies want 128-byte aligned shared addresses: the launch
     // adds 128 bytes of slack and the buffers start at the next boundary
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -774,7 +777,7 @@ __global__ void __launch_bounds__(NT, (FzMinBlocks<R, OP, EXTRA, NT>::v))
 #pragma unroll 1
         for (int c = 0; c < CIN; c++)
 #pragma unroll 1
-            for (int zc = 0; zc < NZB; zc++) tma_load_4d(buf + c * CS + zc * ZB * T, &tmap, 2 * kx0, ky, zc * ZB, c, &bar);
+            for (int zc = 0; zc < NZB; zc++) tma_load_4d(buf + c * CSTR + zc * ZB * T, &tmap, 2 * kx0, ky, zc * ZB, c, &bar);
     }
     const bool ok = mbar_wait(&bar, 0);
     if (__syncthreads_or(!ok)) {
@@ -790,7 +793,7 @@ __global__ void __launch_bounds__(NT, (FzMinBlocks<R, OP, EXTRA, NT>::v))
             if (kx < P) {
                 double2 S[6];
 #pragma unroll
-                for (int c = 0; c < 6; c++) S[c] = z2d(buf[c * CS + idx]);
+                for (int c = 0; c < 6; c++) S[c] = z2d(buf[c * CSTR + idx]);
                 const double g0 = __ldg(a.k2 + kx), g1 = __ldg(a.k2 + ky);
                 const double2 k0 = __ldg(a.ks + kx), k1 = __ldg(a.ks + ky);
                 A = zsub(zadd(zadd(zsc(S[0], g1 - 2.0 * g0), zsc(S[3], g0 - 2.0 * g1)), zsc(S[5], g0 + g1)),
@@ -799,13 +802,13 @@ __global__ void __launch_bounds__(NT, (FzMinBlocks<R, OP, EXTRA, NT>::v))
                 Cc = zadd(zmul(k0, S[2]), zmul(k1, S[4]));
             }
             buf[idx] = mk(R(A.x), R(A.y));
-            buf[CS + idx] = mk(R(B.x), R(B.y));
-            buf[2 * CS + idx] = mk(R(Cc.x), R(Cc.y));
+            buf[CSTR + idx] = mk(R(B.x), R(B.y));
+            buf[2 * CSTR + idx] = mk(R(Cc.x), R(Cc.y));
         }
         __syncthreads();
     }
 #pragma unroll 1
-    for (int c = 0; c < (CONTRACT ? 3 : CIN); c++) fft_lines<N, -1, T, NT>(buf + c * CS, T, tw);
+    for (int c = 0; c < (CONTRACT ? 3 : CIN); c++) fft_lines<N, -1, T, NT, PAD>(buf + c * CSTR, T, tw);
 
     for (int idx = threadIdx.x; idx < CS; idx += NT) {
         const int t = idx % T, n = idx / T, kx = kx0 + t;
@@ -816,7 +819,7 @@ __global__ void __launch_bounds__(NT, (FzMinBlocks<R, OP, EXTRA, NT>::v))
             const double k2 = g0 + g1 + g2;
             double2 chi = make_double2(0.0, 0.0);
             if (k2 > 0.0) {
-                const double2 A = z2d(buf[idx]), B = z2d(buf[CS + idx]), Cc = z2d(buf[2 * CS + idx]);
+                const double2 A = z2d(buf[idx]), B = z2d(buf[CSTR + idx]), Cc = z2d(buf[2 * CSTR + idx]);
                 chi = zsub(zadd(A, zsc(B, g2)), zsc(zmul(k2c, Cc), 6.0));
                 chi = zsc(chi, 1.0 / (2.0 * k2 * k2 * N));
             }
@@ -824,24 +827,24 @@ __global__ void __launch_bounds__(NT, (FzMinBlocks<R, OP, EXTRA, NT>::v))
         } else {
             double2 v[6];
 #pragma unroll
-            for (int c = 0; c < CIN; c++) v[c] = z2d(buf[c * CS + idx]);
+            for (int c = 0; c < CIN; c++) v[c] = z2d(buf[c * CSTR + idx]);
             const int64_t kidx = kx + (int64_t)PP * (ky + (int64_t)N * n);
             fz_apply<R, OP, EXTRA>(a, N, kx, ky, n, kidx, v);
 #pragma unroll
-            for (int c = 0; c < COUT; c++) buf[c * CS + idx] = mk(R(v[c].x), R(v[c].y));
+            for (int c = 0; c < COUT; c++) buf[c * CSTR + idx] = mk(R(v[c].x), R(v[c].y));
         }
     }
     if constexpr (COUT > 0) {
         __syncthreads();
 #pragma unroll 1
-        for (int c = 0; c < COUT; c++) fft_lines<N, 1, T, NT>(buf + c * CS, T, tw);
+        for (int c = 0; c < COUT; c++) fft_lines<N, 1, T, NT, PAD>(buf + c * CSTR, T, tw);
         fence_async_smem();
         __syncthreads();
         if (threadIdx.x == 0) {
 #pragma unroll 1
             for (int c = 0; c < COUT; c++)
 #pragma unroll 1
-                for (int zc = 0; zc < NZB; zc++) tma_store_4d(&tmap, 2 * kx0, ky, zc * ZB, c, buf + c * CS + zc * ZB * T);
+                for (int zc = 0; zc < NZB; zc++) tma_store_4d(&tmap, 2 * kx0, ky, zc * ZB, c, buf + c * CSTR + zc * ZB * T);
             tma_store_drain();
         }
     }

@@ -2,6 +2,7 @@
 // size; included once per precision (solve_f32.cu, solve_f64.cu).
 #pragma once
 
+#include <algorithm>
 #include <stdexcept>
 
 #include "fftpass.cuh"
@@ -54,6 +55,9 @@ template <class R> struct PassCfg {
     static constexpr int TZC = sizeof(R) == 4 ? GEV_TZC_F : GEV_TZC_F / 2;  // contracted scalar
     static constexpr int TIJ6 = sizeof(R) == 4 ? GEV_TIJ6_T_F : GEV_TIJ6_T_F / 2;
 };
+
+// CTAs of `bytes` dynamic shared memory that fit one SM (228 KB, 1 KB reserved per CTA)
+constexpr int smem_ctas(size_t bytes) { return (int)(233472 / (bytes + 1024)); }
 
 template <class K> inline void set_smem(K kernel, size_t bytes)
 {
@@ -168,9 +172,15 @@ void fz_n(const FzArgs<R> &a, const FftTables<R> &tb, cudaStream_t st)
 #if GEV_FZ_TMA
     static_assert(T % 2 == 0 || sizeof(R) == 8, "TMA boxes need 16-byte rows");
     constexpr int CMAX = OpShape<OP, EXTRA>::CMAX;
-    const size_t smem = (size_t)CMAX * N * T * sizeof(C) + 128;
+    constexpr size_t dense = (size_t)CMAX * N * T * sizeof(C) + 128;
+    constexpr size_t padded = (size_t)CMAX * (N + N / 8) * T * sizeof(C) + 128;
+    // padded rows where they spread the banks, keep every component buffer on
+    // a 128-byte boundary, and cost no resident CTA
+    constexpr bool PAD = pad_helps<T, C>() && ((N + N / 8) * T * sizeof(C)) % 128 == 0 &&
+                         smem_ctas(padded) >= std::min(FzMinBlocks<R, OP, EXTRA, NT>::v, smem_ctas(dense));
+    const size_t smem = PAD ? padded : dense;
     const CUtensorMap map = fourier_tensor_map<R>(a.data, N, a.stride, CMAX, T, 1, ZBox<N>::ZB);
-    auto k = k_fz_tma<R, N, T, NT, OP, EXTRA>;
+    auto k = k_fz_tma<R, N, T, NT, OP, EXTRA, PAD>;
     set_smem(k, smem);
     k<<<dim3((N / 2 + 1 + T - 1) / T, N), NT, smem, st>>>(a, tb.tw_full, map);
 #else
