@@ -444,6 +444,7 @@ template <int OP, int EXTRA> struct OpShape {
     // six S_ij (see k_fz), so the z pass transforms three columns instead of six
     static constexpr bool CONTRACT = (OP == OP_SCALAR && EXTRA == 0);
     static constexpr int CBUF = CONTRACT ? 3 : CMAX;
+    static constexpr int CTMA = CONTRACT ? 4 : CMAX;   // buffers of the bulk-copy z pass (k_fz_tma)
 };
 
 // Element-wise solver for one (kx, ky, kz): reads CIN values from v, writes
@@ -770,39 +771,65 @@ __global__ void __launch_bounds__(NT, (FzMinBlocks<R, OP, EXTRA, NT>::v))
     __shared__ __align__(8) uint64_t bar;
     const int kx0 = blockIdx.x * T, ky = blockIdx.y;
 
+    // the contracted scalar solve loads S00, S01, S11, S22 into buffers 0..3,
+    // folds them into A and B (buffers 0, 1), then loads S02, S12 into
+    // buffers 2, 3 and folds them into C (buffer 2): four buffers instead of six
+    constexpr int NL1 = CONTRACT ? 4 : CIN;
+    auto first_comp = [](int s) { return CONTRACT ? (s == 2 ? 3 : (s == 3 ? 5 : s)) : s; };
+    auto load = [&](int slot, int comp) {
+#pragma unroll 1
+        for (int zc = 0; zc < NZB; zc++) tma_load_4d(buf + slot * CSTR + zc * ZB * T, &tmap, 2 * kx0, ky, zc * ZB, comp, &bar);
+    };
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
     if (threadIdx.x == 0) {
-        mbar_expect_tx(&bar, (uint32_t)(CIN * CS * sizeof(C)));
+        mbar_expect_tx(&bar, (uint32_t)(NL1 * CS * sizeof(C)));
 #pragma unroll 1
-        for (int c = 0; c < CIN; c++)
-#pragma unroll 1
-            for (int zc = 0; zc < NZB; zc++) tma_load_4d(buf + c * CSTR + zc * ZB * T, &tmap, 2 * kx0, ky, zc * ZB, c, &bar);
+        for (int s = 0; s < NL1; s++) load(s, first_comp(s));
     }
-    const bool ok = mbar_wait(&bar, 0);
+    bool ok = mbar_wait(&bar, 0);
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0 && a.err) atomicOr(a.err, ERR_TMA_TIMEOUT);
         return;
     }
 
     if constexpr (CONTRACT) {
-        // A, B, C of k_fz's projectFTscalar factorisation, in place into buffers 0..2
+        // A, B, C of k_fz's projectFTscalar factorisation
         for (int idx = threadIdx.x; idx < CS; idx += NT) {
             const int t = idx % T, kx = kx0 + t;
-            double2 A = make_double2(0.0, 0.0), B = A, Cc = A;
+            double2 A = make_double2(0.0, 0.0), B = A;
             if (kx < P) {
-                double2 S[6];
-#pragma unroll
-                for (int c = 0; c < 6; c++) S[c] = z2d(buf[c * CSTR + idx]);
+                const double2 S0 = z2d(buf[idx]), S1 = z2d(buf[CSTR + idx]);
+                const double2 S3 = z2d(buf[2 * CSTR + idx]), S5 = z2d(buf[3 * CSTR + idx]);
                 const double g0 = __ldg(a.k2 + kx), g1 = __ldg(a.k2 + ky);
                 const double2 k0 = __ldg(a.ks + kx), k1 = __ldg(a.ks + ky);
-                A = zsub(zadd(zadd(zsc(S[0], g1 - 2.0 * g0), zsc(S[3], g0 - 2.0 * g1)), zsc(S[5], g0 + g1)),
-                         zsc(zmul(zmul(k0, k1), S[1]), 6.0));
-                B = zsub(zadd(S[0], S[3]), zsc(S[5], 2.0));
-                Cc = zadd(zmul(k0, S[2]), zmul(k1, S[4]));
+                A = zsub(zadd(zadd(zsc(S0, g1 - 2.0 * g0), zsc(S3, g0 - 2.0 * g1)), zsc(S5, g0 + g1)),
+                         zsc(zmul(zmul(k0, k1), S1), 6.0));
+                B = zsub(zadd(S0, S3), zsc(S5, 2.0));
             }
             buf[idx] = mk(R(A.x), R(A.y));
             buf[CSTR + idx] = mk(R(B.x), R(B.y));
+        }
+        __syncthreads();   // buffers 2 and 3 are free
+        if (threadIdx.x == 0) {
+            fence_async_smem();
+            mbar_expect_tx(&bar, (uint32_t)(2 * CS * sizeof(C)));
+            load(2, 2);
+            load(3, 4);
+        }
+        ok = mbar_wait(&bar, 1);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0 && a.err) atomicOr(a.err, ERR_TMA_TIMEOUT);
+            return;
+        }
+        for (int idx = threadIdx.x; idx < CS; idx += NT) {
+            const int t = idx % T, kx = kx0 + t;
+            double2 Cc = make_double2(0.0, 0.0);
+            if (kx < P) {
+                const double2 S2 = z2d(buf[2 * CSTR + idx]), S4 = z2d(buf[3 * CSTR + idx]);
+                const double2 k0 = __ldg(a.ks + kx), k1 = __ldg(a.ks + ky);
+                Cc = zadd(zmul(k0, S2), zmul(k1, S4));
+            }
             buf[2 * CSTR + idx] = mk(R(Cc.x), R(Cc.y));
         }
         __syncthreads();

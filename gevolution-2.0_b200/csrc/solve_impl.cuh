@@ -172,8 +172,9 @@ void fz_n(const FzArgs<R> &a, const FftTables<R> &tb, cudaStream_t st)
 #if GEV_FZ_TMA
     static_assert(T % 2 == 0 || sizeof(R) == 8, "TMA boxes need 16-byte rows");
     constexpr int CMAX = OpShape<OP, EXTRA>::CMAX;
-    constexpr size_t dense = (size_t)CMAX * N * T * sizeof(C) + 128;
-    constexpr size_t padded = (size_t)CMAX * (N + N / 8) * T * sizeof(C) + 128;
+    constexpr int CTMA = OpShape<OP, EXTRA>::CTMA;
+    constexpr size_t dense = (size_t)CTMA * N * T * sizeof(C) + 128;
+    constexpr size_t padded = (size_t)CTMA * (N + N / 8) * T * sizeof(C) + 128;
     // padded rows where they spread the banks, keep every component buffer on
     // a 128-byte boundary, and cost no resident CTA
     constexpr bool PAD = pad_helps<T, C>() && ((N + N / 8) * T * sizeof(C)) % 128 == 0 &&
