@@ -55,7 +55,7 @@ def parse():
     p.add_argument("--tensor", action="store_true", help="keep the h_ij / h_ij' state (full metric solve)")
     p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     p.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-run measurement")
     p.add_argument("--no-late", action="store_true", help="skip the run on to z = 0")
@@ -466,16 +466,19 @@ def run_gpu(args, rank, world, local_rank):
         ev0.record(stream)
         n = ctypes.c_int64()
         lc_bytes = 0
-        for _ in range(args.e2e_steps):
-            c.set_particles(pos_i, q_i, ids_i, mass)           # H2D of the cycle's particle state
+        c.set_particles(pos_i, q_i, ids_i, mass)               # H2D of the first cycle's particle state
+        for k in range(args.e2e_steps):
             cycle(c, st)
             lib.gev_lightcone_fetch(c.handle, lc_cap, pin.ctypes.data_as(ctypes.c_void_p), pinv.ctypes.data_as(ctypes.c_void_p),
                                     pini.ctypes.data_as(ctypes.c_void_p), ctypes.byref(n))
             lc_bytes += n.value * 32
-            lib.gev_particles_get(c.handle, pos_o.ctypes.data_as(ctypes.c_void_p), q_o.ctypes.data_as(ctypes.c_void_p),
-                                  ids_o.ctypes.data_as(ctypes.c_void_p), np_, ctypes.byref(n))
-            # the state read back is the next cycle's input (the first input was the initial conditions)
-            pos_i, pos_o, q_i, q_o, ids_i, ids_o = pos_o, pos_i, q_o, q_i, ids_o, ids_i
+            if k + 1 < args.e2e_steps:
+                # D2H of the cycle's state and H2D of the next cycle's input (that
+                # state, read back) in one call, both directions of the link at once
+                c.exchange_particles(pos_o, q_o, ids_o, pos_o, q_o, ids_o, mass)
+            else:
+                lib.gev_particles_get(c.handle, pos_o.ctypes.data_as(ctypes.c_void_p), q_o.ctypes.data_as(ctypes.c_void_p),
+                                      ids_o.ctypes.data_as(ctypes.c_void_p), np_, ctypes.byref(n))
         ev1.record(stream)
         ev1.synchronize()
         ms_e2e = ev0.elapsed_time(ev1)

@@ -173,6 +173,9 @@ struct CtxBase {
     virtual ~CtxBase() {}
     virtual void particles_set(const double *pos, const double *q, const int64_t *id, int64_t n, double mass) = 0;
     virtual void particles_get(double *pos, double *q, int64_t *id, int64_t cap, int64_t *n_out) = 0;
+    virtual void particles_exchange(double *pos_out, double *q_out, int64_t *id_out, int64_t cap, int64_t *n_out,
+                                    const double *pos_in, const double *q_in, const int64_t *id_in, int64_t n_in,
+                                    double mass) = 0;
     virtual int64_t particles_count() const = 0;
     virtual double particle_mass() const = 0;
     virtual void field_get(int f, double *host) = 0;
@@ -217,6 +220,13 @@ template <class R> struct Ctx final : CtxBase {
     DBuf<double2> tw64_full, tw64_half;  // mixed precision: FP64 twiddles of that measurement
     DBuf<double> stage;                  // particle / field transfer staging
     DBuf<int64_t> stage_id;
+    // particles_exchange: download and upload streams, four staging slots
+    // (two per direction), and the events that order them
+    cudaStream_t sdn = nullptr, sup = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_dn[2] = {nullptr, nullptr}, ev_dn_end = nullptr, ev_up_end = nullptr;
+    DBuf<double> xstage;
+    DBuf<int64_t> xstage_id;
+    static constexpr int64_t XCHUNK = 1 << 21;
     DBuf<float> lc_pos, lc_vel;
     DBuf<int64_t> lc_id;
     DBuf<unsigned long long> idset[8][2];   // per shell: ID logs of the previous and current cycle
@@ -287,6 +297,13 @@ template <class R> struct Ctx final : CtxBase {
             cudaStreamSynchronize(st);
             cudaStreamDestroy(st);
         }
+        for (cudaStream_t s : {sdn, sup})
+            if (s) {
+                cudaStreamSynchronize(s);
+                cudaStreamDestroy(s);
+            }
+        for (cudaEvent_t e : {ev_start, ev_dn[0], ev_dn[1], ev_dn_end, ev_up_end})
+            if (e) cudaEventDestroy(e);
     }
 
     cudaStream_t stream() override { return st; }
@@ -639,6 +656,92 @@ template <class R> struct Ctx final : CtxBase {
             if (id) ck(cudaMemcpyAsync(id + o, stage_id.p, c * sizeof(int64_t), cudaMemcpyDeviceToHost, st), "D2H");
             ck(cudaStreamSynchronize(st), "synchronize");
         }
+    }
+
+    // particles_get followed by particles_set, with the downloads on one copy
+    // stream and the uploads on another so that the two directions of the host
+    // link run at once, chunk by chunk.  The uploads fill the other particle
+    // buffer, so the device sides never conflict; on the host, an input array
+    // that is the matching output array waits chunk by chunk for its download,
+    // any other overlap of an input with an output waits for all downloads.
+    void particles_exchange(double *pos_out, double *q_out, int64_t *id_out, int64_t cap, int64_t *n_out,
+                            const double *pos_in, const double *q_in, const int64_t *id_in, int64_t n_in,
+                            double m) override
+    {
+        if (n_out) *n_out = np;
+        if (cap < np) throw CapacityError("host arrays smaller than the particle count");
+        if (np > 0 && (!pos_out || !q_out || !id_out)) throw ArgError("null particle array");
+        if (n_in < 0 || n_in > cfg.capacity) throw ArgError("particle count exceeds the context capacity");
+        if (n_in > 0 && (!pos_in || !q_in || !id_in)) throw ArgError("null particle array");
+        if (n_in >= (int64_t)UINT32_MAX) throw ArgError("particle count exceeds 2^32 - 1");
+        const int64_t nout = np;
+        struct Span { uintptr_t lo, hi; };
+        auto span = [](const void *p, int64_t bytes) { return Span{(uintptr_t)p, (uintptr_t)p + (uintptr_t)bytes}; };
+        const Span outs[3] = {span(pos_out, 24 * nout), span(q_out, 24 * nout), span(id_out, 8 * nout)};
+        const Span ins[3] = {span(pos_in, 24 * n_in), span(q_in, 24 * n_in), span(id_in, 8 * n_in)};
+        bool overlap = false;
+        for (const Span &i : ins)
+            for (const Span &o : outs) overlap |= i.lo < i.hi && o.lo < o.hi && i.lo < o.hi && o.lo < i.hi;
+        const bool same = pos_in == pos_out && q_in == q_out && id_in == id_out;
+        const bool chunkwise = !overlap || same;
+
+        if (!sdn) {
+            ck(cudaStreamCreateWithFlags(&sdn, cudaStreamNonBlocking), "cudaStreamCreate");
+            ck(cudaStreamCreateWithFlags(&sup, cudaStreamNonBlocking), "cudaStreamCreate");
+            for (cudaEvent_t *e : {&ev_start, &ev_dn[0], &ev_dn[1], &ev_dn_end, &ev_up_end})
+                ck(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
+        }
+        if ((int64_t)xstage.n < 4 * 6 * XCHUNK) xstage.alloc(4 * 6 * XCHUNK, "exchange staging");
+        if ((int64_t)xstage_id.n < 4 * XCHUNK) xstage_id.alloc(4 * XCHUNK, "exchange staging");
+        ck(cudaEventRecord(ev_start, st), "cudaEventRecord");
+        ck(cudaStreamWaitEvent(sdn, ev_start, 0), "cudaStreamWaitEvent");
+        ck(cudaStreamWaitEvent(sup, ev_start, 0), "cudaStreamWaitEvent");
+        const PView<R> src = cur(), dst = view(!cur_is_A);
+        const int64_t ndn = (nout + XCHUNK - 1) / XCHUNK, nup = (n_in + XCHUNK - 1) / XCHUNK;
+        auto down = [&](int64_t i) {
+            const int64_t o = i * XCHUNK, c = std::min(XCHUNK, nout - o);
+            double *sp = xstage.p + (i & 1) * 6 * XCHUNK;
+            int64_t *si = xstage_id.p + (i & 1) * XCHUNK;
+            PView<R> vo = src;
+            vo.cell += o; vo.off += o; vo.q += o; vo.id += o;
+            launch_store_particles<R>(vo, sp, sp + 3 * XCHUNK, si, c, g.N, sdn);
+            launched("store_particles");
+            ck(cudaMemcpyAsync(pos_out + 3 * o, sp, 3 * c * sizeof(double), cudaMemcpyDeviceToHost, sdn), "D2H");
+            ck(cudaMemcpyAsync(q_out + 3 * o, sp + 3 * XCHUNK, 3 * c * sizeof(double), cudaMemcpyDeviceToHost, sdn), "D2H");
+            ck(cudaMemcpyAsync(id_out + o, si, c * sizeof(int64_t), cudaMemcpyDeviceToHost, sdn), "D2H");
+            ck(cudaEventRecord(ev_dn[i & 1], sdn), "cudaEventRecord");
+        };
+        auto up = [&](int64_t i) {
+            const int64_t o = i * XCHUNK, c = std::min(XCHUNK, n_in - o);
+            double *sp = xstage.p + (2 + (i & 1)) * 6 * XCHUNK;
+            int64_t *si = xstage_id.p + (2 + (i & 1)) * XCHUNK;
+            if (chunkwise && same && i < ndn) ck(cudaStreamWaitEvent(sup, ev_dn[i & 1], 0), "cudaStreamWaitEvent");
+            ck(cudaMemcpyAsync(sp, pos_in + 3 * o, 3 * c * sizeof(double), cudaMemcpyHostToDevice, sup), "H2D");
+            ck(cudaMemcpyAsync(sp + 3 * XCHUNK, q_in + 3 * o, 3 * c * sizeof(double), cudaMemcpyHostToDevice, sup), "H2D");
+            ck(cudaMemcpyAsync(si, id_in + o, c * sizeof(int64_t), cudaMemcpyHostToDevice, sup), "H2D");
+            PView<R> vo = dst;
+            vo.cell += o; vo.off += o; vo.q += o; vo.id += o;
+            launch_load_particles<R>(vo, sp, sp + 3 * XCHUNK, si, c, g.N, derr.p, sup);
+            launched("load_particles");
+        };
+        for (int64_t i = 0; i < std::max(ndn, nup); i++) {
+            if (i < ndn) down(i);
+            if (chunkwise && i < nup) up(i);
+        }
+        ck(cudaEventRecord(ev_dn_end, sdn), "cudaEventRecord");
+        if (!chunkwise) {
+            ck(cudaStreamWaitEvent(sup, ev_dn_end, 0), "cudaStreamWaitEvent");
+            for (int64_t i = 0; i < nup; i++) up(i);
+        }
+        ck(cudaEventRecord(ev_up_end, sup), "cudaEventRecord");
+        ck(cudaStreamWaitEvent(st, ev_dn_end, 0), "cudaStreamWaitEvent");
+        ck(cudaStreamWaitEvent(st, ev_up_end, 0), "cudaStreamWaitEvent");
+        np = n_in;
+        mass = m;
+        cur_is_A = !cur_is_A;
+        rebin_from_cells();
+        have_particles = true;
+        sync();
     }
 
     int64_t particles_count() const override { return np; }
@@ -1193,6 +1296,15 @@ int gev_particles_set(gev_ctx *ctx, const double *pos, const double *q, const in
 int gev_particles_get(gev_ctx *ctx, double *pos, double *q, int64_t *id, int64_t capacity, int64_t *n_out)
 {
     return guarded(ctx, [&](gev::CtxBase &c) { c.particles_get(pos, q, id, capacity, n_out); });
+}
+
+int gev_particles_exchange(gev_ctx *ctx, double *pos_out, double *q_out, int64_t *id_out, int64_t capacity,
+                           int64_t *n_out, const double *pos_in, const double *q_in, const int64_t *id_in, int64_t n_in,
+                           double mass)
+{
+    return guarded(ctx, [&](gev::CtxBase &c) {
+        c.particles_exchange(pos_out, q_out, id_out, capacity, n_out, pos_in, q_in, id_in, n_in, mass);
+    });
 }
 
 int gev_particles_count(const gev_ctx *ctx, int64_t *n_out)

@@ -86,6 +86,7 @@ _last_error = _sig("gev_last_error", [_p], ctypes.c_char_p)
 _version = _sig("gev_version", [], ctypes.c_char_p)
 _pset = _sig("gev_particles_set", [_p, _p, _p, _p, _l, _d])
 _pget = _sig("gev_particles_get", [_p, _p, _p, _p, _l, ctypes.POINTER(_l)])
+_pxch = _sig("gev_particles_exchange", [_p, _p, _p, _p, _l, ctypes.POINTER(_l), _p, _p, _p, _l, _d])
 _pcount = _sig("gev_particles_count", [_p, ctypes.POINTER(_l)])
 _fget = _sig("gev_field_get", [_p, _i, _p])
 _fset = _sig("gev_field_set", [_p, _i, _p])
@@ -224,6 +225,24 @@ class Context:
         pos = np.empty((n.value, 3)); q = np.empty((n.value, 3)); ids = np.empty(n.value, dtype=np.int64)
         self._ck(_pget(self._h, _ptr(pos), _ptr(q), _ptr(ids), n.value, ctypes.byref(n)))
         return pos, q, ids
+
+    def exchange_particles(self, pos_out, q_out, ids_out, pos_in, q_in, ids_in, mass=1.0):
+        """Copy the current particles into the output arrays and load the input
+        arrays in one call, both directions of the host link at once
+        (gev_particles_exchange).  The output arrays are written in place:
+        float64 (n, 3), float64 (n, 3) and int64 (n,), C-contiguous; the
+        input arrays may be the same arrays.  Returns the number of particles
+        written."""
+        for arr, dt in ((pos_out, np.float64), (q_out, np.float64), (ids_out, np.int64)):
+            if not (isinstance(arr, np.ndarray) and arr.dtype == dt and arr.flags.c_contiguous):
+                raise TypeError("output arrays must be C-contiguous numpy arrays of float64/float64/int64")
+        pos_in = np.ascontiguousarray(pos_in, dtype=np.float64).reshape(-1, 3)
+        q_in = np.ascontiguousarray(q_in, dtype=np.float64).reshape(-1, 3)
+        ids_in = np.ascontiguousarray(ids_in, dtype=np.int64)
+        n = _l()
+        self._ck(_pxch(self._h, _ptr(pos_out), _ptr(q_out), _ptr(ids_out), ids_out.shape[0], ctypes.byref(n),
+                       _ptr(pos_in), _ptr(q_in), _ptr(ids_in), pos_in.shape[0], float(mass)))
+        return n.value
 
     # ---- fields ----
     def get_field(self, field):

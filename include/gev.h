@@ -95,6 +95,19 @@ int gev_particles_set(gev_ctx *ctx, const double *pos, const double *q, const in
 int gev_particles_get(gev_ctx *ctx, double *pos, double *q, int64_t *id, int64_t capacity,
                       int64_t *n_out);
 int gev_particles_count(const gev_ctx *ctx, int64_t *n_out);
+/* get followed by set in one call, with both directions of the host link in
+ * use at once: copies the current particles to (pos_out, q_out, id_out) as
+ * gev_particles_get does, and replaces them by the n_in particles of
+ * (pos_in, q_in, id_in) as gev_particles_set does (every array required),
+ * chunk by chunk, downloads and uploads on two copy streams.  The input
+ * arrays may be the output arrays themselves (each chunk is uploaded after it
+ * was downloaded: the state goes out and comes back in); other overlaps of an
+ * input with an output array are taken one direction after the other.
+ * Returns when both directions are complete.  No reference counterpart: it
+ * serves callers that keep the particle state on the host between cycles. */
+int gev_particles_exchange(gev_ctx *ctx, double *pos_out, double *q_out, int64_t *id_out, int64_t capacity,
+                           int64_t *n_out, const double *pos_in, const double *q_in, const int64_t *id_in,
+                           int64_t n_in, double mass);
 
 /* Field transfer in double precision (converted to/from the context precision). */
 int gev_field_get(gev_ctx *ctx, int32_t field, double *host);

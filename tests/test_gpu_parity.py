@@ -482,6 +482,55 @@ def test_rebin_order(prec):
 
 
 @pytest.mark.parametrize("prec", PRECS)
+def test_exchange_particles(prec):
+    """gev_particles_exchange = get then set, over several transfer chunks
+    (2^21 particles each): the downloaded state is the one get returns, the
+    uploaded one the one set makes; with the same arrays in and out the state
+    goes out and comes back; with arrays that partly overlap, the upload reads
+    what the download wrote; too small output arrays are refused."""
+    N = 256
+    na, nb = 4_500_000, 3_000_000
+    pa, qa, ia = particles(N, n=na, seed=61)
+    pb, qb, ib = particles(N, n=nb, seed=62)
+    with make_ctx(N, prec, na) as c:
+        c.set_particles(pa, qa, ia, MASS)
+        ref_a = c.get_particles()
+        out = (np.empty((na, 3)), np.empty((na, 3)), np.empty(na, dtype=np.int64))
+        assert c.exchange_particles(*out, pb, qb, ib, MASS) == na
+        for x, y in zip(out, ref_a):
+            assert np.array_equal(x, y)
+        got_b = c.get_particles()
+        c.set_particles(pb, qb, ib, MASS)
+        ref_b = c.get_particles()
+        for x, y in zip(got_b, ref_b):
+            assert np.array_equal(x, y)
+        # the same arrays out and in
+        x = tuple(np.ascontiguousarray(v) for v in ref_b)
+        assert c.exchange_particles(*x, *x, MASS) == nb
+        for u, v in zip(x, ref_b):
+            assert np.array_equal(u, v)
+        got = c.get_particles()
+        c.set_particles(*ref_b, MASS)
+        for u, v in zip(got, c.get_particles()):
+            assert np.array_equal(u, v)
+        # partly overlapping arrays: out = rows [0, nb), in = rows [h, h + nb)
+        h = nb // 2
+        P = np.zeros((nb + h, 3)); Q = np.zeros((nb + h, 3)); I = np.zeros(nb + h, dtype=np.int64)
+        P[nb:], Q[nb:], I[nb:] = pa[:h], qa[:h], ia[:h] + 10 ** 9
+        c.exchange_particles(P[:nb], Q[:nb], I[:nb], P[h:], Q[h:], I[h:], MASS)
+        for u, v in zip((P[:nb], Q[:nb], I[:nb]), ref_b):
+            assert np.array_equal(u, v)
+        got = c.get_particles()
+        c.set_particles(P[h:].copy(), Q[h:].copy(), I[h:].copy(), MASS)
+        for u, v in zip(got, c.get_particles()):
+            assert np.array_equal(u, v)
+        small = (np.empty((10, 3)), np.empty((10, 3)), np.empty(10, dtype=np.int64))
+        with pytest.raises(gev.GevError):
+            c.exchange_particles(*small, pb, qb, ib, MASS)
+        assert c.get_particles()[0].shape == (nb, 3)   # the context stays usable
+
+
+@pytest.mark.parametrize("prec", PRECS)
 def test_empty_and_invalid_particle_input(prec):
     """No particles: every projection is zero and the cycle runs; a context
     without particles refuses to project; a non-finite coordinate surfaces as
