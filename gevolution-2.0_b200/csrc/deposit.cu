@@ -94,6 +94,14 @@ template <int KIND> struct DepShape {
     static constexpr int NFP = (NF + 3) & ~3;   // padded for 16-byte record loads
     static constexpr int CIJ = HAS00 ? 1 : 0;   // first Tij output component
     static constexpr int CS = CIJ + (HASIJ ? 6 : 0);   // first S output component
+    // Record slots of the Tij weights (k = 00, 11, 22, 01, 02, 12) and of the
+    // S momenta.  The 16-value T00+Tij+S record is [d0 d1 d2 E | F G W00 W11 |
+    // W22 P0 P1 P2 | W01 W02 W12 -]: the off-diagonal weights, which only the
+    // vertices two or three of whose offsets are 0 receive, fill the last
+    // 16-byte chunk, which the other half of the gather's corners never load.
+    static constexpr bool SPLIT = HAS00 && HASIJ && HASS;
+    __host__ __device__ static constexpr int fij(int k) { return SPLIT && k >= 3 ? 12 + (k - 3) : FIJ + k; }
+    __host__ __device__ static constexpr int fs(int k) { return SPLIT ? FS - 3 + k : FS + k; }
 };
 
 constexpr int DEP_NCELL = 729;                  // 9^3 cells of a tile's reach
@@ -163,7 +171,7 @@ __device__ __forceinline__ bool make_record(const RawParticle<R> &pr, int N, con
         const int comp[6] = {0, 3, 5, 1, 2, 4};
 #pragma unroll
         for (int k = 0; k < 6; k++) {
-            v[S::FIJ + k] = W[k];
+            v[S::fij(k)] = W[k];
             bnd[S::CIJ + comp[k]] = fabs(W[k]);
         }
     }
@@ -177,7 +185,7 @@ __device__ __forceinline__ bool make_record(const RawParticle<R> &pr, int N, con
     if constexpr (S::HASS) {
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            v[S::FS + k] = m0i * q[k];
+            v[S::fs(k)] = m0i * q[k];
             bnd[S::CS + k] = fabs(m0i * q[k]);
         }
     }
@@ -196,7 +204,7 @@ template <class R, int KIND> __device__ __forceinline__ void scale_record(R *r, 
     if constexpr (S::HASIJ) {
         const int comp[6] = {0, 3, 5, 1, 2, 4};
 #pragma unroll
-        for (int k = 0; k < 6; k++) r[S::FIJ + k] *= scl[S::CIJ + comp[k]];
+        for (int k = 0; k < 6; k++) r[S::fij(k)] *= scl[S::CIJ + comp[k]];
     }
     if constexpr (S::HAS0I) {
 #pragma unroll
@@ -204,7 +212,7 @@ template <class R, int KIND> __device__ __forceinline__ void scale_record(R *r, 
     }
     if constexpr (S::HASS) {
 #pragma unroll
-        for (int k = 0; k < 3; k++) r[S::FS + k] *= scl[S::CS + k];
+        for (int k = 0; k < 3; k++) r[S::fs(k)] *= scl[S::CS + k];
     }
 }
 
@@ -224,12 +232,12 @@ __device__ __forceinline__ void gather_one(const R *r, int bx, int by, int bz, R
     }
     if constexpr (S::HASIJ) {
         constexpr int C = S::CIJ;
-        acc[C + 0] += to_fixed<R>(w * r[S::FIJ + 0]);
-        acc[C + 3] += to_fixed<R>(w * r[S::FIJ + 1]);
-        acc[C + 5] += to_fixed<R>(w * r[S::FIJ + 2]);
-        if (!bx && !by) acc[C + 1] += to_fixed<R>(wz * r[S::FIJ + 3]);   // (0,1): x and x+e2
-        if (!bx && !bz) acc[C + 2] += to_fixed<R>(wy * r[S::FIJ + 4]);   // (0,2): x and x+e1
-        if (!by && !bz) acc[C + 4] += to_fixed<R>(wx * r[S::FIJ + 5]);   // (1,2): x and x+e0
+        acc[C + 0] += to_fixed<R>(w * r[S::fij(0)]);
+        acc[C + 3] += to_fixed<R>(w * r[S::fij(1)]);
+        acc[C + 5] += to_fixed<R>(w * r[S::fij(2)]);
+        if (!bx && !by) acc[C + 1] += to_fixed<R>(wz * r[S::fij(3)]);   // (0,1): x and x+e2
+        if (!bx && !bz) acc[C + 2] += to_fixed<R>(wy * r[S::fij(4)]);   // (0,2): x and x+e1
+        if (!by && !bz) acc[C + 4] += to_fixed<R>(wx * r[S::fij(5)]);   // (1,2): x and x+e0
     }
     if constexpr (S::HAS0I) {
         // component i lands on the vertices with b_i = 0, weighted by the other two
@@ -240,9 +248,9 @@ __device__ __forceinline__ void gather_one(const R *r, int bx, int by, int bz, R
     }
     if constexpr (S::HASS) {
         constexpr int C = S::CS;
-        if (!bx) acc[C + 0] += to_fixed<R>(wy * wz * r[S::FS + 0]);
-        if (!by) acc[C + 1] += to_fixed<R>(wx * wz * r[S::FS + 1]);
-        if (!bz) acc[C + 2] += to_fixed<R>(wx * wy * r[S::FS + 2]);
+        if (!bx) acc[C + 0] += to_fixed<R>(wy * wz * r[S::fs(0)]);
+        if (!by) acc[C + 1] += to_fixed<R>(wx * wz * r[S::fs(1)]);
+        if (!bz) acc[C + 2] += to_fixed<R>(wx * wy * r[S::fs(2)]);
     }
 }
 
@@ -261,12 +269,12 @@ __device__ __forceinline__ void gather_sum(const R *r, int bx, int by, int bz, R
     }
     if constexpr (S::HASIJ) {
         constexpr int C = S::CIJ;
-        acc[C + 0] += w * r[S::FIJ + 0];
-        acc[C + 3] += w * r[S::FIJ + 1];
-        acc[C + 5] += w * r[S::FIJ + 2];
-        if (!bx && !by) acc[C + 1] += wz * r[S::FIJ + 3];
-        if (!bx && !bz) acc[C + 2] += wy * r[S::FIJ + 4];
-        if (!by && !bz) acc[C + 4] += wx * r[S::FIJ + 5];
+        acc[C + 0] += w * r[S::fij(0)];
+        acc[C + 3] += w * r[S::fij(1)];
+        acc[C + 5] += w * r[S::fij(2)];
+        if (!bx && !by) acc[C + 1] += wz * r[S::fij(3)];
+        if (!bx && !bz) acc[C + 2] += wy * r[S::fij(4)];
+        if (!by && !bz) acc[C + 4] += wx * r[S::fij(5)];
     }
     if constexpr (S::HAS0I) {
         if (!bx) acc[0] += wy * wz * r[S::F0I + 0] * ((R)1 + phv + phx);
@@ -275,9 +283,9 @@ __device__ __forceinline__ void gather_sum(const R *r, int bx, int by, int bz, R
     }
     if constexpr (S::HASS) {
         constexpr int C = S::CS;
-        if (!bx) acc[C + 0] += wy * wz * r[S::FS + 0];
-        if (!by) acc[C + 1] += wx * wz * r[S::FS + 1];
-        if (!bz) acc[C + 2] += wx * wy * r[S::FS + 2];
+        if (!bx) acc[C + 0] += wy * wz * r[S::fs(0)];
+        if (!by) acc[C + 1] += wx * wz * r[S::fs(1)];
+        if (!bz) acc[C + 2] += wx * wy * r[S::fs(2)];
     }
 }
 
