@@ -2,7 +2,7 @@
 //
 // One CTA owns the 8^3 vertices of a tile, one thread per vertex, and gathers
 // every particle whose CIC stencil touches them: its own 8 class buckets plus
-// the face-class buckets of the 7 lower neighbour tiles (tile_segments_block).
+// the face-class buckets of the 7 lower neighbour tiles (tile_segments_warp).
 //
 // The CTA
 //   1. turns each particle into a short record of per-particle factors (in the
@@ -106,6 +106,7 @@ template <int KIND> struct DepShape {
 
 constexpr int DEP_NCELL = 729;                  // 9^3 cells of a tile's reach
 constexpr uint16_t DEP_SKIP = 0xFFFFu;
+constexpr int DEP_RUN_NONE = 0x7fffffff;        // run start of a reach cell without records
 
 template <class R> __device__ __forceinline__ long long to_fixed(R v);
 template <> __device__ __forceinline__ long long to_fixed<float>(float v) { return __float2ll_rn(v); }
@@ -420,9 +421,26 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
         const int j = t + u * DEP_NT;
         if ((uint32_t)j < own_n) raw[u] = load_particle(p, own_lo + (uint32_t)j);
     }
-    tile_segments_block(bstart, nt, tx, ty, tz, seg_lo, seg_hi, seg_pre);
+    // the candidate ranges, formed by every warp in registers: the single-chunk
+    // path's neighbour particles are loaded before the barrier below, so their
+    // loads are in flight with the phi stencil and the own particles; warp 0
+    // stores the ranges for the dense-tile paths, and the barrier publishes
+    // them with the phi stencil and the per-cell run bounds
+    TileSegs ts{};
+    if (!DENSE || t < 32) ts = tile_segments_warp(bstart, nt, tx, ty, tz);
+    if (t < 32) tile_segments_store(ts, seg_lo, seg_hi, seg_pre);
+    if constexpr (!DENSE) {
+        if (ts.total <= (uint32_t)CH) {
+#pragma unroll
+            for (int u = 0; u < PP; u++) {
+                const int j = t + u * DEP_NT;
+                const uint32_t src = tile_seg_find(ts, (uint32_t)j);
+                if ((uint32_t)j < ts.total && (uint32_t)j >= own_n) raw[u] = load_particle(p, src);
+            }
+        }
+    }
     if (t < NC) vmax[t] = 0ull;
-    for (int c = t; c < 730; c += DEP_NT) { cstart[c] = 0; ccount[c] = 0; }
+    for (int c = t; c < 730; c += DEP_NT) { cstart[c] = DEP_RUN_NONE; ccount[c] = 0; }
     if (USE_PHI) {
 #pragma unroll
         for (int k = 0; k < PER; k++) {
@@ -495,7 +513,12 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
     // acc in the field precision, in the fixed order (source cell, then ID).
     const int lc0 = (vx + 1) + 9 * ((vy + 1) + 9 * (vz + 1));
     auto sorted_chunk = [&](int n, RawParticle<R> (&raw)[PP], R (&acc)[NC]) {
-        // 1. record j at position j, and the reach cell it came from
+        // 1. record j at position j, the reach cell it came from, and the
+        //    bounds [cstart, cend) of that cell's run as the smallest and
+        //    largest positions of its records (shared-memory atomic min / max:
+        //    the bounds do not depend on the order of the updates; cend shares
+        //    ccount's storage, cstart starts at DEP_RUN_NONE, cend at 0)
+        int *cend = ccount;
 #pragma unroll
         for (int u = 0; u < PP; u++) {
             const int j = t + u * DEP_NT;
@@ -505,34 +528,28 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
             if (make_record<R, KIND, USE_PHI>(raw[u], N, fN, x0, y0, z0, phis, ra, rm00, rmij, rm0i, v, lc, b)) {
                 store_record<R, NFP>(rec, j, v);
                 rcell[j] = (uint16_t)lc;
+                atomicMin(&cstart[lc], j);
+                atomicMax(&cend[lc], j + 1);
             } else {
                 rcell[j] = DEP_SKIP;
             }
         }
         __syncthreads();
-        // 2. cell runs [cstart, cend) from the run boundaries (cend shares ccount's storage)
-        int *cend = ccount;
-        for (int j = t; j < n; j += DEP_NT) {
-            const uint16_t lc = rcell[j];
-            if (lc == DEP_SKIP) continue;
-            if (j == 0 || rcell[j - 1] != lc) cstart[lc] = j;
-            if (j == n - 1 || rcell[j + 1] != lc) cend[lc] = j + 1;
-        }
-        __syncthreads();
-        // 3. every record lies inside its cell's run and is followed by the
-        //    same cell up to the run's end: then each run holds exactly its
-        //    cell's records (otherwise the bucket order was not sorted by cell)
+        // 2. every record is followed by the same cell up to its run's end:
+        //    then each run holds exactly its cell's records (otherwise the
+        //    bucket order was not sorted by cell)
         {
             bool bad = false;
             for (int j = t; j < n; j += DEP_NT) {
                 const uint16_t lc = rcell[j];
                 if (lc == DEP_SKIP) continue;
                 const int e = cend[lc];
-                bad |= j < cstart[lc] || j >= e || (j + 1 < e && rcell[j + 1] != lc);
+                bad |= j + 1 < e && rcell[j + 1] != lc;
             }
             if (bad) atomicOr(err, ERR_BAD_ORDER);
         }
-        // 4. gather: the vertex receives from the cells v - b, b in {0,1}^3
+        // 3. gather: the vertex receives from the cells v - b, b in {0,1}^3
+        //    (a cell without records has cstart = DEP_RUN_NONE > cend = 0)
 #pragma unroll
         for (int b = 0; b < 8; b++) {
             const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
@@ -559,13 +576,7 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
         // the candidate buckets the records of each reach cell form one run,
         // already ordered by ID -- the sum is independent of the order in
         // which the particles were given.
-        const int n = (int)total;
-        // the neighbours' particles (the own ones are loaded already)
-#pragma unroll
-        for (int u = 0; u < PP; u++) {
-            const int j = t + u * DEP_NT;
-            if (j < n && (uint32_t)j >= own_n) raw[u] = load_particle(p, seg_find(seg_lo, seg_pre, (uint32_t)j));
-        }
+        const int n = (int)total;   // every candidate's particle is loaded already
         R acc[NC];
 #pragma unroll
         for (int c = 0; c < NC; c++) acc[c] = 0;
@@ -588,9 +599,11 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
         for (uint32_t base = 0; base < total; base += (uint32_t)CH) {
             const int n = (int)min((uint32_t)CH, total - base);
             if (base > 0) {
-                // records and runs of the previous chunk are done with
+                // records and runs of the previous chunk are done with; the run
+                // bounds start over before any record of this chunk updates them
                 __syncthreads();
-                for (int c = t; c < 730; c += DEP_NT) { cstart[c] = 0; ccount[c] = 0; }
+                for (int c = t; c < 730; c += DEP_NT) { cstart[c] = DEP_RUN_NONE; ccount[c] = 0; }
+                __syncthreads();
             }
             // the chunk's particles (of the first chunk, the own ones are loaded already)
 #pragma unroll

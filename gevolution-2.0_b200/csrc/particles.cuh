@@ -49,19 +49,26 @@ __host__ __device__ __forceinline__ int class_ord(int lx, int ly, int lz)
 
 // Particle ranges a tile's deposit needs: its own 8 class buckets and, from
 // each of the 7 lower neighbour tiles, the classes whose cells lie on the
-// shared faces.  Block-cooperative: thread k < 64 reads candidate k =
-// (neighbour offset m = k >> 3, class c = k & 7), the range of that class in
-// the neighbour tile when the class lies on the faces shared with this tile
-// (c & m == m) and an empty range otherwise; warp 0 then forms the exclusive
-// prefix sums of the 64 range lengths.  seg_lo/seg_hi hold 64 entries and
-// seg_pre 65; the particle at position i of the concatenation is found with
-// seg_find.  Contains __syncthreads(); every thread of the block must call it.
-__device__ __forceinline__ void tile_segments_block(const uint32_t *bstart, int nt, int tx, int ty, int tz,
-                                                    uint32_t *seg_lo, uint32_t *seg_hi, uint32_t *seg_pre)
+// shared faces.  Candidate k = (neighbour offset m = k >> 3, class c = k & 7)
+// is the range of that class in the neighbour tile when the class lies on the
+// faces shared with this tile (c & m == m) and an empty range otherwise; pre
+// holds the exclusive prefix sums of the 64 range lengths.  Formed by every
+// warp that needs them, in registers (lane l holds candidates l and l + 32),
+// with no block barrier; tile_segments_store copies them to shared memory
+// (seg_lo, seg_hi: 64 entries, seg_pre: 65) for seg_find and seg_index.
+struct TileSegs {
+    uint32_t lo[2], hi[2], pre[2];   // candidates l and l + 32 of lane l
+    uint32_t total;                  // length of the concatenation
+};
+
+__device__ __forceinline__ TileSegs tile_segments_warp(const uint32_t *bstart, int nt, int tx, int ty, int tz)
 {
-    const int t = threadIdx.x;
-    if (t < 64) {
-        const int m = t >> 3, c = t & 7;
+    const int l = threadIdx.x & 31;
+    TileSegs s;
+    uint32_t len[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int k = l + 32 * h, m = k >> 3, c = k & 7;
         uint32_t lo = 0, hi = 0;
         if ((c & m) == m) {
             const int dx = m & 1, dy = (m >> 1) & 1, dz = (m >> 2) & 1;
@@ -72,23 +79,55 @@ __device__ __forceinline__ void tile_segments_block(const uint32_t *bstart, int 
             lo = bstart[8 * nb + c];
             hi = bstart[8 * nb + c + 1];
         }
-        seg_lo[t] = lo;
-        seg_hi[t] = hi > lo ? hi : lo;
+        hi = hi > lo ? hi : lo;
+        s.lo[h] = lo;
+        s.hi[h] = hi;
+        len[h] = hi - lo;
     }
-    __syncthreads();
-    if (t < 32) {
-        const uint32_t n0 = seg_hi[2 * t] - seg_lo[2 * t], n1 = seg_hi[2 * t + 1] - seg_lo[2 * t + 1];
-        uint32_t s = n0 + n1, incl = s;
+    uint32_t inc0 = len[0], inc1 = len[1];
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t u = __shfl_up_sync(0xffffffffu, incl, o);
-            if (t >= o) incl += u;
-        }
-        seg_pre[2 * t] = incl - s;
-        seg_pre[2 * t + 1] = incl - s + n0;
-        if (t == 31) seg_pre[64] = incl;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t u0 = __shfl_up_sync(0xffffffffu, inc0, o);
+        const uint32_t u1 = __shfl_up_sync(0xffffffffu, inc1, o);
+        if (l >= o) { inc0 += u0; inc1 += u1; }
     }
-    __syncthreads();
+    const uint32_t tot0 = __shfl_sync(0xffffffffu, inc0, 31);
+    s.pre[0] = inc0 - len[0];
+    s.pre[1] = tot0 + inc1 - len[1];
+    s.total = __shfl_sync(0xffffffffu, tot0 + inc1, 31);
+    return s;
+}
+
+// one warp's segments to shared memory (the caller's next __syncthreads()
+// publishes them to the block)
+__device__ __forceinline__ void tile_segments_store(const TileSegs &s, uint32_t *seg_lo, uint32_t *seg_hi,
+                                                    uint32_t *seg_pre)
+{
+    const int l = threadIdx.x & 31;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        seg_lo[l + 32 * h] = s.lo[h];
+        seg_hi[l + 32 * h] = s.hi[h];
+        seg_pre[l + 32 * h] = s.pre[h];
+    }
+    if (l == 31) seg_pre[64] = s.total;
+}
+
+// seg_find on the warp's registers: position i (< total) -> particle index.
+// Every lane of the warp must call it (lanes whose i is out of range get an
+// unspecified index and must not use it).
+__device__ __forceinline__ uint32_t tile_seg_find(const TileSegs &s, uint32_t i)
+{
+    auto at = [&](const uint32_t (&v)[2], int k) {
+        const uint32_t a = __shfl_sync(0xffffffffu, v[0], k & 31);
+        const uint32_t b = __shfl_sync(0xffffffffu, v[1], k & 31);
+        return k < 32 ? a : b;
+    };
+    int lo = 0;
+#pragma unroll
+    for (int step = 32; step > 0; step >>= 1)
+        if (at(s.pre, lo + step) <= i) lo += step;
+    return at(s.lo, lo) + (i - at(s.pre, lo));
 }
 
 // position i (< seg_pre[64]) of the concatenated candidate ranges -> particle index

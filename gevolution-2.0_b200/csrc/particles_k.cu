@@ -145,6 +145,12 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
         for (int k = 0; k < 8; k++)
             w8[k] = (((k >> 2) & 1) ? d[0] : (R)1 - d[0]) * (((k >> 1) & 1) ? d[1] : (R)1 - d[1]) * ((k & 1) ? d[2] : (R)1 - d[2]);
 
+        // The drift interpolates phi and B_i at the position the kick used
+        // (the particle has not moved yet): when both run, the kick's sums are
+        // kept for it -- phi(x) and the bilinear B_i interpolations in the
+        // planes x_i = 0 of the cell.
+        R phi_x = 0, B_x[3] = {0, 0, 0};
+        bool kick_phi = false, kick_B = false;
         if (kp.do_kick && ok) {
             // update_q, gevolution.hpp:888-1011
             const R a = (R)kp.a_k;
@@ -154,6 +160,8 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
             R phiint = 0;
 #pragma unroll
             for (int k = 0; k < 8; k++) phiint += w8[k] * SF(P_, rx, ry, rz, (k >> 2) & 1, (k >> 1) & 1, k & 1);
+            phi_x = phiint;
+            kick_phi = true;
             const R ie2 = recip(e2);
             phiint *= ie2;
             phiint = (R)4 * phiint * v2 + ((R)1 + a * a * phiint) * (v2 + e2) * ie2;
@@ -204,18 +212,22 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
                     return wxy[0] * SF(B2, rx, ry, rz, 0, 0, z) + wxy[1] * SF(B2, rx, ry, rz, 1, 0, z) +
                            wxy[2] * SF(B2, rx, ry, rz, 0, 1, z) + wxy[3] * SF(B2, rx, ry, rz, 1, 1, z);
                 };
+                B_x[0] = I0(0);
+                B_x[1] = I1(0);
+                B_x[2] = I2(0);
+                kick_B = true;
                 R pg[3];
                 pg[0] = ((1 - d[2]) * (SF(B1, rx, ry, rz, 1, 0, 0) - SF(B1, rx, ry, rz, 0, 0, 0)) + d[2] * (SF(B1, rx, ry, rz, 1, 0, 1) - SF(B1, rx, ry, rz, 0, 0, 1))) * v[1];
                 pg[0] += ((1 - d[1]) * (SF(B2, rx, ry, rz, 1, 0, 0) - SF(B2, rx, ry, rz, 0, 0, 0)) + d[1] * (SF(B2, rx, ry, rz, 1, 1, 0) - SF(B2, rx, ry, rz, 0, 1, 0))) * v[2];
-                pg[0] += ((d[0] - 1) * I0(-1) + (1 - 2 * d[0]) * I0(0) + d[0] * I0(1)) * v[0];
+                pg[0] += ((d[0] - 1) * I0(-1) + (1 - 2 * d[0]) * B_x[0] + d[0] * I0(1)) * v[0];
 
                 pg[1] = ((1 - d[0]) * (SF(B2, rx, ry, rz, 0, 1, 0) - SF(B2, rx, ry, rz, 0, 0, 0)) + d[0] * (SF(B2, rx, ry, rz, 1, 1, 0) - SF(B2, rx, ry, rz, 1, 0, 0))) * v[2];
                 pg[1] += ((1 - d[2]) * (SF(B0, rx, ry, rz, 0, 1, 0) - SF(B0, rx, ry, rz, 0, 0, 0)) + d[2] * (SF(B0, rx, ry, rz, 0, 1, 1) - SF(B0, rx, ry, rz, 0, 0, 1))) * v[0];
-                pg[1] += ((d[1] - 1) * I1(-1) + (1 - 2 * d[1]) * I1(0) + d[1] * I1(1)) * v[1];
+                pg[1] += ((d[1] - 1) * I1(-1) + (1 - 2 * d[1]) * B_x[1] + d[1] * I1(1)) * v[1];
 
                 pg[2] = ((1 - d[1]) * (SF(B0, rx, ry, rz, 0, 0, 1) - SF(B0, rx, ry, rz, 0, 0, 0)) + d[1] * (SF(B0, rx, ry, rz, 0, 1, 1) - SF(B0, rx, ry, rz, 0, 1, 0))) * v[0];
                 pg[2] += ((1 - d[0]) * (SF(B1, rx, ry, rz, 0, 0, 1) - SF(B1, rx, ry, rz, 0, 0, 0)) + d[0] * (SF(B1, rx, ry, rz, 1, 0, 1) - SF(B1, rx, ry, rz, 1, 0, 0))) * v[1];
-                pg[2] += ((d[2] - 1) * I2(-1) + (1 - 2 * d[2]) * I2(0) + d[2] * I2(1)) * v[2];
+                pg[2] += ((d[2] - 1) * I2(-1) + (1 - 2 * d[2]) * B_x[2] + d[2] * I2(1)) * v[2];
 #pragma unroll
                 for (int c = 0; c < 3; c++) gradphi[c] += pg[c] * (ib_k * ie);
             }
@@ -238,8 +250,12 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
             R e2 = v2 + a * a;
             R ph = 0, ch = 0;
             if (kp.nfield_d >= 1) {
+                if (kick_phi) {
+                    ph = phi_x;
+                } else {
 #pragma unroll
-                for (int k = 0; k < 8; k++) ph += w8[k] * SF(P_, rx, ry, rz, (k >> 2) & 1, (k >> 1) & 1, k & 1);
+                    for (int k = 0; k < 8; k++) ph += w8[k] * SF(P_, rx, ry, rz, (k >> 2) & 1, (k >> 1) & 1, k & 1);
+                }
             }
             if (kp.nfield_d >= 2) {
 #pragma unroll
@@ -248,15 +264,21 @@ __global__ void __launch_bounds__(KD_NT, sizeof(R) == 4 ? 4 : 2) k_kick_drift(PV
             v2 = ((R)1 + ((R)3 - v2 * recip(e2)) * ph - ch) * rsqrt_r(e2);
             R dp[3] = {v[0] * v2, v[1] * v2, v[2] * v2};
             if (kp.nfield_d >= 3) {
-                R b0 = SF(B0, rx, ry, rz, 0, 0, 0) * (1 - d[1]) * (1 - d[2]) + SF(B0, rx, ry, rz, 0, 1, 0) * d[1] * (1 - d[2]) +
-                            SF(B0, rx, ry, rz, 0, 0, 1) * (1 - d[1]) * d[2] + SF(B0, rx, ry, rz, 0, 1, 1) * d[1] * d[2];
-                R b1 = SF(B1, rx, ry, rz, 0, 0, 0) * (1 - d[0]) * (1 - d[2]) + SF(B1, rx, ry, rz, 1, 0, 0) * d[0] * (1 - d[2]) +
-                            SF(B1, rx, ry, rz, 0, 0, 1) * (1 - d[0]) * d[2] + SF(B1, rx, ry, rz, 1, 0, 1) * d[0] * d[2];
-                R b2 = SF(B2, rx, ry, rz, 0, 0, 0) * (1 - d[0]) * (1 - d[1]) + SF(B2, rx, ry, rz, 1, 0, 0) * d[0] * (1 - d[1]) +
-                            SF(B2, rx, ry, rz, 0, 1, 0) * (1 - d[0]) * d[1] + SF(B2, rx, ry, rz, 1, 1, 0) * d[0] * d[1];
-                dp[0] += b0 * ib_d;
-                dp[1] += b1 * ib_d;
-                dp[2] += b2 * ib_d;
+                if (!kick_B) {
+                    // the kick's bilinear interpolations, in the same form
+                    const R wyz[4] = {(1 - d[1]) * (1 - d[2]), d[1] * (1 - d[2]), (1 - d[1]) * d[2], d[1] * d[2]};
+                    const R wxz[4] = {(1 - d[0]) * (1 - d[2]), d[0] * (1 - d[2]), (1 - d[0]) * d[2], d[0] * d[2]};
+                    const R wxy[4] = {(1 - d[0]) * (1 - d[1]), d[0] * (1 - d[1]), (1 - d[0]) * d[1], d[0] * d[1]};
+                    B_x[0] = wyz[0] * SF(B0, rx, ry, rz, 0, 0, 0) + wyz[1] * SF(B0, rx, ry, rz, 0, 1, 0) +
+                             wyz[2] * SF(B0, rx, ry, rz, 0, 0, 1) + wyz[3] * SF(B0, rx, ry, rz, 0, 1, 1);
+                    B_x[1] = wxz[0] * SF(B1, rx, ry, rz, 0, 0, 0) + wxz[1] * SF(B1, rx, ry, rz, 1, 0, 0) +
+                             wxz[2] * SF(B1, rx, ry, rz, 0, 0, 1) + wxz[3] * SF(B1, rx, ry, rz, 1, 0, 1);
+                    B_x[2] = wxy[0] * SF(B2, rx, ry, rz, 0, 0, 0) + wxy[1] * SF(B2, rx, ry, rz, 1, 0, 0) +
+                             wxy[2] * SF(B2, rx, ry, rz, 0, 1, 0) + wxy[3] * SF(B2, rx, ry, rz, 1, 1, 0);
+                }
+                dp[0] += B_x[0] * ib_d;
+                dp[1] += B_x[1] * ib_d;
+                dp[2] += B_x[2] * ib_d;
             }
             int cc[3] = {cx, cy, cz};
 #pragma unroll
