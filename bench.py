@@ -156,11 +156,12 @@ SINGLE_KERNEL_STAGES = ("deposit_T00_Tij_T0i",)
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
 # ncu --set full capture of each deposit kernel at 256^3 in mixed precision
 # (python bench.py --N 256 --steps 2 --warmup 3 --no-fp64 --no-e2e --no-cpu
-# --no-adjoint under ncu -k regex:"k_deposit(_dense)?<float, \(int\)4" -c 2 for
-# the cycle's deposit, its tile launch plus its dense-tile launch; the separate
-# T00+Tij and T0i kernels from the earlier capture of the single-launch form),
-# scaled by the particle count; the profiles/ summaries record the captures
-NCU_TRAFFIC_256 = {"deposit_T00_Tij_T0i": 0.7478e9 + 0.6360e9 + 0.0001e9, "deposit_T00_Tij": 0.7451e9 + 0.4423e9,
+# --no-adjoint --no-late under ncu -k regex:"k_deposit<float, \(int\)4" for the
+# cycle's deposit, its tile launch, plus its dense-tile launch (0.07 MB) from
+# the capture of the two-launch form; the separate T00+Tij and T0i kernels
+# from the earlier capture of the single-launch form), scaled by the particle
+# count; the profiles/ summaries record the captures
+NCU_TRAFFIC_256 = {"deposit_T00_Tij_T0i": 0.7499e9 + 0.6387e9 + 0.0001e9, "deposit_T00_Tij": 0.7451e9 + 0.4423e9,
                    "deposit_T0i": 0.7434e9 + 0.1865e9}
 
 

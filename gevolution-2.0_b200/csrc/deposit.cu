@@ -421,23 +421,12 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
         const int j = t + u * DEP_NT;
         if ((uint32_t)j < own_n) raw[u] = load_particle(p, own_lo + (uint32_t)j);
     }
-    // the candidate ranges, formed by every warp in registers: the single-chunk
-    // path's neighbour particles are loaded before the barrier below, so their
-    // loads are in flight with the phi stencil and the own particles; warp 0
-    // stores the ranges for the dense-tile paths, and the barrier publishes
-    // them with the phi stencil and the per-cell run bounds
-    TileSegs ts{};
-    if (!DENSE || t < 32) ts = tile_segments_warp(bstart, nt, tx, ty, tz);
-    if (t < 32) tile_segments_store(ts, seg_lo, seg_hi, seg_pre);
-    if constexpr (!DENSE) {
-        if (ts.total <= (uint32_t)CH) {
-#pragma unroll
-            for (int u = 0; u < PP; u++) {
-                const int j = t + u * DEP_NT;
-                const uint32_t src = tile_seg_find(ts, (uint32_t)j);
-                if ((uint32_t)j < ts.total && (uint32_t)j >= own_n) raw[u] = load_particle(p, src);
-            }
-        }
+    // the candidate ranges, formed by warp 0 in registers and stored to shared
+    // memory; the barrier below publishes them together with the phi stencil
+    // and the per-cell run bounds (no barrier of their own)
+    if (t < 32) {
+        const TileSegs ts = tile_segments_warp(bstart, nt, tx, ty, tz);
+        tile_segments_store(ts, seg_lo, seg_hi, seg_pre);
     }
     if (t < NC) vmax[t] = 0ull;
     for (int c = t; c < 730; c += DEP_NT) { cstart[c] = DEP_RUN_NONE; ccount[c] = 0; }
@@ -576,7 +565,13 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
         // the candidate buckets the records of each reach cell form one run,
         // already ordered by ID -- the sum is independent of the order in
         // which the particles were given.
-        const int n = (int)total;   // every candidate's particle is loaded already
+        const int n = (int)total;
+        // the neighbours' particles (the own ones are loaded already)
+#pragma unroll
+        for (int u = 0; u < PP; u++) {
+            const int j = t + u * DEP_NT;
+            if (j < n && (uint32_t)j >= own_n) raw[u] = load_particle(p, seg_find(seg_lo, seg_pre, (uint32_t)j));
+        }
         R acc[NC];
 #pragma unroll
         for (int c = 0; c < NC; c++) acc[c] = 0;

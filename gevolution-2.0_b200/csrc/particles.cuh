@@ -52,10 +52,10 @@ __host__ __device__ __forceinline__ int class_ord(int lx, int ly, int lz)
 // shared faces.  Candidate k = (neighbour offset m = k >> 3, class c = k & 7)
 // is the range of that class in the neighbour tile when the class lies on the
 // faces shared with this tile (c & m == m) and an empty range otherwise; pre
-// holds the exclusive prefix sums of the 64 range lengths.  Formed by every
-// warp that needs them, in registers (lane l holds candidates l and l + 32),
-// with no block barrier; tile_segments_store copies them to shared memory
-// (seg_lo, seg_hi: 64 entries, seg_pre: 65) for seg_find and seg_index.
+// holds the exclusive prefix sums of the 64 range lengths.  Formed by one
+// warp in registers (lane l holds candidates l and l + 32) with no block
+// barrier; tile_segments_store copies them to shared memory (seg_lo, seg_hi:
+// 64 entries, seg_pre: 65) for seg_find and seg_index.
 struct TileSegs {
     uint32_t lo[2], hi[2], pre[2];   // candidates l and l + 32 of lane l
     uint32_t total;                  // length of the concatenation
@@ -111,23 +111,6 @@ __device__ __forceinline__ void tile_segments_store(const TileSegs &s, uint32_t 
         seg_pre[l + 32 * h] = s.pre[h];
     }
     if (l == 31) seg_pre[64] = s.total;
-}
-
-// seg_find on the warp's registers: position i (< total) -> particle index.
-// Every lane of the warp must call it (lanes whose i is out of range get an
-// unspecified index and must not use it).
-__device__ __forceinline__ uint32_t tile_seg_find(const TileSegs &s, uint32_t i)
-{
-    auto at = [&](const uint32_t (&v)[2], int k) {
-        const uint32_t a = __shfl_sync(0xffffffffu, v[0], k & 31);
-        const uint32_t b = __shfl_sync(0xffffffffu, v[1], k & 31);
-        return k < 32 ? a : b;
-    };
-    int lo = 0;
-#pragma unroll
-    for (int step = 32; step > 0; step >>= 1)
-        if (at(s.pre, lo + step) <= i) lo += step;
-    return at(s.lo, lo) + (i - at(s.pre, lo));
 }
 
 // position i (< seg_pre[64]) of the concatenated candidate ranges -> particle index
