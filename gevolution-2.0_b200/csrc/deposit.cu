@@ -42,7 +42,17 @@
 
 namespace gev {
 
-constexpr int DEP_NT = 512;   // one thread per tile vertex
+constexpr int DEP_NT = 512;   // tile vertices; threads of the dense-tile launch (one per vertex)
+// Threads of the tile launch: 256, each summing the two vertices (x, y, 2k)
+// and (x, y, 2k + 1) of a z column, so that the records of the cell between
+// them are read once for both.
+#ifndef GEV_DEP_NT_TILE
+#define GEV_DEP_NT_TILE 256
+#endif
+static_assert(GEV_DEP_NT_TILE == 256 || GEV_DEP_NT_TILE == 512, "one or two vertices per thread");
+// FP64 records fill the shared memory of two CTAs per SM: the FP64 tile
+// launch keeps one thread per vertex (512 threads) for the resident warps.
+template <class R> __host__ __device__ constexpr int dep_tile_threads() { return sizeof(R) == 8 ? DEP_NT : GEV_DEP_NT_TILE; }
 #ifndef GEV_DEP_MINB_F
 #define GEV_DEP_MINB_F 3
 #endif
@@ -377,6 +387,8 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
     using S = DepShape<KIND>;
     constexpr int NC = S::NC, NF = S::NF, NFP = S::NFP;
     constexpr int CH = DepCh<R, KIND, DENSE>::v;
+    constexpr int NT = DENSE ? DEP_NT : dep_tile_threads<R>();   // threads
+    constexpr int VPT = DEP_NT / NT;                        // vertices per thread
     extern __shared__ __align__(16) unsigned char dsm[];
     R *rec = reinterpret_cast<R *>(dsm);                      // [CH][NFP]
     int *cstart = reinterpret_cast<int *>(rec + CH * NFP);    // 730
@@ -399,12 +411,12 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
     const R ra = (R)a, rm00 = (R)m00, rmij = (R)mij, rm0i = (R)m0i;
     // the phi stencil loads go out first and stay in flight while the bucket
     // ranges are looked up
-    constexpr int PER = (1000 + DEP_NT - 1) / DEP_NT;
+    constexpr int PER = (1000 + NT - 1) / NT;
     R pv[PER];
     if (USE_PHI) {
 #pragma unroll
         for (int k = 0; k < PER; k++) {
-            int s = t + k * DEP_NT;
+            int s = t + k * NT;
             if (s < 1000) {
                 int vx = s % 10 - 1, vy = (s / 10) % 10 - 1, vz = s / 100 - 1;
                 pv[k] = __ldg(phi + sidx(N, wrapi(x0 + vx, N), wrapi(y0 + vy, N), wrapi(z0 + vz, N)));
@@ -413,12 +425,12 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
     }
     // the tile's own particles (candidates 0..7: one contiguous range at the
     // head of the concatenation) are loaded as well, for the single-chunk path
-    constexpr int PP = (CH + DEP_NT - 1) / DEP_NT;   // at most two particles per thread
+    constexpr int PP = (CH + NT - 1) / NT;   // particles per thread (two or three)
     RawParticle<R> raw[PP];
     const uint32_t own_lo = bstart[8 * tile], own_n = bstart[8 * tile + 8] - own_lo;
 #pragma unroll
     for (int u = 0; u < PP; u++) {
-        const int j = t + u * DEP_NT;
+        const int j = t + u * NT;
         if ((uint32_t)j < own_n) raw[u] = load_particle(p, own_lo + (uint32_t)j);
     }
     // the candidate ranges, formed by warp 0 in registers and stored to shared
@@ -429,11 +441,11 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
         tile_segments_store(ts, seg_lo, seg_hi, seg_pre);
     }
     if (t < NC) vmax[t] = 0ull;
-    for (int c = t; c < 730; c += DEP_NT) { cstart[c] = DEP_RUN_NONE; ccount[c] = 0; }
+    for (int c = t; c < 730; c += NT) { cstart[c] = DEP_RUN_NONE; ccount[c] = 0; }
     if (USE_PHI) {
 #pragma unroll
         for (int k = 0; k < PER; k++) {
-            int s = t + k * DEP_NT;
+            int s = t + k * NT;
             if (s < 1000) phis[s] = pv[k];
         }
     }
@@ -441,11 +453,14 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
     const uint32_t total = seg_pre[64];
     if (total == 0) {
         // nothing reaches this tile: the deposit is zero
-        const int gx = x0 + (t & 7), gy = y0 + ((t >> 3) & 7), gz = z0 + (t >> 6);
-        const int64_t gi = sidx(N, gx, gy, gz);
         if (!accumulate) {
 #pragma unroll
-            for (int c = 0; c < NC; c++) out.p[c][gi] = (R)0;
+            for (int i = 0; i < VPT; i++) {
+                const int v = t + i * NT;
+                const int64_t gi = sidx(N, x0 + (v & 7), y0 + ((v >> 3) & 7), z0 + (v >> 6));
+#pragma unroll
+                for (int c = 0; c < NC; c++) out.p[c][gi] = (R)0;
+            }
         }
         return;
     }
@@ -458,7 +473,8 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
         }
     }
 
-    // exclusive scan of the 729 cell counts into cstart (two cells per thread)
+    // exclusive scan of the 729 cell counts into cstart (two cells per thread;
+    // the dense-tile launch's fixed-point path, 512 threads)
     auto scan_cells = [&]() {
         const int c0 = 2 * t, c1 = 2 * t + 1;
         const int n0 = c0 < DEP_NCELL ? ccount[c0] : 0;
@@ -472,13 +488,13 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
         if ((t & 31) == 31) wsum[t >> 5] = incl;
         __syncthreads();
         if (t < 32) {
-            int w = t < DEP_NT / 32 ? wsum[t] : 0, wi = w;
+            int w = t < NT / 32 ? wsum[t] : 0, wi = w;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 int u = __shfl_up_sync(0xffffffffu, wi, o);
                 if (t >= o) wi += u;
             }
-            if (t < DEP_NT / 32) wsum[t] = wi - w;   // exclusive warp offsets
+            if (t < NT / 32) wsum[t] = wi - w;   // exclusive warp offsets
         }
         __syncthreads();
         const int excl = incl - s + wsum[t >> 5];
@@ -486,22 +502,29 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
         if (c1 < DEP_NCELL) cstart[c1] = excl + n0;
     };
 
-    // this thread's vertex and the phi values its contributions need
-    const int vx = t & 7, vy = (t >> 3) & 7, vz = t >> 6;
-    R phv = 0, phx = 0, phy = 0, phz = 0;
-    if (USE_PHI) {
-        phv = phis[phi_slot(vx, vy, vz)];
-        phx = phis[phi_slot(vx + 1, vy, vz)];
-        phy = phis[phi_slot(vx, vy + 1, vz)];
-        phz = phis[phi_slot(vx, vy, vz + 1)];
-    }
-    const int64_t gout = sidx(N, x0 + vx, y0 + vy, z0 + vz);
+    // the phi values of vertex (vx, vy, vz): at the vertex and at its +x, +y, +z neighbours
+    auto vertex_phi = [&](int vx, int vy, int vz, R &pv0, R &pvx, R &pvy, R &pvz) {
+        pv0 = pvx = pvy = pvz = 0;
+        if (USE_PHI) {
+            pv0 = phis[phi_slot(vx, vy, vz)];
+            pvx = phis[phi_slot(vx + 1, vy, vz)];
+            pvy = phis[phi_slot(vx, vy + 1, vz)];
+            pvz = phis[phi_slot(vx, vy, vz + 1)];
+        }
+    };
+    auto write_vertex = [&](int vx, int vy, int vz, const R (&acc)[NC]) {
+        const int64_t g = sidx(N, x0 + vx, y0 + vy, z0 + vz);
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+            R *o = out.p[c];
+            o[g] = accumulate ? (R)(o[g] + acc[c]) : acc[c];
+        }
+    };
 
     // One chunk of n <= CH candidates whose particles are in raw[]: records
-    // stay at their load position and every vertex adds its contributions to
-    // acc in the field precision, in the fixed order (source cell, then ID).
-    const int lc0 = (vx + 1) + 9 * ((vy + 1) + 9 * (vz + 1));
-    auto sorted_chunk = [&](int n, RawParticle<R> (&raw)[PP], R (&acc)[NC]) {
+    // stay at their load position; every vertex then adds their contributions
+    // in the field precision, in a fixed order (source cell, then ID).
+    auto build_chunk = [&](int n, RawParticle<R> (&raw)[PP]) {
         // 1. record j at position j, the reach cell it came from, and the
         //    bounds [cstart, cend) of that cell's run as the smallest and
         //    largest positions of its records (shared-memory atomic min / max:
@@ -510,7 +533,7 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
         int *cend = ccount;
 #pragma unroll
         for (int u = 0; u < PP; u++) {
-            const int j = t + u * DEP_NT;
+            const int j = t + u * NT;
             if (j >= n) continue;
             R v[NF], b[NC];
             int lc;
@@ -527,23 +550,28 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
         // 2. every record is followed by the same cell up to its run's end:
         //    then each run holds exactly its cell's records (otherwise the
         //    bucket order was not sorted by cell)
-        {
-            bool bad = false;
-            for (int j = t; j < n; j += DEP_NT) {
-                const uint16_t lc = rcell[j];
-                if (lc == DEP_SKIP) continue;
-                const int e = cend[lc];
-                bad |= j + 1 < e && rcell[j + 1] != lc;
-            }
-            if (bad) atomicOr(err, ERR_BAD_ORDER);
+        bool bad = false;
+        for (int j = t; j < n; j += NT) {
+            const uint16_t lc = rcell[j];
+            if (lc == DEP_SKIP) continue;
+            const int e = cend[lc];
+            bad |= j + 1 < e && rcell[j + 1] != lc;
         }
-        // 3. gather: the vertex receives from the cells v - b, b in {0,1}^3
-        //    (a cell without records has cstart = DEP_RUN_NONE > cend = 0)
+        if (bad) atomicOr(err, ERR_BAD_ORDER);
+    };
+    // One vertex (VPT == 1): it receives from the cells v - b, b in {0,1}^3,
+    // in the order b = 0..7 (a cell without records has cstart = DEP_RUN_NONE
+    // > cend = 0).
+    const int vx = t & 7, vy = (t >> 3) & 7, vz = t >> 6;
+    auto gather_vertex = [&](R (&acc)[NC]) {
+        R phv, phx, phy, phz;
+        vertex_phi(vx, vy, vz, phv, phx, phy, phz);
+        const int lc0 = (vx + 1) + 9 * ((vy + 1) + 9 * (vz + 1));
 #pragma unroll
         for (int b = 0; b < 8; b++) {
             const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
             const int lc = lc0 - bx - 9 * by - 81 * bz;
-            const int k1 = cend[lc];
+            const int k1 = ccount[lc];
             for (int k = cstart[lc]; k < k1; k++) {
                 R r[NFP];
                 load_record<R, NFP>(rec, k, r);
@@ -551,11 +579,29 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
             }
         }
     };
-    auto write_acc = [&](const R (&acc)[NC]) {
+    // Two vertices of a z column (VPT == 2): (vx, vy, vz2) and (vx, vy, vz2 + 1)
+    // receive from the cells at z = vz2 - 1, vz2, vz2 + 1; the records of the
+    // middle cell feed both (bz = 0 for the lower vertex, bz = 1 for the
+    // upper).  Each vertex sums in a fixed order: cell z from low to high, then
+    // (bx, by) = (0,0), (1,0), (0,1), (1,1), then ID.
+    auto gather_pair = [&](int vz2, R (&acc0)[NC], R (&acc1)[NC]) {
+        R p0v, p0x, p0y, p0z, p1v, p1x, p1y, p1z;
+        vertex_phi(vx, vy, vz2, p0v, p0x, p0y, p0z);
+        vertex_phi(vx, vy, vz2 + 1, p1v, p1x, p1y, p1z);
 #pragma unroll
-        for (int c = 0; c < NC; c++) {
-            R *o = out.p[c];
-            o[gout] = accumulate ? (R)(o[gout] + acc[c]) : acc[c];
+        for (int zc = 0; zc < 3; zc++) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int bx = q & 1, by = q >> 1;
+                const int lc = (vx - bx + 1) + 9 * ((vy - by + 1) + 9 * (vz2 + zc));
+                const int k1 = ccount[lc];
+                for (int k = cstart[lc]; k < k1; k++) {
+                    R r[NFP];
+                    load_record<R, NFP>(rec, k, r);
+                    if (zc <= 1) gather_sum<R, KIND, USE_PHI>(r, bx, by, 1 - zc, p0v, p0x, p0y, p0z, acc0);
+                    if (zc >= 1) gather_sum<R, KIND, USE_PHI>(r, bx, by, 2 - zc, p1v, p1x, p1y, p1z, acc1);
+                }
+            }
         }
     };
 
@@ -569,14 +615,25 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
         // the neighbours' particles (the own ones are loaded already)
 #pragma unroll
         for (int u = 0; u < PP; u++) {
-            const int j = t + u * DEP_NT;
+            const int j = t + u * NT;
             if (j < n && (uint32_t)j >= own_n) raw[u] = load_particle(p, seg_find(seg_lo, seg_pre, (uint32_t)j));
         }
-        R acc[NC];
+        build_chunk(n, raw);
+        if constexpr (VPT == 2) {
+            const int vz2 = 2 * (t >> 6);
+            R acc0[NC], acc1[NC];
 #pragma unroll
-        for (int c = 0; c < NC; c++) acc[c] = 0;
-        sorted_chunk(n, raw, acc);
-        write_acc(acc);
+            for (int c = 0; c < NC; c++) { acc0[c] = 0; acc1[c] = 0; }
+            gather_pair(vz2, acc0, acc1);
+            write_vertex(vx, vy, vz2, acc0);
+            write_vertex(vx, vy, vz2 + 1, acc1);
+        } else {
+            R acc[NC];
+#pragma unroll
+            for (int c = 0; c < NC; c++) acc[c] = 0;
+            gather_vertex(acc);
+            write_vertex(vx, vy, vz, acc);
+        }
         return;
     } else {
 
@@ -597,18 +654,19 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
                 // records and runs of the previous chunk are done with; the run
                 // bounds start over before any record of this chunk updates them
                 __syncthreads();
-                for (int c = t; c < 730; c += DEP_NT) { cstart[c] = DEP_RUN_NONE; ccount[c] = 0; }
+                for (int c = t; c < 730; c += NT) { cstart[c] = DEP_RUN_NONE; ccount[c] = 0; }
                 __syncthreads();
             }
             // the chunk's particles (of the first chunk, the own ones are loaded already)
 #pragma unroll
             for (int u = 0; u < PP; u++) {
-                const uint32_t j = base + (uint32_t)(t + u * DEP_NT);
-                if (t + u * DEP_NT < n && (base > 0 || j >= own_n)) raw[u] = load_particle(p, seg_index(seg_lo, seg_pre, j));
+                const uint32_t j = base + (uint32_t)(t + u * NT);
+                if (t + u * NT < n && (base > 0 || j >= own_n)) raw[u] = load_particle(p, seg_index(seg_lo, seg_pre, j));
             }
-            sorted_chunk(n, raw, acc);
+            build_chunk(n, raw);
+            gather_vertex(acc);
         }
-        write_acc(acc);
+        write_vertex(vx, vy, vz, acc);
         return;
     }
 
@@ -640,7 +698,7 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
         R lb[NC];
 #pragma unroll
         for (int c = 0; c < NC; c++) lb[c] = 0;
-        for (uint32_t j = t; j < total; j += DEP_NT) {
+        for (uint32_t j = t; j < total; j += NT) {
             const uint32_t i = seg_index(seg_lo, seg_pre, j);
             R v[NF], b[NC];
             int lc;
@@ -658,12 +716,14 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
     long long acc[NC];
 #pragma unroll
     for (int c = 0; c < NC; c++) acc[c] = 0;
+    R phv, phx, phy, phz;
+    vertex_phi(vx, vy, vz, phv, phx, phy, phz);
 
     for (uint32_t base = 0; base < total; base += CH) {
         const int n = (int)min((uint32_t)CH, total - base);
         // 1. records and cell counts
         {
-            for (int j = t; j < n; j += DEP_NT) {
+            for (int j = t; j < n; j += NT) {
                 const uint32_t i = seg_index(seg_lo, seg_pre, base + (uint32_t)j);
                 R v[NF], b[NC];
                 int lc;
@@ -682,7 +742,7 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
         scan_cells();
         __syncthreads();
         // 3. counting sort of record indexes by cell
-        for (int j = t; j < n; j += DEP_NT) {
+        for (int j = t; j < n; j += NT) {
             const uint16_t lc = rcell[j];
             if (lc != DEP_SKIP) order[cstart[lc] + rslot[j]] = (uint16_t)j;
         }
@@ -700,7 +760,7 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
             }
         }
         __syncthreads();
-        for (int c = t; c < DEP_NCELL; c += DEP_NT) ccount[c] = 0;
+        for (int c = t; c < DEP_NCELL; c += NT) ccount[c] = 0;
         __syncthreads();
     }
 
@@ -716,7 +776,7 @@ __device__ __forceinline__ void deposit_tile(int tile, uint32_t *work, const PVi
 }
 
 template <class R, int KIND, bool USE_PHI>
-__global__ void __launch_bounds__(DEP_NT, DepMinBlocks<R, KIND>::v)
+__global__ void __launch_bounds__(dep_tile_threads<R>(), DepMinBlocks<R, KIND>::v)
     k_deposit(PView<R> p, const uint32_t *__restrict__ bstart, int N, int nt, const R *__restrict__ phi, DepOut<R> out,
               double a, double m00, double mij, double m0i, int accumulate, uint32_t *work, int *err, FastDiv fN)
 {
@@ -766,7 +826,7 @@ static void launch_k(const PView<R> &p, const uint32_t *bstart, int N, const R *
     const int nt = N / 8;
     const unsigned tiles = (unsigned)nt * nt * nt;
     const FastDiv fN((uint32_t)N);
-    k_deposit<R, KIND, USE_PHI><<<tiles, DEP_NT, smem, st>>>(p, bstart, N, nt, phi, out, a, m00, mij, m0i, accumulate,
+    k_deposit<R, KIND, USE_PHI><<<tiles, dep_tile_threads<R>(), smem, st>>>(p, bstart, N, nt, phi, out, a, m00, mij, m0i, accumulate,
                                                                work, err, fN);
     // one wave of resident CTAs; those that find the list empty return at once
     const unsigned grid = std::min(tiles, (unsigned)(sm_count() * GEV_DEP_MINB_DENSE));
