@@ -1,7 +1,8 @@
 // deposit.cu -- deterministic tile deposits of T00, Tij and T0i.
 //
-// One CTA owns the 8^3 vertices of a tile, one thread per vertex, and gathers
-// every particle whose CIC stencil touches them: its own 8 class buckets plus
+// One CTA owns the 8^3 vertices of a tile (one thread per vertex, or, in the
+// FP32 tile launch, per pair of vertices of a z column) and gathers every
+// particle whose CIC stencil touches them: its own 8 class buckets plus
 // the face-class buckets of the 7 lower neighbour tiles (tile_segments_warp).
 //
 // The CTA
@@ -15,14 +16,15 @@
 //      in chunks of records that fit shared memory (one chunk in the common
 //      case); tiles that touch a larger bucket sort record indexes by cell
 //      (counting sort) chunk by chunk;
-//   3. lets every vertex thread walk the 8 cells whose stencil covers it and
+//   3. lets every thread walk the cells whose stencil covers its vertex (8
+//      cells) or its two vertices (12 cells, the 4 between them shared) and
 //      accumulate the contributions in registers -- no shared-memory atomics
 //      on the accumulation path, each output vertex written once with plain
 //      stores, no global atomics and no halo fold (projection_comm1,
 //      gevolution.hpp:1543, is not needed on one GPU).
 // The result does not depend on the order in which the particles were given
 // (bitwise reproducible, for unique particle IDs):
-//   - sorted candidates: each vertex sums in R in the fixed order (source
+//   - sorted candidates: each vertex sums in R in a fixed order (source
 //     cell, ID), chunk after chunk;
 //   - tiles that touch a bucket above REBIN_SORT_MAX (kept in slot order)
 //     accumulate 64-bit fixed point with a per-CTA, per-component scale from
@@ -361,10 +363,10 @@ __host__ __device__ constexpr size_t dep_smem_bytes()
 }
 
 // Resident CTAs per SM the register budget is sized for.  The kernel is bound
-// by the latency of its dependent phases, so FP32 trades a few spilled
-// registers for more resident CTAs: three for the T00/Tij records (40
-// registers; their shared memory fits no fourth), four for the smaller T0i
-// records (32 registers).  FP64 records fill the shared memory of two CTAs.
+// by the latency of its dependent phases, so FP32 keeps as many CTAs as the
+// shared memory allows: three for the T00/Tij records (their shared memory
+// fits no fourth), four for the smaller T0i records.  FP64 records fill the
+// shared memory of two CTAs.
 template <class R, int KIND> struct DepMinBlocks { static constexpr int v = sizeof(R) == 4 ? GEV_DEP_MINB_F : 2; };
 template <> struct DepMinBlocks<float, DEP_T0I> { static constexpr int v = GEV_DEP_MINB_T0I_F; };
 template <> struct DepMinBlocks<float, DEP_T00_TIJ_S0I> { static constexpr int v = GEV_DEP_MINB_S_F; };
