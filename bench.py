@@ -160,7 +160,10 @@ SINGLE_KERNEL_STAGES = ("deposit_T00_Tij_T0i",)
 # cycle's deposit, its tile launch, plus its dense-tile launch (0.07 MB) from
 # the capture of the two-launch form; the separate T00+Tij and T0i kernels
 # from the earlier capture of the single-launch form), scaled by the particle
-# count; the profiles/ summaries record the captures
+# count; the profiles/ summaries record the captures.  The cycle's deposit was
+# captured with one vertex per thread; the two-vertex tile launch reads and
+# writes the same global arrays (it changes only how often a record is read
+# from shared memory).
 NCU_TRAFFIC_256 = {"deposit_T00_Tij_T0i": 0.7499e9 + 0.6387e9 + 0.0001e9, "deposit_T00_Tij": 0.7451e9 + 0.4423e9,
                    "deposit_T0i": 0.7434e9 + 0.1865e9}
 
